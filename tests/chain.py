@@ -1,0 +1,105 @@
+"""One fit iteration run operator by operator through a CPU library
+(the C restatement or the reference's own kernels compiled for the host).
+
+Used by the tests to compare the two CPU implementations with each other and
+with the CUDA path, and by tests/golden/make_golden.py.
+"""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def f32(shape, fill=0.0):
+    return np.full(shape, fill, np.float32)
+
+
+def build_pyramid(scene, texels, lib=None):
+    lib = lib or O.orc()
+    tw, th, C, L = scene.tex_w, scene.tex_h, scene.C, scene.levels
+    pyr = np.zeros(O.pyramid_size(tw, th, C, L), np.float32)
+    pyr[: tw * th * C] = texels.reshape(-1)
+    lib.mip_build(tw, th, C, L, pyr)
+    return pyr
+
+
+def project(lib, scene, pos):
+    clip = f32((scene.views, scene.nv, 4))
+    for v in range(scene.views):
+        out = f32((scene.nv, 4))
+        lib.project_fwd(scene.nv, scene.mvp[v].copy(), pos, 4, out)
+        clip[v] = out
+    return clip
+
+
+def run_chain(lib, scene, mode=0, target=None, rast=None, db=None, pos=None, pyr=None,
+              lobes=None, raster_lib=None, adam_step=1):
+    """Forward + backward of the predicted render, then one Adam step on a
+    copy of the texture level 0.  Returns a dict of every intermediate."""
+    S = scene
+    W, H, V, C, K = S.W, S.H, S.views, S.C, S.K
+    N = W * H * V
+    r = {}
+    pos = S.pos if pos is None else pos
+    r["clip"] = clip = project(lib, S, pos)
+    if rast is None:
+        rl = raster_lib or O.orc()
+        rast = f32((N, 4)); db = f32((N, 4))
+        rl.rasterize_fwd(W, H, V, clip, S.nv, S.tri, S.nt, 1, rast, db)
+    r["rast"], r["db"] = rast, db
+    uv = f32((N, 2)); uv_da = f32((N, 4))
+    lib.interpolate_fwd(W, H, V, 2, 1, rast, db, S.uv, S.tri, uv, uv_da)
+    r["uv"], r["uv_da"] = uv, uv_da
+    if pyr is None:
+        pyr = build_pyramid(S, S.tex_init)
+    r["pyr"] = pyr
+    diffuse = f32((N, C))
+    lib.texture_fwd(W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, uv, uv_da, diffuse)
+    r["diffuse"] = diffuse
+    normal = f32((N, 3)); lib.normal_axis_fwd(W, H, V, rast, S.rot, S.normal, S.tri, normal)
+    view = f32((N, 3)); lib.view_axis_fwd(W, H, V, S.pvinv, view)
+    r["normal"], r["view"] = normal, view
+    rough = f32((N,), S.roughness)
+    sax = f32((N, 3)); ssh = f32((N,)); sam = f32((N,))
+    lib.sg_specular_fwd(W, H, V, rast, normal, view, rough, S.ior, sax, ssh, sam)
+    r["spec_axis"], r["spec_sharp"], r["spec_amp"] = sax, ssh, sam
+    axis, sharp, amp = lobes if lobes is not None else (S.lobe_axis_init, S.lobe_sharp_init, S.lobe_amp_init)
+    color = f32((N, C)); denv = f32((N, C)); senv = f32((N, C))
+    lib.sg_fwd(W, H, V, C, rast, K, axis, sharp, amp, normal, diffuse, sax, ssh, sam, color, denv, senv)
+    r["color"], r["diffenv"], r["specenv"] = color, denv, senv
+    aa = f32((N, C))
+    lib.antialias_fwd(W, H, V, C, clip, S.nv, S.tri, rast, color, aa)
+    r["aa"] = aa
+    if target is None:
+        target = np.random.default_rng(S.seed + 7).random((N, C)).astype(np.float32)
+    r["target"] = target
+    g_aa = f32((N, C))
+    r["loss"] = lib.mse(mode, N * C, aa, target, g_aa)
+    r["g_aa"] = g_aa
+    g_color = f32((N, C)); g_clip = f32((V, S.nv, 4))
+    lib.antialias_bwd(mode, W, H, V, C, clip, S.nv, S.tri, rast, color, g_aa, g_color, g_clip)
+    r["g_color"], r["g_clip_aa"] = g_color, g_clip.copy()
+    g_diffuse = f32((N, C)); g_axis = f32((K, 3)); g_sharp = f32((K,)); g_amp = f32((K, C))
+    g_sax = f32((N, 3)); g_ssh = f32((N,)); g_sam = f32((N * C,))
+    lib.sg_bwd(mode, W, H, V, C, rast, K, axis, sharp, amp, normal, diffuse, sax, ssh, sam, g_color,
+               g_diffuse, g_axis, g_sharp, g_amp, g_sax, g_ssh, g_sam)
+    r.update(g_diffuse=g_diffuse, g_axis=g_axis, g_sharp=g_sharp, g_amp=g_amp, g_sax=g_sax, g_ssh=g_ssh, g_sam=g_sam)
+    g_rough = f32((N,))
+    lib.sg_specular_bwd(W, H, V, rast, normal, view, rough, S.ior, g_sam, g_ssh, g_rough)
+    r["g_rough"] = g_rough
+    g_pyr = np.zeros_like(pyr); g_uv = f32((N, 2)); g_uv_da = f32((N, 4))
+    lib.texture_bwd(W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, uv, uv_da, g_diffuse, g_pyr, g_uv, g_uv_da)
+    r["g_pyr"], r["g_uv"], r["g_uv_da"] = g_pyr, g_uv, g_uv_da
+    g_uvattr = f32((S.nv, 2)); g_bary = f32((N, 2))
+    lib.interpolate_bwd(mode, W, H, V, 2, rast, S.uv, S.tri, g_uv, g_uvattr, g_bary)
+    r["g_uvattr"], r["g_bary"] = g_uvattr, g_bary
+    lib.rasterize_bwd(W, H, V, clip, S.nv, S.tri, rast, g_bary, g_clip)
+    r["g_clip"] = g_clip
+    g_pos = f32((S.nv, 3))
+    for v in range(V):
+        lib.project_bwd(S.nv, S.mvp[v].copy(), np.ascontiguousarray(g_clip[v]), 4, g_pos)
+    r["g_pos"] = g_pos
+    n0 = S.tex_w * S.tex_h * C
+    p = pyr[:n0].copy(); m = f32((n0,)); vv = f32((n0,))
+    lib.adam(mode, n0, p, np.ascontiguousarray(g_pyr[:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, adam_step)
+    r["adam_p"], r["adam_m"], r["adam_v"] = p, m, vv
+    return r
