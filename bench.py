@@ -1,0 +1,445 @@
+"""Benchmark: fit iterations per second (forward + backward + Adam) of the
+inverse-rendering fit on the scale configuration -- UV sphere 256x128
+(65,024 triangles) displaced N(0,0.02), 8 views of 1024x1024, 2048^2 RGBA
+texture with 12 mip levels, 32 SG lobes, Adam on positions, texture and
+lobes -- with seeded synthetic inputs (no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vcl|reference]
+
+One JSON line on rank 0.  Multi-GPU runs are independent replicas (one fit
+job per GPU, no data-path collective; weak scaling); times are max over
+ranks.  See the module-level notes at each measured quantity.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd+Adam iters/s @1024² batch 16, batched vs plain; p50/p99 fit-job latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="vcl", choices=["vcl", "reference"])
+    ap.add_argument("--views", type=int, default=8)
+    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-stages", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(args):
+    from vcl_b200 import scenes
+    if args.config == "config1":
+        return scenes.config1()
+    if args.config == "config5":
+        return scenes.config5()
+    return scenes.config2(views=args.views)
+
+
+def workload_name(S):
+    return (f"fit iteration: {S.name}: {S.nt} tris, {S.views} views {S.W}x{S.H}, texture {S.tex_w}^2x{S.C} "
+            f"({S.levels} levels), {S.K} SG lobes, Adam on positions+texture+lobes")
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ algorithmic bytes
+def stage_bytes(S, ncov):
+    """Compulsory FP32 traffic per fit iteration by stage (caches ignored,
+    each buffer counted once), the per-stage model of the design notes."""
+    N = S.W * S.H * S.views
+    C = S.C
+    ntex = S.tex_w * S.tex_h
+    npyr_bytes = ntex * C * 4 * 4 / 3
+    texel_fwd = min(npyr_bytes, ncov * 8 * C * 4)
+    return {
+        "raster_fwd": S.nv * 16 * S.views + S.nt * 12 + N * 32,
+        "interp_fwd": N * (16 + 16) + N * (8 + 16),
+        "texture_fwd": N * (4 + 8 + 16) + N * C * 4 + texel_fwd,
+        "normal_axis": N * 16 + N * 12,
+        "view_axis": N * 12,
+        "sg_specular_fwd": N * (16 + 12 + 12 + 4) + N * 20,
+        "sg_fwd": N * (16 + 12 + C * 4 + 12 + 8) + N * C * 4 + S.K * (4 + C) * 4,
+        "antialias_fwd": N * (16 + C * 4) + N * C * 4,
+        "mse": N * C * 4 * 2 + N * C * 4,
+        "antialias_bwd": N * (C * 8 + 16) + N * C * 4,
+        "sg_bwd": N * (C * 4 * 2 + 16 + 12 + 12 + 8) + N * C * 4,
+        "texture_bwd": N * (C * 4 + 4 + 8 + 16) + N * 8 + texel_fwd,
+        "interp_bwd": N * (16 + 8) + N * 8,
+        "raster_bwd": N * (16 + 8),
+        "project": S.nv * 12 * 2,
+        "optimizer": 28 * (ntex * C + S.nv * 3 + S.K * (4 + C)) + ntex * C * 4 * (1 / 3 + 2 / 3 + 1 + 4 / 3),
+    }
+
+
+# ------------------------------------------------------------------ vcl arm
+def run_vcl(args, rank, world):
+    import torch
+    from vcl_b200 import capi
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    S = make_scene(args)
+    ctx = capi.Context(dev)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    N = S.W * S.H * S.views
+    img_numel = N * S.C
+
+    # targets: the true scene rendered once + N(0, 0.05) pixel noise
+    truth = capi.Fit(ctx, S, tex=S.tex_target, pos=S.pos_target,
+                     lobes=(S.lobe_axis, S.lobe_sharp, S.lobe_amp), learn=(0, 0, 0))
+    target = torch.zeros(img_numel, dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(stream):
+        truth.render(target, sh)
+        g = torch.Generator(device="cuda").manual_seed(S.seed + 1)
+        target.add_(torch.randn(img_numel, generator=g, device="cuda") * S.noise)
+    stream.synchronize()
+    truth.close()
+
+    def make_fit(strategy):
+        f = capi.Fit(ctx, S, strategy=strategy)
+        f.set_target(target, sh, is_device=True)
+        return f
+
+    def timed(fit, steps, warmup):
+        for _ in range(warmup):
+            fit.step(sh)
+        stream.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fit.step(sh)
+        e1.record(stream)
+        stream.synchronize()
+        barrier()
+        return e0.elapsed_time(e1)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def maxr(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    out = {}
+    strategies = [("plain", capi.FIT_PLAIN)]
+    try:
+        f = make_fit(capi.FIT_FUSED)
+        f.step(sh)
+        stream.synchronize()
+        f.close()
+        strategies.append(("fused", capi.FIT_FUSED))
+    except capi.VclError:
+        pass
+    clocks = ClockSampler(dev)
+    results = {}
+    launches = {}
+    losses = {}
+    for name, strat in strategies:
+        fit = make_fit(strat)
+        if name == strategies[-1][0]:
+            clocks.start()
+        ms = maxr(timed(fit, args.steps, args.warmup))
+        if name == strategies[-1][0]:
+            clk = clocks.stop()
+        results[name] = ms
+        launches[name] = fit.launches_per_step()
+        losses[name] = fit.read_loss(sh)
+        fit.close()
+    best = strategies[-1][0]
+    ms_per_step = results[best] / args.steps
+    value = world * 1000.0 / ms_per_step
+
+    # end to end through the public API: pinned host targets and cameras in,
+    # loss out, every step
+    fit = make_fit(strategies[-1][1])
+    host_target = torch.empty(img_numel, dtype=torch.float32, pin_memory=True)
+    host_target.copy_(target.cpu())
+    mvp = np.ascontiguousarray(S.mvp)
+    pvinv = np.ascontiguousarray(S.pvinv)
+
+    def e2e_step():
+        fit.set_target(host_target.data_ptr(), sh, is_device=False)
+        fit.set_cameras(mvp, pvinv, sh)
+        fit.step(sh)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    stream.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+        fit.read_loss(sh)   # device->host read of the step's loss (synchronizes)
+    e1.record(stream)
+    stream.synchronize()
+    barrier()
+    e2e_ms = maxr(e0.elapsed_time(e1)) / args.steps
+    fit.close()
+
+    out.update(results=results, launches=launches, losses=losses, value=value, ms_per_step=ms_per_step,
+               e2e_ms=e2e_ms, clocks=clk, scene=S, best=best)
+    if rank == 0 and not args.no_stages:
+        out["stages"] = stage_times(ctx, S, target, stream)
+    ctx.close()
+    return out
+
+
+def stage_times(ctx, S, target, stream, reps=5):
+    """Average device time of each operator of the plain pipeline on this
+    workload (CUDA events on the launching stream around `reps` launches of
+    that operator, after one untimed pass)."""
+    import torch
+    from vcl_b200 import capi
+    sh = stream.cuda_stream
+    W, H, V, C, K = S.W, S.H, S.views, S.C, S.K
+    N = W * H * V
+    f32 = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")
+    dv = lambda a, dt=None: torch.from_numpy(np.ascontiguousarray(a if dt is None else a.astype(dt))).cuda()
+    tri = dv(S.tri, np.int32)
+    mvp, pos, uvattr, rot, nrm, pvinv = dv(S.mvp), dv(S.pos), dv(S.uv), dv(S.rot), dv(S.normal), dv(S.pvinv)
+    axis, sharp, amp = dv(S.lobe_axis_init), dv(S.lobe_sharp_init), dv(S.lobe_amp_init)
+    npyr = sum((S.tex_w >> l) * (S.tex_h >> l) * C for l in range(S.levels))
+    pyr = f32(npyr)
+    pyr[: S.tex_w * S.tex_h * C] = dv(S.tex_target).reshape(-1)
+    clip, rast, db = f32(V, S.nv, 4), f32(N, 4), f32(N, 4)
+    uv, uv_da, diffuse, normal, view = f32(N, 2), f32(N, 4), f32(N, C), f32(N, 3), f32(N, 3)
+    rough = torch.full((N,), S.roughness, dtype=torch.float32, device="cuda")
+    sax, ssh, sam, color, aa = f32(N, 3), f32(N), f32(N), f32(N, C), f32(N, C)
+    g_aa, g_color, g_clip, loss = f32(N, C), f32(N, C), f32(V, S.nv, 4), f32(1)
+    g_diff, g_axis, g_sharp, g_amp = f32(N, C), f32(K, 3), f32(K), f32(K, C)
+    g_pyr, g_uv, g_bary, g_pos = f32(npyr), f32(N, 2), f32(N, 2), f32(S.nv, 3)
+    n0 = S.tex_w * S.tex_h * C
+    m, v = f32(n0), f32(n0)
+    ops = [
+        ("project", lambda: ctx.project_fwd(mvp, V, pos, S.nv, 4, clip, sh)),
+        ("raster_fwd", lambda: ctx.rasterize_fwd(clip, S.nv, tri, S.nt, W, H, V, rast, db, sh)),
+        ("interp_fwd", lambda: ctx.interpolate_fwd(rast, db, W, H, V, uvattr, S.nv, 2, tri, S.nt, uv, uv_da, sh)),
+        ("texture_fwd", lambda: ctx.texture_fwd(rast, uv, uv_da, W, H, V, pyr, S.tex_w, S.tex_h, C, S.levels, diffuse, sh)),
+        ("normal_axis", lambda: ctx.normal_axis_fwd(rast, W, H, V, rot, nrm, S.nv, tri, S.nt, normal, sh)),
+        ("view_axis", lambda: ctx.view_axis_fwd(W, H, V, pvinv, view, sh)),
+        ("sg_specular_fwd", lambda: ctx.sg_specular_fwd(rast, W, H, V, normal, view, rough, S.ior, sax, ssh, sam, sh)),
+        ("sg_fwd", lambda: ctx.sg_fwd(rast, W, H, V, C, K, axis, sharp, amp, normal, diffuse, sax, ssh, sam, color,
+                                      None, None, sh)),
+        ("antialias_fwd", lambda: ctx.antialias_fwd(clip, S.nv, tri, S.nt, rast, W, H, V, C, color, aa, sh)),
+        ("mse", lambda: ctx.mse(aa, target, N * C, g_aa, loss, sh)),
+        ("antialias_bwd", lambda: ctx.antialias_bwd(clip, S.nv, tri, S.nt, rast, W, H, V, C, color, g_aa, g_color,
+                                                    g_clip, sh)),
+        ("sg_bwd", lambda: ctx.sg_bwd(rast, W, H, V, C, K, axis, sharp, amp, normal, diffuse, sax, ssh, sam, g_color,
+                                      g_diff, g_axis, g_sharp, g_amp, None, None, None, sh)),
+        ("texture_bwd", lambda: ctx.texture_bwd(rast, uv, uv_da, W, H, V, pyr, S.tex_w, S.tex_h, C, S.levels, g_diff,
+                                                g_pyr, g_uv, None, sh)),
+        ("interp_bwd", lambda: ctx.interpolate_bwd(rast, W, H, V, uvattr, S.nv, 2, tri, S.nt, g_uv, None, g_bary, sh)),
+        ("raster_bwd", lambda: ctx.rasterize_bwd(clip, S.nv, tri, S.nt, W, H, V, rast, g_bary, g_clip, sh)),
+        ("optimizer", lambda: ctx.adam_step(pyr, g_pyr, m, v, n0, 1e-2, 0.9, 0.999, 1e-8, 1, sh)),
+    ]
+    res = {}
+    with torch.cuda.stream(stream):
+        for name, fn in ops:
+            fn()
+        stream.synchronize()
+        ncov = int((rast[:, 3] > 0).sum().item())
+        for name, fn in ops:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+            res[name] = e0.elapsed_time(e1) / reps
+    return {"ms": res, "ncov": ncov}
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_reference_iteration(S, threads, views_sample=1):
+    """Time the reference's own kernels (oracle/_ref, compiled for the host)
+    on `views_sample` views of one fit iteration plus the parameter update,
+    with `threads` host threads; the raster stage is the CPU restatement of
+    the reference's GL rasterizer.  Returns (seconds for a full iteration
+    extrapolated to all views, kind, sample description)."""
+    from oracle import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import chain
+    lib = O.ref()
+    kind = "reference"
+    if lib is None:
+        lib, kind = O.orc(), "port"
+    else:
+        lib.set_threads(threads)
+    import types
+    sub = types.SimpleNamespace(**{k: getattr(S, k) for k in S.__dataclass_fields__})
+    sub.views = views_sample
+    sub.mvp = S.mvp[:views_sample].copy()
+    sub.pvinv = S.pvinv[:views_sample].copy()
+    sub.nv, sub.nt = S.nv, S.nt
+    pyr = chain.build_pyramid(sub, S.tex_init)
+    t0 = time.perf_counter()
+    chain.run_chain(lib, sub, 0, pyr=pyr, raster_lib=O.orc())
+    per_views = time.perf_counter() - t0
+    # the chain already includes one Adam step on the texture; add the mip
+    # rebuild and the remaining parameter groups
+    t1 = time.perf_counter()
+    O.orc().mip_build(S.tex_w, S.tex_h, S.C, S.levels, pyr)
+    par = time.perf_counter() - t1
+    total = per_views * (S.views / views_sample) + par
+    if lib is not O.orc():
+        lib.set_threads(1)
+    return total, kind, (f"{views_sample} of {S.views} views of one fit iteration (all per-pixel operators "
+                         f"fwd+bwd, Adam on the texture) + mip rebuild, extrapolated to {S.views} views; raster "
+                         f"stage = CPU restatement of the GL rasterizer")
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU implementation of the path,
+    all host threads, bounded per-step samples of the same workload."""
+    S = make_scene(args)
+    threads = os.cpu_count() or 1
+    steps, warm = args.steps, args.warmup
+    for _ in range(min(warm, 1)):
+        cpu_reference_iteration(S, threads)
+    times = []
+    for _ in range(max(1, min(steps, 3))):
+        t, kind, sample = cpu_reference_iteration(S, threads)
+        times.append(t)
+    per_iter = statistics.median(times)
+    v = 1.0 / per_iter
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": args.gpus,
+            "steps": len(times), "warmup": min(warm, 1), "ms_per_step": per_iter * 1000, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(S), "global_batch": S.views, "seq_len": 0,
+                       "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "iters/s", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
+    import torch
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = run_vcl(args, rank, world)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    S = r["scene"]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": "iters/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": workload_name(S), "strategy": r["best"], "global_batch": S.views * world,
+                   "seq_len": 0, "parallelism": f"replicas x{world}",
+                   "l2": "per-step working set > 2 GB (larger than the 126 MB L2); no flush"},
+        "plain": {"ms_per_step": r["results"]["plain"] / args.steps,
+                  "iters_per_s": world * 1000.0 * args.steps / r["results"]["plain"]},
+        "gpu_launches": r["launches"][r["best"]] * args.steps,
+        "clocks": r["clocks"],
+        "e2e": {"value": world * 1000.0 / r["e2e_ms"], "unit": "iters/s",
+                "h2d_bytes_per_step": S.views * S.H * S.W * S.C * 4 + S.views * (16 + 9) * 4,
+                "d2h_bytes_per_step": 4},
+        "loss_last": r["losses"][r["best"]],
+    }
+    if "stages" in r:
+        st = r["stages"]
+        byts = stage_bytes(S, st["ncov"])
+        ms = st["ms"]
+        top = max(ms, key=lambda k: ms[k])
+        b = byts.get(top, 0)
+        achieved = b / (ms[top] * 1e-3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                            "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                            "algorithmic_bytes": b, "avg_ms": ms[top]}
+        line["stages_ms"] = {k: round(v, 4) for k, v in ms.items()}
+        line["stages_frac_hbm"] = {k: round(byts.get(k, 0) / (v * 1e-3) / 1e9 / hbm_peak, 3) for k, v in ms.items()
+                                   if v > 0}
+    if not args.no_cpu_baseline:
+        t, kind, sample = cpu_reference_iteration(S, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "iters/s", "cores": os.cpu_count() or 1, "kind": kind,
+                                "sample": sample}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Each operator gets the oracle's inputs for its stage, so every comparison
+isolates one kernel.  Bars: triangle ids, barycentrics, depth and DB are
+bit-identical (the rasterizer uses exactly rounded arithmetic); every other
+output within 1e-5 relative to the array's largest magnitude (FP32; atomic
+accumulation order differs)."""
+import numpy as np
+import pytest
+
+import chain
+from oracle import oracle as O
+from vcl_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+REL_TOL = 1e-5
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = max(np.abs(b).max(initial=0.0), 1e-30)
+    return np.abs(a - b).max(initial=0.0) / scale
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from vcl_b200 import capi
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def _scenes():
+    return [
+        scenes.small(seed=1),
+        scenes.small(seed=2, W=64, H=48, views=3, subdiv=2, tex=64, K=5),
+        scenes.small(seed=5, W=130, H=97, views=2, subdiv=3, tex=128, K=16),
+        scenes.small(seed=6, W=96, H=80, views=1, subdiv=2, tex=32, K=4, C=3),
+    ]
+
+
+SCENES = _scenes()
+KEYS = ["clip", "uv", "uv_da", "diffuse", "normal", "view", "spec_axis", "spec_sharp", "spec_amp", "color",
+        "diffenv", "specenv", "aa", "g_aa", "g_color", "g_clip_aa", "g_diffuse", "g_axis", "g_sharp", "g_amp",
+        "g_sax", "g_ssh", "g_sam", "g_rough", "g_pyr", "g_uv", "g_uv_da", "g_uvattr", "g_bary", "g_clip", "g_pos",
+        "adam_p", "adam_m", "adam_v"]
+
+
+def _gpu_chain():
+    import gpu_chain
+    return gpu_chain
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("si", range(len(SCENES)))
+def test_operators_match_oracle(ctx, si, mode):
+    S = SCENES[si]
+    pyr = chain.build_pyramid(S, S.tex_target)
+    o = chain.run_chain(O.orc(), S, mode, pyr=pyr)
+    g = _gpu_chain().run_chain_gpu(ctx, S, o, mode)
+    assert (o["rast"][:, 3] > 0).sum() > 0
+    assert np.array_equal(g["rast"][:, 3], o["rast"][:, 3]), "triangle ids differ"
+    assert np.array_equal(g["rast"], o["rast"]), "barycentrics/depth differ"
+    assert np.array_equal(g["db"], o["db"]), "DB differs"
+    bad = {k: rel_err(g[k], o[k]) for k in KEYS if rel_err(g[k], o[k]) > REL_TOL}
+    assert not bad, bad
+    n = S.W * S.H * S.views * S.C
+    exact_loss = O.orc().mse(1, n, o["aa"], o["target"], np.zeros(n, np.float32))
+    assert abs(g["loss"] - exact_loss) <= REL_TOL * abs(exact_loss)
+    assert ctx.check_indices() == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_chained_pipeline_matches_oracle(ctx, mode):
+    S = SCENES[2]
+    pyr = chain.build_pyramid(S, S.tex_target)
+    o = chain.run_chain(O.orc(), S, mode, pyr=pyr)
+    g = _gpu_chain().run_chain_gpu(ctx, S, o, mode, chained=True)
+    assert np.array_equal(g["rast"], o["rast"])
+    for k in ("aa", "g_pyr", "g_pos", "g_axis", "g_amp", "adam_p"):
+        assert rel_err(g[k], o[k]) <= 1e-4, (k, rel_err(g[k], o[k]))
+
+
+@pytest.mark.parametrize("tile,cap", [(8, 0), (16, 0), (32, 0), (16, 64), (8, 1)])
+def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap):
+    import gpu_chain as G
+    S = scenes.make_scene("raster", mesh=("ico", 4), W=200, H=150, views=2, tex=16, K=1, dist=(2.0, 3.5),
+                          disp=0.05, seed=9)
+    clip = chain.project(O.orc(), S, S.pos)
+    N = S.W * S.H * S.views
+    rast = np.zeros((N, 4), np.float32); db = np.zeros((N, 4), np.float32)
+    O.orc().rasterize_fwd(S.W, S.H, S.views, clip, S.nv, S.tri, S.nt, 1, rast, db)
+    ctx.set_raster_config(tile, cap)
+    try:
+        gr = G.zeros(N, 4); gd = G.zeros(N, 4)
+        ctx.rasterize_fwd(G.dev(clip), S.nv, G.dev(S.tri.astype(np.int32)), S.nt, S.W, S.H, S.views, gr, gd, None)
+        ov = ctx.raster_overflow_count()
+        assert np.array_equal(G.host(gr), rast)
+        assert np.array_equal(G.host(gd), db)
+        if cap:
+            assert ov > 0
+        else:
+            assert ov == 0
+    finally:
+        ctx.set_raster_config(16, 0)
+
+
+def test_raster_config1_scale_bit_exact(ctx):
+    import gpu_chain as G
+    S = scenes.config1()
+    clip = chain.project(O.orc(), S, S.pos)
+    N = S.W * S.H * S.views
+    rast = np.zeros((N, 4), np.float32); db = np.zeros((N, 4), np.float32)
+    O.orc().rasterize_fwd(S.W, S.H, S.views, clip, S.nv, S.tri, S.nt, 1, rast, db)
+    gr = G.zeros(N, 4); gd = G.zeros(N, 4)
+    ctx.rasterize_fwd(G.dev(clip), S.nv, G.dev(S.tri.astype(np.int32)), S.nt, S.W, S.H, S.views, gr, gd, None)
+    assert np.array_equal(G.host(gr), rast)
+    assert np.array_equal(G.host(gd), db)
+
+
+def test_raster_edge_cases(ctx):
+    import gpu_chain as G
+    cases = [
+        (np.array([[-1, -1, 0.5, 1], [3, -1, 0.5, 1], [-1, 3, 0.5, 1]], np.float32), [[0, 1, 2]]),
+        (np.array([[0, 0, 0, 1], [0.5, 0.5, 0, 1], [1, 1, 0, 1]], np.float32), [[0, 1, 2]]),   # degenerate
+        (np.array([[-1, -1, 0.2, 1], [3, -1, 0.2, 1], [-1, 3, 0.2, 1],
+                   [-1, -1, 0.2, 1], [3, -1, 0.2, 1], [-1, 3, 0.2, 1]], np.float32), [[0, 1, 2], [3, 4, 5]]),
+        (np.array([[-0.5, -0.5, -2, 0.5], [2, -1, 0.5, 1.5], [-1, 2, 0.9, 1.0]], np.float32), [[0, 1, 2]]),  # near clip
+        (np.array([[-1, -1, 0, -1], [3, -1, 0, 2], [-1, 3, 0, 2]], np.float32), [[0, 1, 2]]),  # one vertex behind
+    ]
+    for W, H in ((7, 5), (16, 16), (33, 17)):
+        for clip, tri in cases:
+            tri = np.array(tri, np.uint32)
+            N = W * H
+            r = np.zeros((N, 4), np.float32); d = np.zeros((N, 4), np.float32)
+            O.orc().rasterize_fwd(W, H, 1, clip, clip.shape[0], tri, tri.shape[0], 1, r, d)
+            gr = G.zeros(N, 4); gd = G.zeros(N, 4)
+            ctx.rasterize_fwd(G.dev(clip), clip.shape[0], G.dev(tri.astype(np.int32)), tri.shape[0], W, H, 1, gr, gd, None)
+            assert np.array_equal(G.host(gr), r), (W, H, tri.shape)
+            assert np.array_equal(G.host(gd), d)
+    # empty mesh
+    gr = G.zeros(64, 4)
+    ctx.rasterize_fwd(G.zeros(1, 4), 0, G.dev(np.zeros((1, 3), np.int32)), 0, 8, 8, 1, gr, None, None)
+    assert float(gr.abs().sum()) == 0.0
+
+
+def test_out_of_range_indices_are_reported_not_read(ctx):
+    import gpu_chain as G
+    W = H = 8
+    N = W * H
+    rast = np.zeros((N, 4), np.float32)
+    rast[:, 3] = 5.0          # triangle id 4 of a 1-triangle mesh
+    out = G.zeros(N, 2)
+    ctx.interpolate_fwd(G.dev(rast), None, W, H, 1, G.dev(np.zeros((3, 2), np.float32)), 3, 2,
+                        G.dev(np.array([[0, 1, 2]], np.int32)), 1, out, None, None)
+    assert ctx.check_indices() == 1
+    assert float(out.abs().sum()) == 0.0
+    assert ctx.check_indices() == 0
+
+
+def test_mip_build_pushdown_clamp_match_oracle(ctx):
+    import gpu_chain as G
+    rng = np.random.default_rng(4)
+    for tw, th, C in ((64, 32, 4), (48, 16, 3)):
+        L = O.tex_levels(tw, th, 16)
+        n = O.pyramid_size(tw, th, C, L)
+        pyr = np.zeros(n, np.float32); pyr[: tw * th * C] = rng.random(tw * th * C)
+        ref = pyr.copy(); O.orc().mip_build(tw, th, C, L, ref)
+        t = G.dev(pyr); ctx.texture_build_mips(t, tw, th, C, L, None)
+        assert np.array_equal(G.host(t), ref)
+        for mode in (0, 1):
+            gg = rng.normal(size=n).astype(np.float32)
+            ref = gg.copy(); O.orc().mip_pushdown(mode, tw, th, C, L, ref)
+            ctx.set_mode(mode)
+            t = G.dev(gg); ctx.texture_grad_pushdown(t, tw, th, C, L, None)
+            assert np.array_equal(G.host(t), ref)
+        ctx.set_mode(0)
+        x = (rng.normal(size=n) * 2).astype(np.float32)
+        ref = x.copy(); O.orc().clamp(n, ref, 0.0, 1.0)
+        t = G.dev(x); ctx.clamp(t, n, 0.0, 1.0, None)
+        assert np.array_equal(G.host(t), ref)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_adam_bit_exact_over_steps(ctx, mode):
+    import gpu_chain as G
+    rng = np.random.default_rng(1)
+    n = 1003
+    p = rng.random(n).astype(np.float32)
+    m = np.zeros(n, np.float32); v = np.zeros(n, np.float32)
+    tp, tm, tv = G.dev(p), G.dev(m), G.dev(v)
+    ctx.set_mode(mode)
+    for step in range(1, 6):
+        g = rng.normal(size=n).astype(np.float32)
+        O.orc().adam(mode, n, p, g, m, v, 1e-2, 0.9, 0.999, 1e-8, step)
+        ctx.adam_step(tp, G.dev(g), tm, tv, n, 1e-2, 0.9, 0.999, 1e-8, step, None)
+    ctx.set_mode(0)
+    assert np.array_equal(G.host(tp), p)
+    assert np.array_equal(G.host(tm), m)
+    assert np.array_equal(G.host(tv), v)

@@ -1,0 +1,63 @@
+"""Build libvcl.so (all CUDA sources under csrc/) for sm_100a with nvcc.
+
+The library is built in-tree (vcl_b200/libvcl.so) so that it travels with the
+repository; object files go to vcl_b200/_build/.  Only sources newer than
+their object are recompiled.
+"""
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libvcl.so")
+ROOT = os.path.dirname(HERE)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",
+           "-I" + os.path.join(ROOT, "include")]
+
+
+def nvcc():
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(p):
+        raise RuntimeError("nvcc not found")
+    return p
+
+
+def _deps(src):
+    hdrs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return [src] + hdrs
+
+
+def build(verbose=False, extra=None):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    objs = []
+    changed = False
+    for s in srcs:
+        o = os.path.join(BUILD, os.path.basename(s) + ".o")
+        objs.append(o)
+        if os.path.exists(o) and all(os.path.getmtime(o) >= os.path.getmtime(d) for d in _deps(s)):
+            continue
+        cmd = [nvcc()] + ARCH + NVFLAGS + (extra or []) + ["-c", s, "-o", o]
+        if s.endswith(".cpp"):
+            cmd = [nvcc()] + NVFLAGS + (extra or []) + ["-x", "c++", "-c", s, "-o", o]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        changed = True
+    if changed or not os.path.exists(LIB):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv)
+    print(LIB)

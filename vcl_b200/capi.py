@@ -1,0 +1,263 @@
+"""ctypes binding of the vcl C ABI (include/vcl.h) in libvcl.so.
+
+This is the reference-side binding a Python caller uses: every function of
+vcl.h is declared here with its argument types.  Buffers are passed as raw
+device addresses (for example ``tensor.data_ptr()`` of a CUDA tensor) and
+streams as raw ``cudaStream_t`` handles.  There is no fallback: if the
+library is missing or a call fails, an exception is raised.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvcl.so")
+
+c_int, c_ll, c_size, c_float, c_double, c_void_p, c_char_p = (
+    ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_float, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p)
+P = c_void_p
+
+MODE_COMPAT = 0
+MODE_EXACT = 1
+
+# name: (restype, [argtypes])
+SIGNATURES = {
+    "vcl_version": (c_char_p, []),
+    "vcl_create": (c_int, [c_int, ctypes.POINTER(c_void_p)]),
+    "vcl_destroy": (None, [P]),
+    "vcl_last_error": (c_char_p, [P]),
+    "vcl_set_mode": (c_int, [P, c_int]),
+    "vcl_get_mode": (c_int, [P]),
+    "vcl_set_raster_config": (c_int, [P, c_int, c_ll]),
+    "vcl_get_raster_config": (c_int, [P, ctypes.POINTER(c_int), ctypes.POINTER(c_ll)]),
+    "vcl_raster_overflow_count": (c_int, [P, P, ctypes.POINTER(c_ll)]),
+    "vcl_check_indices": (c_int, [P, P, ctypes.POINTER(c_int)]),
+    "vcl_reserve_raster": (c_int, [P, c_int, c_int, c_int, c_int]),
+    "vcl_tex_levels": (c_int, [c_int, c_int, c_int]),
+    "vcl_tex_level_offset": (c_size, [c_int, c_int, c_int, c_int]),
+    "vcl_project_fwd": (c_int, [P, P, c_int, P, c_int, c_int, P, P]),
+    "vcl_project_bwd": (c_int, [P, P, c_int, P, c_int, c_int, P, P]),
+    "vcl_rasterize_fwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
+    "vcl_rasterize_bwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
+    "vcl_interpolate_fwd": (c_int, [P, P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P]),
+    "vcl_interpolate_bwd": (c_int, [P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P, P]),
+    "vcl_texture_fwd": (c_int, [P, P, P, P, c_int, c_int, c_int, P, c_int, c_int, c_int, c_int, P, P]),
+    "vcl_texture_bwd": (c_int, [P, P, P, P, c_int, c_int, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P, P]),
+    "vcl_texture_build_mips": (c_int, [P, P, c_int, c_int, c_int, c_int, P]),
+    "vcl_texture_grad_pushdown": (c_int, [P, P, c_int, c_int, c_int, c_int, P]),
+    "vcl_clamp": (c_int, [P, P, c_size, c_float, c_float, P]),
+    "vcl_antialias_fwd": (c_int, [P, P, c_int, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
+    "vcl_antialias_bwd": (c_int, [P, P, c_int, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P, P]),
+    "vcl_normal_axis_fwd": (c_int, [P, P, c_int, c_int, c_int, P, P, c_int, P, c_int, P, P]),
+    "vcl_view_axis_fwd": (c_int, [P, c_int, c_int, c_int, P, P, P]),
+    "vcl_sg_specular_fwd": (c_int, [P, P, c_int, c_int, c_int, P, P, P, c_float, P, P, P, P]),
+    "vcl_sg_specular_bwd": (c_int, [P, P, c_int, c_int, c_int, P, P, P, c_float, P, P, P, P]),
+    "vcl_sg_fwd": (c_int, [P, P, c_int, c_int, c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, P, P, P]),
+    "vcl_sg_bwd": (c_int, [P, P, c_int, c_int, c_int, c_int, c_int, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
+                           P]),
+    "vcl_mse": (c_int, [P, P, P, c_size, P, P, P]),
+    "vcl_adam_step": (c_int, [P, P, P, P, P, c_size, c_double, c_double, c_double, c_double, c_int, P]),
+    "vcl_fit_create": (c_int, [P, P, ctypes.POINTER(c_void_p)]),
+    "vcl_fit_destroy": (None, [P]),
+    "vcl_fit_set_strategy": (c_int, [P, c_int]),
+    "vcl_fit_set_target": (c_int, [P, P, c_int, P]),
+    "vcl_fit_set_cameras": (c_int, [P, P, P, P]),
+    "vcl_fit_step": (c_int, [P, P]),
+    "vcl_fit_render": (c_int, [P, P, P]),
+    "vcl_fit_loss_device": (c_void_p, [P]),
+    "vcl_fit_read_loss": (c_int, [P, P, P]),
+    "vcl_fit_read_params": (c_int, [P, P, P, P, P, P, P]),
+    "vcl_fit_footprint": (c_size, [P]),
+    "vcl_fit_launches_per_step": (c_int, [P]),
+}
+
+FIT_PLAIN = 0
+FIT_FUSED = 1
+
+
+class FitDesc(ctypes.Structure):
+    """vcl_fit_desc of include/vcl.h."""
+    _fields_ = [("W", c_int), ("H", c_int), ("views", c_int), ("C", c_int), ("K", c_int), ("nv", c_int),
+                ("nt", c_int), ("tex_w", c_int), ("tex_h", c_int), ("levels", c_int),
+                ("pos", c_void_p), ("tri", c_void_p), ("uv", c_void_p), ("normal", c_void_p), ("tex", c_void_p),
+                ("lobe_axis", c_void_p), ("lobe_sharp", c_void_p), ("lobe_amp", c_void_p), ("mvp", c_void_p),
+                ("pvinv", c_void_p), ("rot", c_void_p), ("roughness", c_float), ("ior", c_float),
+                ("lr", c_double), ("beta1", c_double), ("beta2", c_double), ("eps", c_double),
+                ("learn_pos", c_int), ("learn_tex", c_int), ("learn_lobes", c_int)]
+
+
+class VclError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load libvcl.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise VclError(f"{LIB_PATH} is missing: build it with `python -m vcl_b200.build` (nvcc, sm_100a)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return list(SIGNATURES)
+
+
+def _addr(x):
+    """Device address of a torch tensor / int / None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+class Context:
+    """Owns one vcl_ctx.  Methods mirror the C functions without the ``vcl_``
+    prefix; tensor arguments may be torch CUDA tensors or raw addresses."""
+
+    def __init__(self, device=0, mode=MODE_COMPAT):
+        self.lib = lib()
+        h = c_void_p()
+        st = self.lib.vcl_create(device, ctypes.byref(h))
+        if st != 0:
+            raise VclError(f"vcl_create(device={device}) failed with status {st}")
+        self.h = h
+        self.device = device
+        self.set_mode(mode)
+
+    def close(self):
+        if self.h:
+            self.lib.vcl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, name):
+        if st != 0:
+            msg = self.lib.vcl_last_error(self.h)
+            raise VclError(f"{name} failed (status {st}): {msg.decode() if msg else ''}")
+
+    def set_mode(self, mode):
+        self._check(self.lib.vcl_set_mode(self.h, mode), "vcl_set_mode")
+
+    def set_raster_config(self, tile, bin_capacity=0):
+        self._check(self.lib.vcl_set_raster_config(self.h, tile, bin_capacity), "vcl_set_raster_config")
+
+    def raster_overflow_count(self, stream=None):
+        c = c_ll()
+        self._check(self.lib.vcl_raster_overflow_count(self.h, stream, ctypes.byref(c)), "vcl_raster_overflow_count")
+        return c.value
+
+    def check_indices(self, stream=None):
+        c = c_int()
+        self._check(self.lib.vcl_check_indices(self.h, stream, ctypes.byref(c)), "vcl_check_indices")
+        return c.value
+
+    def call(self, name, *args):
+        fn = getattr(self.lib, "vcl_" + name)
+        conv = []
+        for a, t in zip(args, fn.argtypes[1:]):
+            conv.append(_addr(a) if t is P else a)
+        self._check(fn(self.h, *conv), "vcl_" + name)
+
+    def __getattr__(self, name):
+        if name.startswith("_") or "vcl_" + name not in SIGNATURES:
+            raise AttributeError(name)
+        return lambda *a: self.call(name, *a)
+
+
+class Fit:
+    """A resident fit job (vcl_fit_*).  `scene` is a vcl_b200.scenes.Scene;
+    its host arrays are uploaded at creation."""
+
+    def __init__(self, ctx, scene, tex=None, pos=None, lobes=None, learn=(1, 1, 1), strategy=FIT_PLAIN):
+        import numpy as np
+        self.ctx = ctx
+        self.scene = S = scene
+        tex = S.tex_init if tex is None else tex
+        pos = S.pos if pos is None else pos
+        axis, sharp, amp = lobes if lobes is not None else (S.lobe_axis_init, S.lobe_sharp_init, S.lobe_amp_init)
+        keep = [np.ascontiguousarray(a, dtype=dt) for a, dt in (
+            (pos, np.float32), (S.tri, np.uint32), (S.uv, np.float32), (S.normal, np.float32), (tex, np.float32),
+            (axis, np.float32), (sharp, np.float32), (amp, np.float32), (S.mvp, np.float32), (S.pvinv, np.float32),
+            (S.rot, np.float32))]
+        d = FitDesc()
+        d.W, d.H, d.views, d.C, d.K = S.W, S.H, S.views, S.C, S.K
+        d.nv, d.nt, d.tex_w, d.tex_h, d.levels = S.nv, S.nt, S.tex_w, S.tex_h, S.levels
+        (d.pos, d.tri, d.uv, d.normal, d.tex, d.lobe_axis, d.lobe_sharp, d.lobe_amp, d.mvp, d.pvinv,
+         d.rot) = [a.ctypes.data for a in keep]
+        d.roughness, d.ior = S.roughness, S.ior
+        d.lr, d.beta1, d.beta2, d.eps = S.lr, 0.9, 0.999, 1e-8
+        d.learn_pos, d.learn_tex, d.learn_lobes = learn
+        self.desc = d
+        h = c_void_p()
+        ctx._check(ctx.lib.vcl_fit_create(ctx.h, ctypes.byref(d), ctypes.byref(h)), "vcl_fit_create")
+        self.h = h
+        self.set_strategy(strategy)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.vcl_fit_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, st, name):
+        self.ctx._check(st, name)
+
+    def set_strategy(self, s):
+        self._c(self.ctx.lib.vcl_fit_set_strategy(self.h, s), "vcl_fit_set_strategy")
+
+    def set_target(self, src, stream=None, is_device=None):
+        if is_device is None:
+            is_device = not hasattr(src, "ctypes")
+        addr = src.ctypes.data if hasattr(src, "ctypes") else _addr(src)
+        self._c(self.ctx.lib.vcl_fit_set_target(self.h, addr, int(is_device), stream), "vcl_fit_set_target")
+
+    def set_cameras(self, mvp, pvinv, stream=None):
+        self._c(self.ctx.lib.vcl_fit_set_cameras(self.h, mvp.ctypes.data, pvinv.ctypes.data, stream),
+                "vcl_fit_set_cameras")
+
+    def step(self, stream=None):
+        self._c(self.ctx.lib.vcl_fit_step(self.h, stream), "vcl_fit_step")
+
+    def render(self, out, stream=None):
+        self._c(self.ctx.lib.vcl_fit_render(self.h, _addr(out), stream), "vcl_fit_render")
+
+    def read_loss(self, stream=None):
+        out = ctypes.c_float()
+        self._c(self.ctx.lib.vcl_fit_read_loss(self.h, ctypes.byref(out), stream), "vcl_fit_read_loss")
+        return out.value
+
+    def loss_address(self):
+        return self.ctx.lib.vcl_fit_loss_device(self.h)
+
+    def launches_per_step(self):
+        return self.ctx.lib.vcl_fit_launches_per_step(self.h)
+
+    def read_params(self, stream=None):
+        import numpy as np
+        S = self.scene
+        pos = np.zeros((S.nv, 3), np.float32)
+        tex = np.zeros((S.tex_h, S.tex_w, S.C), np.float32)
+        ax = np.zeros((S.K, 3), np.float32); sh = np.zeros(S.K, np.float32); am = np.zeros((S.K, S.C), np.float32)
+        self._c(self.ctx.lib.vcl_fit_read_params(self.h, pos.ctypes.data, tex.ctypes.data, ax.ctypes.data,
+                                                 sh.ctypes.data, am.ctypes.data, stream), "vcl_fit_read_params")
+        return pos, tex, (ax, sh, am)

@@ -1,0 +1,76 @@
+// Shared device helpers and the context object of the vcl C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <cstdio>
+#include <cstdarg>
+#include "../../include/vcl.h"
+
+struct vcl_ctx {
+    int device = 0;
+    int mode = VCL_MODE_COMPAT;
+    int sm_count = 148;
+    std::string err;
+    // raster binning schedule
+    int tile = 16;
+    long long bin_capacity = 0;   // 0 = automatic
+    // raster workspace (grown on demand, owned here)
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    int* dev_flags = nullptr;     // [0] = overflowed tiles of the last raster call
+};
+
+vcl_status vcl_fail(vcl_ctx* ctx, vcl_status code, const char* fmt, ...);
+vcl_status vcl_cuda_check(vcl_ctx* ctx, cudaError_t e, const char* what);
+vcl_status vcl_launch_check(vcl_ctx* ctx, const char* what);
+// Grows the context workspace to at least `bytes` (synchronizes the device
+// when it has to reallocate).
+vcl_status vcl_ws_reserve(vcl_ctx* ctx, size_t bytes);
+
+#define VCL_REQUIRE(cond, ...) \
+    do { if (!(cond)) return vcl_fail(ctx, VCL_ERR_ARG, __VA_ARGS__); } while (0)
+#define VCL_CTX_CHECK() \
+    do { if (!ctx) return VCL_ERR_ARG; } while (0)
+
+static inline unsigned vcl_blocks(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+#define DEV __device__ __forceinline__
+
+// common.h:181-182 (AddNaNcheck), for values owned by one thread.
+DEV void add_nan_check(float& a, float b) {
+    if (!isfinite(a)) a = 0.f;
+    else { float v = a + b; if (isfinite(v)) a = v; }
+}
+DEV void add_nan_check3(float* a, float bx, float by, float bz) {
+    if (!(isfinite(a[0]) && isfinite(a[1]) && isfinite(a[2]))) { a[0] = a[1] = a[2] = 0.f; }
+    else {
+        float x = a[0] + bx, y = a[1] + by, z = a[2] + bz;
+        if (isfinite(x) && isfinite(y) && isfinite(z)) { a[0] = x; a[1] = y; a[2] = z; }
+    }
+}
+
+DEV float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+DEV float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+DEV float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+DEV float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+DEV float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+DEV float len3(float3 a) { return sqrtf(dot3(a, a)); }
+DEV float3 normalize3(float3 v) { float d = 1.f / len3(v); return f3(v.x * d, v.y * d, v.z * d); }
+DEV float3 ld3(const float* p, size_t i) { return f3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+DEV void st3(float* p, size_t i, float3 v) { p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z; }
+DEV float lerpf_(float a, float b, float t) { return a + t * (b - a); }
+
+// sm_90+ vector reduction: one red.global.add.v4.f32 instead of four.
+DEV void red_add4(float* p, float a, float b, float c, float d) {
+    atomicAdd(reinterpret_cast<float4*>(p), make_float4(a, b, c, d));
+}
+DEV void red_add2(float* p, float a, float b) {
+    atomicAdd(reinterpret_cast<float2*>(p), make_float2(a, b));
+}
+
+// Triangle id of a raster texel (u, v, z/w, id+1); -1 for background.
+DEV int rast_id(float w) { return (int)w - 1; }

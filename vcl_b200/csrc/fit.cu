@@ -1,0 +1,253 @@
+// Fit jobs: the reference's PresetPrimitives iteration (preset_primitives.cpp
+// :160-230) as a resident device object.  All parameters, Adam moments,
+// gradients and per-view buffers live in one device arena allocated at
+// creation; a step allocates nothing and only enqueues work on the caller's
+// stream, so it can be captured in a CUDA graph.
+#include "common.cuh"
+#include "fit.cuh"
+#include <vector>
+#include <cstring>
+
+namespace {
+
+size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct Layout {
+    size_t total = 0;
+    size_t add(size_t bytes) { size_t o = total; total += al(bytes ? bytes : 1); return o; }
+};
+
+}  // namespace
+
+// Buffer offsets inside the arena, shared by create() and footprint().
+static void plan(const vcl_fit_desc& d, vcl_fit* f, Layout& L) {
+    const size_t N = (size_t)d.W * d.H * d.views;
+    const size_t F = sizeof(float);
+    const size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, d.C, d.levels);
+    const size_t n0 = (size_t)d.tex_w * d.tex_h * d.C;
+    size_t o[64];
+    int i = 0;
+    o[i++] = L.add(F * d.nv * 3);             // pos
+    o[i++] = L.add(sizeof(uint32_t) * d.nt * 3);
+    o[i++] = L.add(F * d.nv * 2);             // uv attr
+    o[i++] = L.add(F * d.nv * 3);             // normal attr
+    o[i++] = L.add(F * npyr);                 // pyramid
+    o[i++] = L.add(F * d.K * (4 + d.C));      // lobes: axis [K][3] | sharpness [K] | amplitude [K][C]
+    o[i++] = L.add(F * d.views * 16);         // mvp
+    o[i++] = L.add(F * d.views * 9);          // pvinv
+    o[i++] = L.add(F * 16);                   // rot
+    o[i++] = L.add(F * d.views * d.nv * 4);   // clip
+    o[i++] = L.add(F * N * 4);                // rast
+    o[i++] = L.add(F * N * 4);                // db
+    o[i++] = L.add(F * N * 2);                // uv
+    o[i++] = L.add(F * N * 4);                // uv_da
+    o[i++] = L.add(F * N * d.C);              // diffuse
+    o[i++] = L.add(F * N * 3);                // normal
+    o[i++] = L.add(F * N * 3);                // view
+    o[i++] = L.add(F * N);                    // rough
+    o[i++] = L.add(F * N * 3);                // spec axis
+    o[i++] = L.add(F * N);                    // spec sharp
+    o[i++] = L.add(F * N);                    // spec amp
+    o[i++] = L.add(F * N * d.C);              // color
+    o[i++] = L.add(F * N * d.C);              // aa
+    o[i++] = L.add(F * N * d.C);              // target
+    o[i++] = L.add(F * N * d.C);              // g_aa
+    o[i++] = L.add(F * N * d.C);              // g_color
+    o[i++] = L.add(F * N * d.C);              // g_diffuse
+    o[i++] = L.add(F * N * 2);                // g_uv
+    o[i++] = L.add(F * N * 2);                // g_bary
+    o[i++] = L.add(F * d.views * d.nv * 4);   // g_clip
+    o[i++] = L.add(F * npyr);                 // g_pyr
+    o[i++] = L.add(F * d.nv * 3);             // g_pos
+    o[i++] = L.add(F * d.K * (4 + d.C));      // lobe gradients, same layout
+    o[i++] = L.add(F * n0 * 2);               // adam m,v texture
+    o[i++] = L.add(F * d.nv * 3 * 2);         // adam m,v pos
+    o[i++] = L.add(F * d.K * (4 + d.C) * 2);  // adam m,v lobes (axis|sharp|amp)
+    o[i++] = L.add(F * 4);                    // loss
+    if (f) {
+        char* b = (char*)f->arena;
+        int j = 0;
+        f->pos = (float*)(b + o[j++]); f->tri = (uint32_t*)(b + o[j++]); f->uvattr = (float*)(b + o[j++]);
+        f->nrmattr = (float*)(b + o[j++]); f->pyr = (float*)(b + o[j++]); f->lobe = (float*)(b + o[j++]);
+        f->mvp = (float*)(b + o[j++]);
+        f->pvinv = (float*)(b + o[j++]); f->rot = (float*)(b + o[j++]); f->clip = (float*)(b + o[j++]);
+        f->rast = (float*)(b + o[j++]); f->db = (float*)(b + o[j++]); f->uv = (float*)(b + o[j++]);
+        f->uv_da = (float*)(b + o[j++]); f->diffuse = (float*)(b + o[j++]); f->normal = (float*)(b + o[j++]);
+        f->view = (float*)(b + o[j++]); f->rough = (float*)(b + o[j++]); f->sax = (float*)(b + o[j++]);
+        f->ssh = (float*)(b + o[j++]); f->sam = (float*)(b + o[j++]); f->color = (float*)(b + o[j++]);
+        f->aa = (float*)(b + o[j++]); f->target = (float*)(b + o[j++]); f->g_aa = (float*)(b + o[j++]);
+        f->g_color = (float*)(b + o[j++]); f->g_diffuse = (float*)(b + o[j++]); f->g_uv = (float*)(b + o[j++]);
+        f->g_bary = (float*)(b + o[j++]); f->g_clip = (float*)(b + o[j++]); f->g_pyr = (float*)(b + o[j++]);
+        f->g_pos = (float*)(b + o[j++]); f->g_lobe = (float*)(b + o[j++]);
+        f->mv_tex = (float*)(b + o[j++]); f->mv_pos = (float*)(b + o[j++]); f->mv_lobe = (float*)(b + o[j++]);
+        f->loss = (float*)(b + o[j++]);
+        f->axis = f->lobe; f->sharp = f->lobe + 3 * d.K; f->amp = f->lobe + 4 * d.K;
+        f->g_axis = f->g_lobe; f->g_sharp = f->g_lobe + 3 * d.K; f->g_amp = f->g_lobe + 4 * d.K;
+    }
+}
+
+static vcl_status validate(vcl_ctx* ctx, const vcl_fit_desc* d) {
+    VCL_REQUIRE(d, "null descriptor");
+    VCL_REQUIRE(d->W > 0 && d->H > 0 && d->views > 0 && d->nv > 0 && d->nt > 0, "bad fit sizes");
+    VCL_REQUIRE(d->C >= 1 && d->C <= 8 && d->K >= 0 && d->K <= 1024, "bad channel/lobe counts");
+    VCL_REQUIRE(d->tex_w > 0 && d->tex_h > 0 && d->levels >= 1 && d->levels == vcl_tex_levels(d->tex_w, d->tex_h, d->levels),
+                "bad texture size/levels");
+    VCL_REQUIRE(d->pos && d->tri && d->uv && d->normal && d->tex && d->mvp && d->pvinv && d->rot, "null host array");
+    VCL_REQUIRE(d->K == 0 || (d->lobe_axis && d->lobe_sharp && d->lobe_amp), "null lobe array");
+    return VCL_OK;
+}
+
+extern "C" {
+
+VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc) {
+    if (!desc) return 0;
+    Layout L;
+    plan(*desc, nullptr, L);
+    return L.total;
+}
+
+VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fit** out) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(out, "null output");
+    *out = nullptr;
+    vcl_status st = validate(ctx, desc);
+    if (st) return st;
+    vcl_fit* f = new vcl_fit();
+    f->ctx = ctx;
+    f->d = *desc;
+    Layout L;
+    plan(f->d, nullptr, L);
+    cudaError_t e = cudaMalloc(&f->arena, L.total);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete f;
+        return vcl_fail(ctx, VCL_ERR_NOMEM, "fit arena of %zu bytes: %s", L.total, cudaGetErrorString(e));
+    }
+    f->arena_bytes = L.total;
+    plan(f->d, f, L);
+    const vcl_fit_desc& d = f->d;
+    const size_t N = (size_t)d.W * d.H * d.views;
+    const size_t n0 = (size_t)d.tex_w * d.tex_h * d.C;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "fit upload");
+    };
+    st = vcl_cuda_check(ctx, cudaMemset(f->arena, 0, L.total), "fit clear");
+    up(f->pos, d.pos, sizeof(float) * d.nv * 3);
+    up(f->tri, d.tri, sizeof(uint32_t) * d.nt * 3);
+    up(f->uvattr, d.uv, sizeof(float) * d.nv * 2);
+    up(f->nrmattr, d.normal, sizeof(float) * d.nv * 3);
+    up(f->pyr, d.tex, sizeof(float) * n0);
+    if (d.K) {
+        up(f->axis, d.lobe_axis, sizeof(float) * d.K * 3);
+        up(f->sharp, d.lobe_sharp, sizeof(float) * d.K);
+        up(f->amp, d.lobe_amp, sizeof(float) * d.K * d.C);
+    }
+    up(f->mvp, d.mvp, sizeof(float) * d.views * 16);
+    up(f->pvinv, d.pvinv, sizeof(float) * d.views * 9);
+    up(f->rot, d.rot, sizeof(float) * 16);
+    if (st == VCL_OK) {
+        std::vector<float> r(N, d.roughness);
+        up(f->rough, r.data(), sizeof(float) * N);
+    }
+    if (st == VCL_OK) st = vcl_texture_build_mips(ctx, f->pyr, d.tex_w, d.tex_h, d.C, d.levels, nullptr);
+    if (st == VCL_OK) st = vcl_reserve_raster(ctx, d.W, d.H, d.views, d.nt);
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaDeviceSynchronize(), "fit create");
+    if (st) {
+        vcl_fit_destroy(f);
+        return st;
+    }
+    // host pointers are not kept
+    f->d.pos = nullptr; f->d.tri = nullptr; f->d.uv = nullptr; f->d.normal = nullptr; f->d.tex = nullptr;
+    f->d.lobe_axis = nullptr; f->d.lobe_sharp = nullptr; f->d.lobe_amp = nullptr;
+    f->d.mvp = nullptr; f->d.pvinv = nullptr; f->d.rot = nullptr;
+    *out = f;
+    return VCL_OK;
+}
+
+VCL_API void vcl_fit_destroy(vcl_fit* f) {
+    if (!f) return;
+    if (f->arena) cudaFree(f->arena);
+    fit_fused_release(f);
+    delete f;
+}
+
+VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* f, int strategy) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(strategy == VCL_FIT_PLAIN || strategy == VCL_FIT_FUSED, "unknown strategy %d", strategy);
+    f->strategy = strategy;
+    return VCL_OK;
+}
+
+VCL_API vcl_status vcl_fit_set_target(vcl_fit* f, const float* src, int src_is_device, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(src, "null target");
+    size_t bytes = sizeof(float) * (size_t)f->d.W * f->d.H * f->d.views * f->d.C;
+    return vcl_cuda_check(ctx, cudaMemcpyAsync(f->target, src, bytes, src_is_device ? cudaMemcpyDeviceToDevice
+                                                                                        : cudaMemcpyHostToDevice,
+                                               (cudaStream_t)stream), "fit target copy");
+}
+
+VCL_API vcl_status vcl_fit_set_cameras(vcl_fit* f, const float* mvp, const float* pvinv, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(mvp && pvinv, "null camera arrays");
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->mvp, mvp, sizeof(float) * 16 * f->d.views,
+                                                        cudaMemcpyHostToDevice, s), "camera copy");
+    if (st) return st;
+    return vcl_cuda_check(ctx, cudaMemcpyAsync(f->pvinv, pvinv, sizeof(float) * 9 * f->d.views, cudaMemcpyHostToDevice, s),
+                          "camera copy");
+}
+
+VCL_API const float* vcl_fit_loss_device(const vcl_fit* f) { return f ? f->loss : nullptr; }
+
+VCL_API vcl_status vcl_fit_read_loss(vcl_fit* f, float* loss_host, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(loss_host, "null loss output");
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(loss_host, f->loss, sizeof(float), cudaMemcpyDeviceToHost, s),
+                                   "loss readback");
+    if (st) return st;
+    return vcl_cuda_check(ctx, cudaStreamSynchronize(s), "loss readback sync");
+}
+
+VCL_API vcl_status vcl_fit_read_params(vcl_fit* f, float* pos, float* tex0, float* axis, float* sharp, float* amp,
+                                       void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    cudaStream_t s = (cudaStream_t)stream;
+    const vcl_fit_desc& d = f->d;
+    vcl_status st = VCL_OK;
+    auto dn = [&](void* dst, const void* src, size_t bytes) {
+        if (dst && st == VCL_OK)
+            st = vcl_cuda_check(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "param readback");
+    };
+    dn(pos, f->pos, sizeof(float) * d.nv * 3);
+    dn(tex0, f->pyr, sizeof(float) * d.tex_w * d.tex_h * d.C);
+    dn(axis, f->axis, sizeof(float) * d.K * 3);
+    dn(sharp, f->sharp, sizeof(float) * d.K);
+    dn(amp, f->amp, sizeof(float) * d.K * d.C);
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "param readback sync");
+    return st;
+}
+
+VCL_API int vcl_fit_launches_per_step(const vcl_fit* f) {
+    if (!f) return 0;
+    return f->strategy == VCL_FIT_FUSED ? fit_fused_launches(f) : fit_plain_launches(f);
+}
+
+VCL_API vcl_status vcl_fit_render(vcl_fit* f, float* out, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    return fit_forward(f, out, (cudaStream_t)stream);
+}
+
+VCL_API vcl_status vcl_fit_step(vcl_fit* f, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    return f->strategy == VCL_FIT_FUSED ? fit_step_fused(f, s) : fit_step_plain(f, s);
+}
+
+}  // extern "C"

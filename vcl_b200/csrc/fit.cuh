@@ -1,0 +1,31 @@
+// Internal state of a fit job (see vcl_fit_* in include/vcl.h).
+#pragma once
+#include "common.cuh"
+
+struct vcl_fit {
+    vcl_ctx* ctx = nullptr;
+    vcl_fit_desc d{};
+    int strategy = VCL_FIT_PLAIN;
+    int step_count = 0;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    // parameters and constant attributes
+    float *pos, *uvattr, *nrmattr, *pyr, *lobe, *axis, *sharp, *amp, *mvp, *pvinv, *rot;
+    uint32_t* tri;
+    // per-view / per-pixel buffers
+    float *clip, *rast, *db, *uv, *uv_da, *diffuse, *normal, *view, *rough, *sax, *ssh, *sam, *color, *aa, *target;
+    // gradients
+    float *g_aa, *g_color, *g_diffuse, *g_uv, *g_bary, *g_clip, *g_pyr, *g_pos, *g_lobe, *g_axis, *g_sharp, *g_amp;
+    // Adam moments: [m | v] per group
+    float *mv_tex, *mv_pos, *mv_lobe;
+    float* loss;
+    // fused-strategy resources
+    void* fused = nullptr;
+};
+
+vcl_status fit_step_plain(vcl_fit* f, cudaStream_t s);
+vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s);
+vcl_status fit_forward(vcl_fit* f, float* out, cudaStream_t s);
+int fit_plain_launches(const vcl_fit* f);
+int fit_fused_launches(const vcl_fit* f);
+void fit_fused_release(vcl_fit* f);

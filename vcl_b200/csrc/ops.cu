@@ -1,0 +1,814 @@
+// Per-pixel / per-element operators of the vcl C ABI: project, interpolate,
+// texture (+ mip chain), antialias, loss and Adam.  One thread per pixel
+// (or vertex / texel / parameter) over a flat 1-D grid, reading and writing
+// the reference's interleaved layouts with vector loads where the channel
+// count allows.  Gradient scatters use FP32 vector reductions
+// (red.global.add.v4.f32 / .v2.f32, sm_90+).
+#include "common.cuh"
+
+namespace {
+
+DEV float mul(float a, float b) { return __fmul_rn(a, b); }
+DEV float add(float a, float b) { return __fadd_rn(a, b); }
+DEV float sub(float a, float b) { return __fsub_rn(a, b); }
+
+// ------------------------------------------------------------- project
+// project.cu:26-34
+__global__ void k_project_fwd(const float* __restrict__ mats, int views, const float* __restrict__ pos, int nv, int dim,
+                              float* __restrict__ out) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)views * nv) return;
+    int view = (int)(gid / nv), p = (int)(gid % nv);
+    const float* m = mats + (size_t)view * 16;
+    float x = pos[3 * (size_t)p], y = pos[3 * (size_t)p + 1], z = pos[3 * (size_t)p + 2];
+    float* o = out + (size_t)gid * dim;
+    for (int i = 0; i < dim; ++i) o[i] = m[i] * x + m[4 + i] * y + m[8 + i] * z + m[12 + i];
+}
+
+// project.cu:71-88; one thread per vertex sums its views (no atomics)
+__global__ void k_project_bwd(const float* __restrict__ mats, int views, const float* __restrict__ gout, int nv, int dim,
+                              float* __restrict__ gpos) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nv) return;
+    float gx = gpos[3 * (size_t)p], gy = gpos[3 * (size_t)p + 1], gz = gpos[3 * (size_t)p + 2];
+    for (int v = 0; v < views; ++v) {
+        const float* m = mats + (size_t)v * 16;
+        const float* g = gout + ((size_t)v * nv + p) * dim;
+        for (int i = 0; i < dim; ++i) {
+            float gi = g[i];
+            gx += m[i] * gi;
+            gy += m[4 + i] * gi;
+            gz += m[8 + i] * gi;
+        }
+    }
+    gpos[3 * (size_t)p] = gx; gpos[3 * (size_t)p + 1] = gy; gpos[3 * (size_t)p + 2] = gz;
+}
+
+// --------------------------------------------------------- interpolate
+DEV bool tri_ok(int idx, int nt, const uint32_t* tri, int nv, uint32_t& i0, uint32_t& i1, uint32_t& i2, int* flags) {
+    if (idx < 0) return false;
+    if (idx >= nt) { atomicOr(&flags[1], 1); return false; }
+    i0 = tri[3 * (size_t)idx]; i1 = tri[3 * (size_t)idx + 1]; i2 = tri[3 * (size_t)idx + 2];
+    if (i0 >= (uint32_t)nv || i1 >= (uint32_t)nv || i2 >= (uint32_t)nv) { atomicOr(&flags[1], 1); return false; }
+    return true;
+}
+
+// interpolate.cu:20-49 (+ the output clears of :51-60)
+__global__ void k_interp_fwd(const float4* __restrict__ rast, const float4* __restrict__ db, const float* __restrict__ attr,
+                             int nv, int dim, const uint32_t* __restrict__ tri, int nt, long long npix,
+                             float* __restrict__ out, float2* __restrict__ out_da, int* flags) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float4 r = rast[p];
+    uint32_t i0, i1, i2;
+    if (!tri_ok(rast_id(r.w), nt, tri, nv, i0, i1, i2, flags)) {
+        for (int i = 0; i < dim; ++i) out[p * dim + i] = 0.f;
+        if (out_da) for (int i = 0; i < dim; ++i) out_da[p * dim + i] = make_float2(0.f, 0.f);
+        return;
+    }
+    float4 d = out_da ? db[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
+    for (int i = 0; i < dim; ++i) {
+        float a0 = attr[(size_t)i0 * dim + i], a1 = attr[(size_t)i1 * dim + i], a2 = attr[(size_t)i2 * dim + i];
+        out[p * dim + i] = (float)__dadd_rn((double)add(mul(a0, r.x), mul(a1, r.y)), __dmul_rn((double)a2, l2));
+        if (out_da) {
+            float dadu = a0 - a2, dadv = a1 - a2;
+            out_da[p * dim + i] = make_float2(add(mul(dadu, d.x), mul(dadv, d.z)), add(mul(dadu, d.y), mul(dadv, d.w)));
+        }
+    }
+}
+
+// interpolate.cu:114-143
+__global__ void k_interp_bwd(const float4* __restrict__ rast, const float* __restrict__ attr, int nv, int dim,
+                             const uint32_t* __restrict__ tri, int nt, long long npix, const float* __restrict__ gout,
+                             float* __restrict__ gattr, float2* __restrict__ gbary, int accumulate, int* flags) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    float4 r = rast[p];
+    uint32_t i0, i1, i2;
+    if (!tri_ok(rast_id(r.w), nt, tri, nv, i0, i1, i2, flags)) return;
+    float gu = 0.f, gv = 0.f;
+    double l2 = (1.0 - (double)r.x) - (double)r.y;
+    const float* g = gout + p * dim;
+    if (gattr && dim == 2) {
+        float g0 = g[0], g1 = g[1];
+        red_add2(gattr + (size_t)i0 * 2, g0 * r.x, g1 * r.x);
+        red_add2(gattr + (size_t)i1 * 2, g0 * r.y, g1 * r.y);
+        red_add2(gattr + (size_t)i2 * 2, (float)((double)g0 * l2), (float)((double)g1 * l2));
+    } else if (gattr && dim == 4) {
+        float4 gg = make_float4(g[0], g[1], g[2], g[3]);
+        red_add4(gattr + (size_t)i0 * 4, gg.x * r.x, gg.y * r.x, gg.z * r.x, gg.w * r.x);
+        red_add4(gattr + (size_t)i1 * 4, gg.x * r.y, gg.y * r.y, gg.z * r.y, gg.w * r.y);
+        red_add4(gattr + (size_t)i2 * 4, (float)((double)gg.x * l2), (float)((double)gg.y * l2),
+                 (float)((double)gg.z * l2), (float)((double)gg.w * l2));
+    } else if (gattr) {
+        for (int i = 0; i < dim; ++i) {
+            float gi = g[i];
+            atomicAdd(&gattr[(size_t)i0 * dim + i], gi * r.x);
+            atomicAdd(&gattr[(size_t)i1 * dim + i], gi * r.y);
+            atomicAdd(&gattr[(size_t)i2 * dim + i], (float)((double)gi * l2));
+        }
+    }
+    for (int i = 0; i < dim; ++i) {
+        float gi = g[i];
+        float a2 = attr[(size_t)i2 * dim + i];
+        gu += gi * (attr[(size_t)i0 * dim + i] - a2);
+        gv += gi * (attr[(size_t)i1 * dim + i] - a2);
+    }
+    if (gbary) {
+        if (accumulate) { float2 o = gbary[p]; gbary[p] = make_float2(o.x + gu, o.y + gv); }
+        else gbary[p] = make_float2(gu, gv);
+    }
+}
+
+// -------------------------------------------------------------- texture
+struct TexDesc {
+    int tw, th, C, L;
+    long long off[16];
+};
+
+// texturemap.cu:22-47 (level) and :160-197 (level + Jacobian); the level
+// arithmetic is rounded exactly like the CPU restatement so that the same
+// mip levels are chosen.
+DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, float4* dl, int exact) {
+    float dsdx = mul(da.x, (float)t.tw), dsdy = mul(da.y, (float)t.tw);
+    float dtdx = mul(da.z, (float)t.th), dtdy = mul(da.w, (float)t.th);
+    float s2 = add(mul(dsdx, dsdx), mul(dsdy, dsdy));
+    float t2 = add(mul(dtdx, dtdx), mul(dtdy, dtdy));
+    float a = sub(mul(dsdx, dtdy), mul(dtdx, dsdy));
+    float b = mul(.5f, add(s2, t2));
+    float c2 = sub(mul(b, b), mul(a, a));
+    float c = sqrtf(c2);
+    float level = mul(.5f, log2f(add(b, c)));
+    const int L = t.L;
+    l0 = level <= 0 ? 0 : (float)(L - 2) <= level ? L - 2 : (int)floorf(level);
+    l1 = level <= 1 ? 1 : (float)(L - 1) <= level ? L - 1 : (int)floorf(level) + 1;
+    fl = level <= 0 ? 0.f : (float)(L - 1) <= level ? 1.f : level - floorf(level);
+    if (dl) {
+        float d = b * c + c2;
+        if ((double)fabsf(d) > 1e-6) {
+            d = 0.72134752f / d;
+            float bc = b + c;
+            *dl = make_float4(d * (bc * dsdx - a * dtdy), d * (bc * dsdy + a * dtdx), bc * dtdx + a * dsdy,
+                              bc * dtdy - a * dsdx);
+            if (exact) { dl->z *= d; dl->w *= d; }
+        } else if ((double)fabsf(b) > 1e-6) {
+            d = 1 / b;
+            *dl = make_float4(d * dsdx, d * dsdy, d * dtdx, d * dtdy);
+        } else {
+            *dl = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+}
+
+// texturemap.cu:49-65
+DEV void index_fetch(const TexDesc& t, int level, float2 uv, int idx[4], float2& f) {
+    int sx = t.tw >> level, sy = t.th >> level;
+    float tx = uv.x * (float)sx, ty = uv.y * (float)sy;
+    int u0 = tx < 0 ? 0 : tx > (float)(sx - 1) ? sx - 1 : (int)tx;
+    int u1 = tx < 1 ? 0 : tx > (float)(sx - 2) ? sx - 1 : (int)tx + 1;
+    int v0 = ty < 0 ? 0 : ty > (float)(sy - 1) ? sy - 1 : (int)ty;
+    int v1 = ty < 1 ? 0 : ty > (float)(sy - 2) ? sy - 1 : (int)ty + 1;
+    idx[0] = v0 * sx + u0; idx[1] = v0 * sx + u1; idx[2] = v1 * sx + u0; idx[3] = v1 * sx + u1;
+    f.x = tx < 0 ? 0.f : (float)sx < tx ? 1.f : tx - floorf(tx);
+    f.y = ty < 0 ? 0.f : (float)sy < ty ? 1.f : ty - floorf(ty);
+}
+
+DEV float4 ld4(const float* p, int i) { return reinterpret_cast<const float4*>(p)[i]; }
+DEV float4 bilerp4(float4 a, float4 b, float4 c, float4 d, float2 t) {
+    float4 r;
+    r.x = lerpf_(lerpf_(a.x, b.x, t.x), lerpf_(c.x, d.x, t.x), t.y);
+    r.y = lerpf_(lerpf_(a.y, b.y, t.x), lerpf_(c.y, d.y, t.x), t.y);
+    r.z = lerpf_(lerpf_(a.z, b.z, t.x), lerpf_(c.z, d.z, t.x), t.y);
+    r.w = lerpf_(lerpf_(a.w, b.w, t.x), lerpf_(c.w, d.w, t.x), t.y);
+    return r;
+}
+DEV float bilerp1(float a, float b, float c, float d, float2 t) { return lerpf_(lerpf_(a, b, t.x), lerpf_(c, d, t.x), t.y); }
+
+// texturemap.cu:67-114
+template <int C4>
+__global__ void k_tex_fwd(TexDesc t, const float* __restrict__ pyr, const float4* __restrict__ rast,
+                          const float2* __restrict__ uv, const float4* __restrict__ uv_da, long long npix,
+                          float* __restrict__ out) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    const int C = C4 ? 4 : t.C;
+    if (rast[p].w < 1.f) {
+        if (C4) reinterpret_cast<float4*>(out)[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        else for (int i = 0; i < C; ++i) out[p * C + i] = 0.f;
+        return;
+    }
+    float2 u = uv[p];
+    int l0 = 0, l1 = 0;
+    float fl = 0.f;
+    if (t.L > 1) calc_level(t, uv_da[p], l0, l1, fl, nullptr, 0);
+    int i0[4];
+    float2 f0;
+    index_fetch(t, l0, u, i0, f0);
+    const float* T0 = pyr + t.off[l0];
+    if (C4) {
+        float4 o = bilerp4(ld4(T0, i0[0]), ld4(T0, i0[1]), ld4(T0, i0[2]), ld4(T0, i0[3]), f0);
+        if (t.L > 1 && fl > 0) {
+            int i1[4];
+            float2 f1;
+            index_fetch(t, l1, u, i1, f1);
+            const float* T1 = pyr + t.off[l1];
+            float4 o1 = bilerp4(ld4(T1, i1[0]), ld4(T1, i1[1]), ld4(T1, i1[2]), ld4(T1, i1[3]), f1);
+            o = make_float4(lerpf_(o.x, o1.x, fl), lerpf_(o.y, o1.y, fl), lerpf_(o.z, o1.z, fl), lerpf_(o.w, o1.w, fl));
+        }
+        reinterpret_cast<float4*>(out)[p] = o;
+    } else {
+        int i1[4];
+        float2 f1;
+        bool tri = t.L > 1 && fl > 0;
+        if (tri) index_fetch(t, l1, u, i1, f1);
+        const float* T1 = pyr + t.off[l1];
+        for (int i = 0; i < C; ++i) {
+            float o = bilerp1(T0[i0[0] * C + i], T0[i0[1] * C + i], T0[i0[2] * C + i], T0[i0[3] * C + i], f0);
+            if (tri) o = lerpf_(o, bilerp1(T1[i1[0] * C + i], T1[i1[1] * C + i], T1[i1[2] * C + i], T1[i1[3] * C + i], f1), fl);
+            out[p * C + i] = o;
+        }
+    }
+}
+
+// texturemap.cu:229-319
+template <int C4>
+__global__ void k_tex_bwd(TexDesc t, const float* __restrict__ pyr, const float4* __restrict__ rast,
+                          const float2* __restrict__ uv, const float4* __restrict__ uv_da, long long npix,
+                          const float* __restrict__ gout, float* __restrict__ gpyr, float2* __restrict__ guv,
+                          float4* __restrict__ guv_da, int exact) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    if (rast[p].w < 1.f) return;
+    const int C = C4 ? 4 : t.C;
+    const bool mip = t.L > 1;
+    float2 u = uv[p];
+    int l0 = 0, l1 = 0;
+    float fl = 0.f;
+    float4 dl = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (mip) calc_level(t, uv_da[p], l0, l1, fl, &dl, exact);
+    int i0[4], i1[4];
+    float2 f0, f1 = make_float2(0.f, 0.f);
+    index_fetch(t, l0, u, i0, f0);
+    if (mip) index_fetch(t, l1, u, i1, f1);
+    const float* T0 = pyr + t.off[l0];
+    const float* T1 = pyr + t.off[l1];
+    float* G0 = gpyr ? gpyr + t.off[l0] : nullptr;
+    float* G1 = gpyr ? gpyr + t.off[l1] : nullptr;
+    const float s0x = (float)(t.tw >> l0), s0y = (float)(t.th >> l0);
+    const float s1x = (float)(t.tw >> l1), s1y = (float)(t.th >> l1);
+    const float wl0 = mip ? 1.f - fl : 1.f;
+    const bool tri = mip && fl > 0;
+    float w00 = wl0 * (1.f - f0.x) * (1.f - f0.y), w01 = wl0 * f0.x * (1.f - f0.y);
+    float w10 = wl0 * (1.f - f0.x) * f0.y, w11 = wl0 * f0.x * f0.y;
+    float v00 = fl * (1.f - f1.x) * (1.f - f1.y), v01 = fl * f1.x * (1.f - f1.y);
+    float v10 = fl * (1.f - f1.x) * f1.y, v11 = fl * f1.x * f1.y;
+    float gu = 0.f, gv = 0.f, gl = 0.f;
+    if (C4) {
+        float4 g = reinterpret_cast<const float4*>(gout)[p];
+        if (G0) {
+            red_add4(G0 + 4 * i0[0], w00 * g.x, w00 * g.y, w00 * g.z, w00 * g.w);
+            red_add4(G0 + 4 * i0[1], w01 * g.x, w01 * g.y, w01 * g.z, w01 * g.w);
+            red_add4(G0 + 4 * i0[2], w10 * g.x, w10 * g.y, w10 * g.z, w10 * g.w);
+            red_add4(G0 + 4 * i0[3], w11 * g.x, w11 * g.y, w11 * g.z, w11 * g.w);
+            if (tri) {
+                red_add4(G1 + 4 * i1[0], v00 * g.x, v00 * g.y, v00 * g.z, v00 * g.w);
+                red_add4(G1 + 4 * i1[1], v01 * g.x, v01 * g.y, v01 * g.z, v01 * g.w);
+                red_add4(G1 + 4 * i1[2], v10 * g.x, v10 * g.y, v10 * g.z, v10 * g.w);
+                red_add4(G1 + 4 * i1[3], v11 * g.x, v11 * g.y, v11 * g.z, v11 * g.w);
+            }
+        }
+        float4 a00 = ld4(T0, i0[0]), a01 = ld4(T0, i0[1]), a10 = ld4(T0, i0[2]), a11 = ld4(T0, i0[3]);
+        float ga[4] = {g.x, g.y, g.z, g.w};
+        float A00[4] = {a00.x, a00.y, a00.z, a00.w}, A01[4] = {a01.x, a01.y, a01.z, a01.w};
+        float A10[4] = {a10.x, a10.y, a10.z, a10.w}, A11[4] = {a11.x, a11.y, a11.z, a11.w};
+        float B00[4], B01[4], B10[4], B11[4];
+        if (tri) {
+            float4 b00 = ld4(T1, i1[0]), b01 = ld4(T1, i1[1]), b10 = ld4(T1, i1[2]), b11 = ld4(T1, i1[3]);
+            B00[0] = b00.x; B00[1] = b00.y; B00[2] = b00.z; B00[3] = b00.w;
+            B01[0] = b01.x; B01[1] = b01.y; B01[2] = b01.z; B01[3] = b01.w;
+            B10[0] = b10.x; B10[1] = b10.y; B10[2] = b10.z; B10[3] = b10.w;
+            B11[0] = b11.x; B11[1] = b11.y; B11[2] = b11.z; B11[3] = b11.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], f0.y) * s0x;
+            float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], f0.x) * s0y;
+            if (tri) {
+                float l = bilerp1(A00[i], A01[i], A10[i], A11[i], f0);
+                du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], f1.y) * s1x, fl);
+                dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], f1.x) * s1y, fl);
+                gl += (bilerp1(B00[i], B01[i], B10[i], B11[i], f1) - l) * ga[i];
+            }
+            gu += du * ga[i];
+            gv += dv * ga[i];
+        }
+    } else {
+        for (int i = 0; i < C; ++i) {
+            float g = gout[p * C + i];
+            if (G0) {
+                atomicAdd(&G0[i0[0] * C + i], w00 * g); atomicAdd(&G0[i0[1] * C + i], w01 * g);
+                atomicAdd(&G0[i0[2] * C + i], w10 * g); atomicAdd(&G0[i0[3] * C + i], w11 * g);
+                if (tri) {
+                    atomicAdd(&G1[i1[0] * C + i], v00 * g); atomicAdd(&G1[i1[1] * C + i], v01 * g);
+                    atomicAdd(&G1[i1[2] * C + i], v10 * g); atomicAdd(&G1[i1[3] * C + i], v11 * g);
+                }
+            }
+            float a00 = T0[i0[0] * C + i], a01 = T0[i0[1] * C + i], a10 = T0[i0[2] * C + i], a11 = T0[i0[3] * C + i];
+            float du = lerpf_(a01 - a00, a11 - a10, f0.y) * s0x;
+            float dv = lerpf_(a10 - a00, a11 - a01, f0.x) * s0y;
+            if (tri) {
+                float l = bilerp1(a00, a01, a10, a11, f0);
+                float b00 = T1[i1[0] * C + i], b01 = T1[i1[1] * C + i], b10 = T1[i1[2] * C + i], b11 = T1[i1[3] * C + i];
+                du = lerpf_(du, lerpf_(b01 - b00, b11 - b10, f1.y) * s1x, fl);
+                dv = lerpf_(dv, lerpf_(b10 - b00, b11 - b01, f1.x) * s1y, fl);
+                gl += (bilerp1(b00, b01, b10, b11, f1) - l) * g;
+            }
+            gu += du * g;
+            gv += dv * g;
+        }
+    }
+    if (guv) guv[p] = make_float2(gu, gv);
+    if (guv_da && mip) guv_da[p] = make_float4(gl * dl.x, gl * dl.y, gl * dl.z, gl * dl.w);
+}
+
+// buffer.cu:449-472
+__global__ void k_mip_down(const float* __restrict__ src, float* __restrict__ dst, int w, int h, int C) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)w * h) return;
+    int px = (int)(i % w), py = (int)(i / w);
+    int pw = w * 2;
+    size_t p00 = (size_t)(2 * px) + (size_t)pw * (2 * py), p01 = p00 + 1, p10 = p00 + pw, p11 = p10 + 1;
+    if (C == 4) {
+        float4 a = ld4(src, (int)p00), b = ld4(src, (int)p01), c = ld4(src, (int)p10), d = ld4(src, (int)p11);
+        reinterpret_cast<float4*>(dst)[i] = make_float4(add(add(add(a.x, b.x), c.x), d.x) * 0.25f,
+                                                        add(add(add(a.y, b.y), c.y), d.y) * 0.25f,
+                                                        add(add(add(a.z, b.z), c.z), d.z) * 0.25f,
+                                                        add(add(add(a.w, b.w), c.w), d.w) * 0.25f);
+    } else {
+        for (int k = 0; k < C; ++k)
+            dst[i * C + k] = add(add(add(src[p00 * C + k], src[p01 * C + k]), src[p10 * C + k]), src[p11 * C + k]) * 0.25f;
+    }
+}
+
+// buffer.cu:615-636
+__global__ void k_mip_push(const float* __restrict__ src, float* __restrict__ dst, int w, int h, int C, float weight) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)w * h * C) return;
+    int k = (int)(i % C);
+    long long t = i / C;
+    int px = (int)(t % w), py = (int)(t / w);
+    int pw = w * 2;
+    size_t p00 = (size_t)(2 * px) + (size_t)pw * (2 * py), p01 = p00 + 1, p10 = p00 + pw, p11 = p10 + 1;
+    float v = src[i] * weight;
+    add_nan_check(dst[p00 * C + k], v);
+    add_nan_check(dst[p01 * C + k], v);
+    add_nan_check(dst[p10 * C + k], v);
+    add_nan_check(dst[p11 * C + k], v);
+}
+
+__global__ void k_clamp(float* __restrict__ p, long long n, float lo, float hi) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a = p[i];
+    p[i] = a < lo ? lo : a > hi ? hi : a;
+}
+
+// ------------------------------------------------------------ antialias
+struct AATri { float2 v[3]; float iw[3]; uint32_t id[3]; };
+
+// antialias.cu:37-55 / :240-257.  Screen positions use exactly rounded
+// arithmetic so that the edge decisions match the CPU restatement.
+DEV bool aa_fetch(const float4* __restrict__ proj, int nv, const uint32_t* __restrict__ tri, int nt,
+                  const float4* __restrict__ rast, long long pidx, float2 s, float2 f, AATri& t, int* flags) {
+    uint32_t i[3];
+    if (!tri_ok(rast_id(rast[pidx].w), nt, tri, nv, i[0], i[1], i[2], flags)) return false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float4 c = proj[i[k]];
+        t.id[k] = i[k];
+        t.iw[k] = __fdiv_rn(1.f, c.w);
+        t.v[k] = make_float2(sub(mul(add(mul(c.x, t.iw[k]), 1.f), s.x), f.x), sub(mul(add(mul(c.y, t.iw[k]), 1.f), s.y), f.y));
+    }
+    return true;
+}
+
+DEV float cross_rn(float ax, float ay, float bx, float by) { return sub(mul(ax, by), mul(ay, bx)); }
+
+// Shared edge geometry of antialias.cu:17-27 / :196-206; false when the
+// pixel pair does not straddle this edge.
+DEV bool aa_edge(float2 pa, float2 pb, float2 o, float& a, float& alpha, float& ia, float2& e, float& n) {
+    a = cross_rn(pa.x, pa.y, pb.x, pb.y);
+    float oa = cross_rn(sub(pa.x, o.x), sub(pa.y, o.y), sub(pb.x, o.x), sub(pb.y, o.y));
+    if (mul(a, oa) > 0.f) return false;
+    e = make_float2(sub(pa.x, pb.x), sub(pa.y, pb.y));
+    n = mul(add(o.x, o.y), sub(o.x, o.y));
+    if (mul(mul(add(e.x, e.y), sub(e.x, e.y)), n) > 0.f) return false;
+    float so = add(o.x, o.y);
+    e.x = mul(e.x, so); e.y = mul(e.y, so);
+    float D = n > 0.f ? -e.y : e.x;
+    ia = (float)(1.0 / ((double)D + (D > 0 ? 1e-3 : -1e-3)));
+    alpha = sub(mul(a, ia), .5f);
+    return true;
+}
+
+template <int C4>
+__global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
+                         const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
+                         float* __restrict__ out, int* flags) {
+    long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pidx >= npix) return;
+    const int C = C4 ? 4 : Cr;
+    long long hw = (long long)W * H;
+    int view = (int)(pidx / hw);
+    int rem = (int)(pidx - view * hw);
+    int py = rem / W, px = rem - py * W;
+    const float4* proj = clip + (size_t)view * nv;
+    const float2 s = make_float2(W / 2.f, H / 2.f);
+    float4 tr = rast[pidx];
+    for (int dir = 0; dir < 2; ++dir) {
+        if (dir == 0 ? px == 0 : py == 0) continue;
+        long long oidx = dir == 0 ? pidx - 1 : pidx - W;
+        float4 to = rast[oidx];
+        if (to.w == tr.w) continue;
+        long long pp = (int)tr.w ? pidx : oidx;
+        long long op = (int)to.w ? pidx : oidx;
+        if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
+        float2 f, o;
+        if (dir == 0) { f = make_float2((float)px + (pp > op ? .5f : -.5f), (float)py + .5f); o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
+        else { f = make_float2((float)px + .5f, (float)py + (pp > op ? .5f : -.5f)); o = make_float2(0.f, pp > op ? -1.f : 1.f); }
+        AATri t;
+        if (!aa_fetch(proj, nv, tri, nt, rast, pp, s, f, t, flags)) continue;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float a, alpha, ia, n;
+            float2 e;
+            if (!aa_edge(t.v[k], t.v[(k + 1) % 3], o, a, alpha, ia, e, n)) continue;
+            long long tgt = alpha > 0 ? op : pp;
+            if (C4) {
+                float4 ip = reinterpret_cast<const float4*>(in)[pp], io = reinterpret_cast<const float4*>(in)[op];
+                red_add4(out + tgt * 4, alpha * (ip.x - io.x), alpha * (ip.y - io.y), alpha * (ip.z - io.z), alpha * (ip.w - io.w));
+            } else {
+                for (int i = 0; i < C; ++i) atomicAdd(&out[tgt * C + i], alpha * (in[pp * C + i] - in[op * C + i]));
+            }
+        }
+    }
+}
+
+template <int C4>
+__global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
+                         const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
+                         const float* __restrict__ gout, float* __restrict__ gin, float* __restrict__ gclip, int exact,
+                         int* flags) {
+    long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pidx >= npix) return;
+    const int C = C4 ? 4 : Cr;
+    long long hw = (long long)W * H;
+    int view = (int)(pidx / hw);
+    int rem = (int)(pidx - view * hw);
+    int py = rem / W, px = rem - py * W;
+    const float4* proj = clip + (size_t)view * nv;
+    float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
+    const float2 s = make_float2(W / 2.f, H / 2.f);
+    float4 tr = rast[pidx];
+    for (int dir = 0; dir < 2; ++dir) {
+        if (dir == 0 ? px == 0 : py == 0) continue;
+        long long oidx = dir == 0 ? pidx - 1 : pidx - W;
+        float4 to = rast[oidx];
+        if (to.w == tr.w) continue;
+        long long pp = (int)tr.w ? pidx : oidx;
+        // antialias.cu:279 uses the current pixel's id here (horizontal pairs)
+        long long op = (int)((dir == 0 && !exact) ? tr.w : to.w) ? pidx : oidx;
+        if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
+        float2 f, o;
+        if (dir == 0) { f = make_float2((float)px + (pp > op ? .5f : -.5f), (float)py + .5f); o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
+        else { f = make_float2((float)px + .5f, (float)py + (pp > op ? .5f : -.5f)); o = make_float2(0.f, pp > op ? -1.f : 1.f); }
+        AATri t;
+        if (!aa_fetch(proj, nv, tri, nt, rast, pp, s, f, t, flags)) continue;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float a, alpha, ia, n;
+            float2 e;
+            const int ka = k, kb = (k + 1) % 3;
+            if (!aa_edge(t.v[ka], t.v[kb], o, a, alpha, ia, e, n)) continue;
+            const long long src = alpha > 0 ? op : pp;
+            float d = 0.f;
+            if (C4) {
+                float4 g = reinterpret_cast<const float4*>(gout)[src];
+                float4 ip = reinterpret_cast<const float4*>(in)[pp], io = reinterpret_cast<const float4*>(in)[op];
+                red_add4(gin + pp * 4, alpha * g.x, alpha * g.y, alpha * g.z, alpha * g.w);
+                red_add4(gin + op * 4, -alpha * g.x, -alpha * g.y, -alpha * g.z, -alpha * g.w);
+                d = g.x * (ip.x - io.x) + g.y * (ip.y - io.y) + g.z * (ip.z - io.z) + g.w * (ip.w - io.w);
+            } else {
+                for (int i = 0; i < C; ++i) {
+                    float g = gout[src * C + i];
+                    atomicAdd(&gin[pp * C + i], alpha * g);
+                    atomicAdd(&gin[op * C + i], -alpha * g);
+                    d += g * (in[pp * C + i] - in[op * C + i]);
+                }
+            }
+            if (gv) {
+                float2 pa = t.v[ka], pb = t.v[kb];
+                d *= ia;
+                float2 da = make_float2(d * s.x * t.iw[ka], d * s.y * t.iw[ka]);
+                float2 dbv = make_float2(d * s.x * t.iw[kb], d * s.y * t.iw[kb]);
+                float r = (n > 0 ? e.x : -e.y) * ia;
+                if (n > 0) {
+                    da.x *= pb.y; da.y *= pb.y; da.y *= r;
+                    dbv.x *= -pa.y; dbv.y *= -pa.y; dbv.y *= r;
+                } else {
+                    da.x *= -pb.x; da.y *= -pb.x; da.x *= r;
+                    dbv.x *= pa.x; dbv.y *= pa.x; dbv.x *= r;
+                }
+                red_add4(gv + (size_t)t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * pa.x + da.y * pa.y));
+                red_add4(gv + (size_t)t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * pb.x + dbv.y * pb.y));
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------- loss
+__global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, long long n, float* __restrict__ grad,
+                      float* __restrict__ loss) {
+    __shared__ double part[32];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float g = pred[i] - tgt[i];
+        grad[i] = g;
+        acc += (double)g * (double)g;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) atomicAdd(loss, (float)(acc * 0.5));
+    }
+}
+
+// ----------------------------------------------------------------- adam
+// optimize.cu:95-106: moments rounded to FP32, update in FP64, NaN-guarded.
+DEV void adam_one(float& p, float g, float& m, float& v, double b1, double b2, double lr, double eps, double c1,
+                  double c2) {
+    m = (float)__dadd_rn(__dmul_rn(b1, (double)m), __dmul_rn(1.0 - b1, (double)g));
+    v = (float)__dadd_rn(__dmul_rn(b2, (double)v), __dmul_rn(__dmul_rn(1.0 - b2, (double)g), (double)g));
+    double mh = (double)m / c1;
+    double vh = (double)v / c2;
+    add_nan_check(p, (float)(-mh * lr / (sqrt(vh) + eps)));
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       long long n, double b1, double b2, double lr, double eps, double c1, double c2, int vec) {
+    long long n4 = vec ? n / 4 : 0;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        float4 P = reinterpret_cast<float4*>(p)[i], G = reinterpret_cast<const float4*>(g)[i];
+        float4 M = reinterpret_cast<float4*>(m)[i], V = reinterpret_cast<float4*>(v)[i];
+        adam_one(P.x, G.x, M.x, V.x, b1, b2, lr, eps, c1, c2);
+        adam_one(P.y, G.y, M.y, V.y, b1, b2, lr, eps, c1, c2);
+        adam_one(P.z, G.z, M.z, V.z, b1, b2, lr, eps, c1, c2);
+        adam_one(P.w, G.w, M.w, V.w, b1, b2, lr, eps, c1, c2);
+        reinterpret_cast<float4*>(p)[i] = P; reinterpret_cast<float4*>(m)[i] = M; reinterpret_cast<float4*>(v)[i] = V;
+    }
+    for (long long i = n4 * 4 + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        adam_one(p[i], g[i], m[i], v[i], b1, b2, lr, eps, c1, c2);
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+TexDesc make_desc(int tw, int th, int C, int L) {
+    TexDesc d;
+    d.tw = tw; d.th = th; d.C = C; d.L = L;
+    long long off = 0;
+    for (int l = 0; l < 16; ++l) {
+        d.off[l] = off;
+        if (l < L) off += (long long)(tw >> l) * (th >> l) * C;
+    }
+    return d;
+}
+
+int grid_for(long long n, int threads, int sm) {
+    long long b = (n + threads - 1) / threads;
+    long long cap = (long long)sm * 8;
+    return (int)(b < 1 ? 1 : b > cap ? cap : b);
+}
+
+}  // namespace
+
+extern "C" {
+
+VCL_API vcl_status vcl_check_indices(vcl_ctx* ctx, void* stream, int* bad) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(bad, "bad is null");
+    cudaStream_t s = (cudaStream_t)stream;
+    int h = 0;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(&h, ctx->dev_flags + 1, sizeof(int), cudaMemcpyDeviceToHost, s),
+                                   "index flag readback");
+    if (!st) st = vcl_cuda_check(ctx, cudaMemsetAsync(ctx->dev_flags + 1, 0, sizeof(int), s), "index flag clear");
+    if (!st) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "index flag sync");
+    *bad = h;
+    return st;
+}
+
+VCL_API vcl_status vcl_project_fwd(vcl_ctx* ctx, const float* mats, int views, const float* pos, int nv, int dim,
+                                   float* out, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(mats && pos && out && views > 0 && nv >= 0 && (dim == 3 || dim == 4), "bad project_fwd arguments");
+    long long n = (long long)views * nv;
+    if (n == 0) return VCL_OK;
+    k_project_fwd<<<vcl_blocks(n, 256), 256, 0, (cudaStream_t)stream>>>(mats, views, pos, nv, dim, out);
+    return vcl_launch_check(ctx, "project_fwd");
+}
+
+VCL_API vcl_status vcl_project_bwd(vcl_ctx* ctx, const float* mats, int views, const float* grad_out, int nv, int dim,
+                                   float* grad_pos, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(mats && grad_out && grad_pos && views > 0 && nv >= 0 && (dim == 3 || dim == 4), "bad project_bwd arguments");
+    if (nv == 0) return VCL_OK;
+    k_project_bwd<<<vcl_blocks(nv, 256), 256, 0, (cudaStream_t)stream>>>(mats, views, grad_out, nv, dim, grad_pos);
+    return vcl_launch_check(ctx, "project_bwd");
+}
+
+VCL_API vcl_status vcl_interpolate_fwd(vcl_ctx* ctx, const float* rast, const float* db, int W, int H, int views,
+                                       const float* attr, int nv, int dim, const uint32_t* tri, int nt, float* out,
+                                       float* out_da, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(rast && attr && tri && out && W > 0 && H > 0 && views > 0 && dim > 0, "bad interpolate_fwd arguments");
+    VCL_REQUIRE(!out_da || db, "out_da needs db");
+    VCL_REQUIRE(aligned16(rast) && (!db || aligned16(db)) && ((uintptr_t)out_da & 7) == 0, "misaligned buffer");
+    long long npix = (long long)W * H * views;
+    k_interp_fwd<<<vcl_blocks(npix, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const float4*)rast, (const float4*)db, attr, nv, dim, tri, nt, npix, out, (float2*)out_da, ctx->dev_flags);
+    return vcl_launch_check(ctx, "interpolate_fwd");
+}
+
+VCL_API vcl_status vcl_interpolate_bwd(vcl_ctx* ctx, const float* rast, int W, int H, int views, const float* attr,
+                                       int nv, int dim, const uint32_t* tri, int nt, const float* grad_out,
+                                       float* grad_attr, float* grad_bary, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(rast && attr && tri && grad_out && W > 0 && H > 0 && views > 0 && dim > 0, "bad interpolate_bwd arguments");
+    VCL_REQUIRE(aligned16(rast) && ((uintptr_t)grad_bary & 7) == 0 && (dim != 4 || aligned16(grad_attr)) &&
+                    ((uintptr_t)grad_attr & 7) == 0, "misaligned buffer");
+    long long npix = (long long)W * H * views;
+    k_interp_bwd<<<vcl_blocks(npix, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const float4*)rast, attr, nv, dim, tri, nt, npix, grad_out, grad_attr, (float2*)grad_bary,
+        ctx->mode == VCL_MODE_EXACT, ctx->dev_flags);
+    return vcl_launch_check(ctx, "interpolate_bwd");
+}
+
+VCL_API vcl_status vcl_texture_fwd(vcl_ctx* ctx, const float* rast, const float* uv, const float* uv_da, int W, int H,
+                                   int views, const float* pyramid, int tw, int th, int C, int levels, float* out,
+                                   void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(rast && uv && pyramid && out && W > 0 && H > 0 && views > 0 && C > 0 && tw > 0 && th > 0,
+                "bad texture_fwd arguments");
+    VCL_REQUIRE(levels >= 1 && levels == vcl_tex_levels(tw, th, levels), "levels %d invalid for %dx%d", levels, tw, th);
+    VCL_REQUIRE(levels == 1 || uv_da, "uv_da needed for a mip-mapped texture");
+    VCL_REQUIRE(aligned16(rast) && ((uintptr_t)uv & 7) == 0 && (!uv_da || aligned16(uv_da)), "misaligned buffer");
+    TexDesc d = make_desc(tw, th, C, levels);
+    long long npix = (long long)W * H * views;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (C == 4 && aligned16(pyramid) && aligned16(out))
+        k_tex_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>(d, pyramid, (const float4*)rast, (const float2*)uv,
+                                                          (const float4*)uv_da, npix, out);
+    else
+        k_tex_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>(d, pyramid, (const float4*)rast, (const float2*)uv,
+                                                          (const float4*)uv_da, npix, out);
+    return vcl_launch_check(ctx, "texture_fwd");
+}
+
+VCL_API vcl_status vcl_texture_bwd(vcl_ctx* ctx, const float* rast, const float* uv, const float* uv_da, int W, int H,
+                                   int views, const float* pyramid, int tw, int th, int C, int levels,
+                                   const float* grad_out, float* grad_pyramid, float* grad_uv, float* grad_uv_da,
+                                   void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(rast && uv && pyramid && grad_out && W > 0 && H > 0 && views > 0 && C > 0 && tw > 0 && th > 0,
+                "bad texture_bwd arguments");
+    VCL_REQUIRE(levels >= 1 && levels == vcl_tex_levels(tw, th, levels), "levels %d invalid for %dx%d", levels, tw, th);
+    VCL_REQUIRE(levels == 1 || uv_da, "uv_da needed for a mip-mapped texture");
+    VCL_REQUIRE(aligned16(rast) && ((uintptr_t)uv & 7) == 0 && (!uv_da || aligned16(uv_da)) &&
+                    ((uintptr_t)grad_uv & 7) == 0 && aligned16(grad_uv_da), "misaligned buffer");
+    TexDesc d = make_desc(tw, th, C, levels);
+    long long npix = (long long)W * H * views;
+    cudaStream_t s = (cudaStream_t)stream;
+    int exact = ctx->mode == VCL_MODE_EXACT;
+    if (C == 4 && aligned16(pyramid) && aligned16(grad_out) && aligned16(grad_pyramid))
+        k_tex_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>(d, pyramid, (const float4*)rast, (const float2*)uv,
+                                                          (const float4*)uv_da, npix, grad_out, grad_pyramid,
+                                                          (float2*)grad_uv, (float4*)grad_uv_da, exact);
+    else
+        k_tex_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>(d, pyramid, (const float4*)rast, (const float2*)uv,
+                                                          (const float4*)uv_da, npix, grad_out, grad_pyramid,
+                                                          (float2*)grad_uv, (float4*)grad_uv_da, exact);
+    return vcl_launch_check(ctx, "texture_bwd");
+}
+
+VCL_API vcl_status vcl_texture_build_mips(vcl_ctx* ctx, float* pyramid, int tw, int th, int C, int levels, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(pyramid && tw > 0 && th > 0 && C > 0, "bad build_mips arguments");
+    VCL_REQUIRE(levels >= 1 && levels == vcl_tex_levels(tw, th, levels), "levels %d invalid for %dx%d", levels, tw, th);
+    VCL_REQUIRE(C != 4 || aligned16(pyramid), "misaligned pyramid");
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int l = 1; l < levels; ++l) {
+        int w = tw >> l, h = th >> l;
+        k_mip_down<<<vcl_blocks((long long)w * h, 256), 256, 0, s>>>(pyramid + vcl_tex_level_offset(tw, th, C, l - 1),
+                                                                      pyramid + vcl_tex_level_offset(tw, th, C, l), w, h, C);
+    }
+    return vcl_launch_check(ctx, "build_mips");
+}
+
+VCL_API vcl_status vcl_texture_grad_pushdown(vcl_ctx* ctx, float* grad_pyramid, int tw, int th, int C, int levels,
+                                             void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(grad_pyramid && tw > 0 && th > 0 && C > 0, "bad pushdown arguments");
+    VCL_REQUIRE(levels >= 1 && levels == vcl_tex_levels(tw, th, levels), "levels %d invalid for %dx%d", levels, tw, th);
+    cudaStream_t s = (cudaStream_t)stream;
+    float wgt = ctx->mode == VCL_MODE_EXACT ? 0.25f : 1.f;
+    for (int l = levels - 1; l > 0; --l) {
+        int w = tw >> l, h = th >> l;
+        k_mip_push<<<vcl_blocks((long long)w * h * C, 256), 256, 0, s>>>(
+            grad_pyramid + vcl_tex_level_offset(tw, th, C, l), grad_pyramid + vcl_tex_level_offset(tw, th, C, l - 1), w, h,
+            C, wgt);
+    }
+    return vcl_launch_check(ctx, "grad_pushdown");
+}
+
+VCL_API vcl_status vcl_clamp(vcl_ctx* ctx, float* p, size_t n, float lo, float hi, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(p || n == 0, "null buffer");
+    if (n == 0) return VCL_OK;
+    k_clamp<<<vcl_blocks((long long)n, 256), 256, 0, (cudaStream_t)stream>>>(p, (long long)n, lo, hi);
+    return vcl_launch_check(ctx, "clamp");
+}
+
+VCL_API vcl_status vcl_antialias_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
+                                     const float* rast, int W, int H, int views, int C, const float* in, float* out,
+                                     void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(clip && tri && rast && in && out && W > 0 && H > 0 && views > 0 && C > 0, "bad antialias_fwd arguments");
+    VCL_REQUIRE(aligned16(clip) && aligned16(rast), "misaligned buffer");
+    VCL_REQUIRE(in != out, "antialias_fwd cannot run in place");
+    long long npix = (long long)W * H * views;
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(out, in, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s),
+                                   "antialias copy");
+    if (st) return st;
+    if (C == 4 && aligned16(in) && aligned16(out))
+        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, out, ctx->dev_flags);
+    else
+        k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, out, ctx->dev_flags);
+    return vcl_launch_check(ctx, "antialias_fwd");
+}
+
+VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
+                                     const float* rast, int W, int H, int views, int C, const float* in,
+                                     const float* grad_out, float* grad_in, float* grad_clip, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(clip && tri && rast && in && grad_out && grad_in && W > 0 && H > 0 && views > 0 && C > 0,
+                "bad antialias_bwd arguments");
+    VCL_REQUIRE(aligned16(clip) && aligned16(rast) && aligned16(grad_clip), "misaligned buffer");
+    VCL_REQUIRE(grad_in != grad_out, "antialias_bwd cannot run in place");
+    long long npix = (long long)W * H * views;
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = vcl_cuda_check(
+        ctx, cudaMemcpyAsync(grad_in, grad_out, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s), "antialias copy");
+    if (st) return st;
+    int exact = ctx->mode == VCL_MODE_EXACT;
+    if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in))
+        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+    else
+        k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+    return vcl_launch_check(ctx, "antialias_bwd");
+}
+
+VCL_API vcl_status vcl_mse(vcl_ctx* ctx, const float* pred, const float* target, size_t n, float* grad, float* loss_dev,
+                           void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(pred && target && grad && loss_dev, "bad mse arguments");
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(loss_dev, 0, sizeof(float), s), "mse clear");
+    if (st) return st;
+    if (n == 0) return VCL_OK;
+    k_mse<<<grid_for((long long)n, 256, ctx->sm_count), 256, 0, s>>>(pred, target, (long long)n, grad, loss_dev);
+    return vcl_launch_check(ctx, "mse");
+}
+
+VCL_API vcl_status vcl_adam_step(vcl_ctx* ctx, float* p, const float* g, float* m, float* v, size_t n, double lr,
+                                 double beta1, double beta2, double eps, int step, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(p && g && m && v && step >= 1, "bad adam arguments");
+    if (n == 0) return VCL_OK;
+    int vec = aligned16(p) && aligned16(g) && aligned16(m) && aligned16(v);
+    double c1 = ctx->mode == VCL_MODE_EXACT ? 1.0 : beta1, c2 = ctx->mode == VCL_MODE_EXACT ? 1.0 : beta2;
+    for (int k = 0; k < step; ++k) { c1 *= beta1; c2 *= beta2; }
+    k_adam<<<grid_for((long long)(n + 3) / 4, 256, ctx->sm_count), 256, 0, (cudaStream_t)stream>>>(
+        p, g, m, v, (long long)n, beta1, beta2, lr, eps, 1.0 - c1, 1.0 - c2, vec);
+    return vcl_launch_check(ctx, "adam_step");
+}
+
+}  // extern "C"

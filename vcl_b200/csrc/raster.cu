@@ -1,0 +1,423 @@
+// CUDA rasterizer replacing the reference's OpenGL draw (rasterize.cpp:
+// 91-202, fixed-function state :252-268) and its backward pass
+// (rasterize.cu:84-141).
+//
+// Forward = triangle setup -> tile binner -> fine rasterizer:
+//   1. setup   one thread per (view, triangle): homogeneous-2D edge
+//              functions, orientation, trivial reject, conservative pixel
+//              box; counts the tiles the box overlaps (atomic per tile);
+//   2. scan    exclusive prefix sum of the per-tile counts -> bin offsets;
+//   3. emit    one thread per (view, triangle) writes its id into each
+//              overlapped tile's bin (order inside a bin is irrelevant);
+//   4. fine    one CTA per tile, one thread per pixel: stages the bin's
+//              triangle records through shared memory in chunks, keeps the
+//              nearest (z/w, id) per pixel -- strictly nearer wins, equal
+//              depth keeps the lower id, which is what GL_LESS gives for
+//              triangles drawn in index order -- then writes
+//              (u, v, z/w, id+1) and the barycentric derivatives (DB).
+// A tile whose bin does not fit the bin-list capacity is rasterized by
+// testing every triangle of its view (same results, slower).
+//
+// The coverage/depth arithmetic uses explicitly rounded operations
+// (__fmul_rn etc., never fused) so that it is bit-identical to the CPU
+// restatement of the same rules: triangle ids, barycentrics and depth match
+// exactly.
+#include "common.cuh"
+
+namespace {
+
+DEV float mul(float a, float b) { return __fmul_rn(a, b); }
+DEV float add(float a, float b) { return __fadd_rn(a, b); }
+DEV float sub(float a, float b) { return __fsub_rn(a, b); }
+DEV float dvd(float a, float b) { return __fdiv_rn(a, b); }
+
+struct __align__(16) RTri {
+    float4 a;   // a0 a1 a2 sigma
+    float4 b;   // b0 b1 b2 -
+    float4 k;   // k0 k1 k2 -
+    float4 z;   // z0 z1 z2 -
+    float4 w;   // w0 w1 w2 -
+    int4 box;   // x0 x1 y0 y1 ; empty when x0 > x1
+};
+
+constexpr int CHUNK = 128;
+
+// Pixel-centre NDC coordinate (2p+1-W)/W: exact numerator, one rounding.
+DEV float ndc(int p, int W) { return dvd((float)(2 * p + 1 - W), (float)W); }
+
+DEV float edge(float a, float b, float k, float sx, float sy) { return add(add(mul(a, sx), mul(b, sy)), k); }
+
+DEV bool edge_in(float A, float a, float b, float sigma) {
+    float sA = mul(sigma, A);
+    if (sA > 0.f) return true;
+    if (A != 0.f) return false;
+    float gx = mul(sigma, a), gy = mul(sigma, b);
+    return gx > 0.f || (gx == 0.f && gy < 0.f);
+}
+
+DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool& valid) {
+    float x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y, x2 = c2.x, y2 = c2.y;
+    float w0 = c0.w, w1 = c1.w, w2 = c2.w;
+    t.a = make_float4(sub(mul(w2, y1), mul(w1, y2)), sub(mul(w0, y2), mul(w2, y0)), sub(mul(w1, y0), mul(w0, y1)), 0.f);
+    t.b = make_float4(sub(mul(w1, x2), mul(w2, x1)), sub(mul(w2, x0), mul(w0, x2)), sub(mul(w0, x1), mul(w1, x0)), 0.f);
+    t.k = make_float4(sub(mul(x1, y2), mul(y1, x2)), sub(mul(x2, y0), mul(y2, x0)), sub(mul(x0, y1), mul(y0, x1)), 0.f);
+    float det = add(add(mul(w0, t.k.x), mul(w1, t.k.y)), mul(w2, t.k.z));
+    valid = det != 0.f && isfinite(det);
+    t.a.w = det > 0.f ? 1.f : -1.f;
+    t.z = make_float4(c0.z, c1.z, c2.z, 0.f);
+    t.w = make_float4(w0, w1, w2, 0.f);
+    // trivial reject: all three vertices outside one clip plane
+    bool o0 = x0 > w0 && x1 > w1 && x2 > w2, o1 = x0 < -w0 && x1 < -w1 && x2 < -w2;
+    bool o2 = y0 > w0 && y1 > w1 && y2 > w2, o3 = y0 < -w0 && y1 < -w1 && y2 < -w2;
+    bool o4 = c0.z > w0 && c1.z > w1 && c2.z > w2, o5 = c0.z < -w0 && c1.z < -w1 && c2.z < -w2;
+    if (o0 || o1 || o2 || o3 || o4 || o5) valid = false;
+    // conservative pixel box (the CPU restatement's raster_bbox)
+    int bx0 = 0, bx1 = W - 1, by0 = 0, by1 = H - 1;
+    if (w0 > 0.f && w1 > 0.f && w2 > 0.f) {
+        float X0 = dvd(x0, w0), X1 = dvd(x1, w1), X2 = dvd(x2, w2);
+        float Y0 = dvd(y0, w0), Y1 = dvd(y1, w1), Y2 = dvd(y2, w2);
+        float xmn = fminf(fminf(X0, X1), X2), xmx = fmaxf(fmaxf(X0, X1), X2);
+        float ymn = fminf(fminf(Y0, Y1), Y2), ymx = fmaxf(fmaxf(Y0, Y1), Y2);
+        float hw = mul(0.5f, (float)W), hh = mul(0.5f, (float)H);
+        float fx0 = sub(mul(add(xmn, 1.f), hw), 0.5f), fx1 = sub(mul(add(xmx, 1.f), hw), 0.5f);
+        float fy0 = sub(mul(add(ymn, 1.f), hh), 0.5f), fy1 = sub(mul(add(ymx, 1.f), hh), 0.5f);
+        fx0 = fmaxf(fminf(fx0, (float)W), -2.f); fx1 = fmaxf(fminf(fx1, (float)W), -2.f);
+        fy0 = fmaxf(fminf(fy0, (float)H), -2.f); fy1 = fmaxf(fminf(fy1, (float)H), -2.f);
+        if (fx0 == fx0 && fx1 == fx1 && fy0 == fy0 && fy1 == fy1) {
+            bx0 = max((int)floorf(fx0) - 1, 0); bx1 = min((int)ceilf(fx1) + 1, W - 1);
+            by0 = max((int)floorf(fy0) - 1, 0); by1 = min((int)ceilf(fy1) + 1, H - 1);
+        }
+    }
+    if (!valid) { bx0 = 1; bx1 = 0; }
+    t.box = make_int4(bx0, bx1, by0, by1);
+}
+
+__global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W, int H,
+                        int views, int tile, int tiles_x, int ntiles, RTri* __restrict__ setup, int* __restrict__ count,
+                        int* __restrict__ flags) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)views * nt) return;
+    int view = (int)(gid / nt), t = (int)(gid % nt);
+    uint32_t i0 = tri[3 * (size_t)t], i1 = tri[3 * (size_t)t + 1], i2 = tri[3 * (size_t)t + 2];
+    RTri r;
+    bool valid = false;
+    if (i0 < (uint32_t)nv && i1 < (uint32_t)nv && i2 < (uint32_t)nv) {
+        const float4* cv = clip + (size_t)view * nv;
+        setup_tri(cv[i0], cv[i1], cv[i2], W, H, r, valid);
+    } else {
+        atomicOr(&flags[1], 1);  // out-of-range vertex index: triangle dropped
+        r.box = make_int4(1, 0, 1, 0);
+    }
+    setup[gid] = r;
+    if (r.box.x > r.box.y || r.box.z > r.box.w) return;
+    int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
+    int* cnt = count + (size_t)view * ntiles;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&cnt[ty * tiles_x + tx], 1);
+}
+
+// Exclusive scan of n ints by one CTA of 1024 threads (chunked).
+__global__ void k_scan(const int* __restrict__ in, int* __restrict__ out, int n) {
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        int i = base + tid;
+        int v = i < n ? in[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) warp_sums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int s = warp_sums[lane];
+            for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, s, o); if (lane >= o) s += y; }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        int excl = carry + (wid ? warp_sums[wid - 1] : 0) + x - v;
+        if (i < n) out[i] = excl;
+        __syncthreads();
+        if (tid == 1023) carry = excl + v;
+        __syncthreads();
+    }
+}
+
+__global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int tile, int tiles_x, int ntiles,
+                       const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list, long long cap) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)views * nt) return;
+    int view = (int)(gid / nt), t = (int)(gid % nt);
+    int4 box = setup[gid].box;
+    if (box.x > box.y || box.z > box.w) return;
+    int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) {
+            size_t ti = (size_t)view * ntiles + ty * tiles_x + tx;
+            int slot = atomicAdd(&cursor[ti], 1);
+            long long p = (long long)offset[ti] + slot;
+            if (p < cap) list[p] = t;
+        }
+}
+
+// The reference geometry shader's per-vertex barycentric derivatives
+// (rasterize.cpp:141-164), evaluated at (u, v) and scaled by w (:176).
+DEV float4 db_eval(float4 c0, float4 c1, float4 c2, float xs, float ys, float u, float v) {
+    float w0 = c0.w, w1 = c1.w, w2 = c2.w;
+    float e0x = sub(mul(w0, c2.x), mul(w2, c0.x)), e0y = sub(mul(w0, c2.y), mul(w2, c0.y));
+    float e1x = sub(mul(w1, c2.x), mul(w2, c1.x)), e1y = sub(mul(w1, c2.y), mul(w2, c1.y));
+    float ex = sub(mul(w0, c1.x), mul(w1, c0.x)), ey = sub(mul(w0, c1.y), mul(w1, c0.y));
+    float a = sub(mul(e0x, e1y), mul(e0y, e1x));
+    const float eps = 1e-6f;
+    float ca = (fabsf(a) >= eps) ? a : (a < 0.f) ? -eps : eps;
+    float sx = dvd(mul(ys, w2), ca), sy = dvd(mul(xs, w2), ca);
+    e0x = mul(e0x, sx); e0y = mul(e0y, sy);
+    e1x = mul(e1x, sx); e1y = mul(e1y, sy);
+    ex = mul(ex, sx); ey = mul(ey, sy);
+    float d0[4] = {sub(e0y, ey), add(-e0x, ex), -e0y, e0x};
+    float d1[4] = {e1y, -e1x, sub(-e1y, ey), add(e1x, ex)};
+    float d2[4] = {e1y, -e1x, -e0y, e0x};
+    float l2 = sub(sub(1.f, u), v);
+    float wi = add(add(mul(u, w0), mul(v, w1)), mul(l2, w2));
+    float o[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) o[c] = mul(add(add(mul(u, d0[c]), mul(v, d1[c])), mul(l2, d2[c])), wi);
+    return make_float4(o[0], o[1], o[2], o[3]);
+}
+
+template <int T>
+__global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, const int* __restrict__ count,
+                                                const int* __restrict__ offset, const int* __restrict__ list,
+                                                long long cap, int nt, int W, int H, int tiles_x, int ntiles,
+                                                const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri,
+                                                float4* __restrict__ rast, float4* __restrict__ db, int* __restrict__ flags) {
+    __shared__ RTri s_tri[CHUNK];
+    __shared__ int s_id[CHUNK];
+    const int view = blockIdx.y, tile_id = blockIdx.x;
+    const int tx = tile_id % tiles_x, ty = tile_id / tiles_x;
+    const int px = tx * T + threadIdx.x, py = ty * T + threadIdx.y;
+    const int tid = threadIdx.y * T + threadIdx.x;
+    const bool inside = px < W && py < H;
+    const float sx = ndc(px, W), sy = ndc(py, H);
+    const size_t ti = (size_t)view * ntiles + tile_id;
+    const int c = count[ti];
+    const int off = offset[ti];
+    const bool overflow = (long long)off + c > cap;
+    const int n_iter = overflow ? nt : c;
+    const RTri* vs = setup + (size_t)view * nt;
+    float best_z = 1.f;
+    int best_t = -1;
+    for (int i0 = 0; i0 < n_iter; i0 += CHUNK) {
+        if (tid < CHUNK && i0 + tid < n_iter) {
+            int t = overflow ? i0 + tid : list[off + i0 + tid];
+            s_id[tid] = t;
+            s_tri[tid] = vs[t];
+        }
+        __syncthreads();
+        const int m = min(CHUNK, n_iter - i0);
+        if (inside) {
+            for (int j = 0; j < m; ++j) {
+                const int4 box = s_tri[j].box;
+                if (px < box.x || px > box.y || py < box.z || py > box.w) continue;
+                const float4 a = s_tri[j].a, b = s_tri[j].b, k = s_tri[j].k;
+                float A0 = edge(a.x, b.x, k.x, sx, sy);
+                float A1 = edge(a.y, b.y, k.y, sx, sy);
+                float A2 = edge(a.z, b.z, k.z, sx, sy);
+                if (!edge_in(A0, a.x, b.x, a.w) || !edge_in(A1, a.y, b.y, a.w) || !edge_in(A2, a.z, b.z, a.w)) continue;
+                float D = add(add(A0, A1), A2);
+                if (!(mul(a.w, D) > 0.f)) continue;
+                const float4 z = s_tri[j].z, w = s_tri[j].w;
+                float zn = add(add(mul(A0, z.x), mul(A1, z.y)), mul(A2, z.z));
+                float wn = add(add(mul(A0, w.x), mul(A1, w.y)), mul(A2, w.z));
+                float zw = dvd(zn, wn);
+                if (!(zw >= -1.f && zw <= 1.f)) continue;
+                int t = s_id[j];
+                if (zw < best_z || (zw == best_z && best_t >= 0 && t < best_t)) { best_z = zw; best_t = t; }
+            }
+        }
+        __syncthreads();
+    }
+    if (overflow && tid == 0) atomicAdd(&flags[0], 1);
+    if (!inside) return;
+    const size_t pix = ((size_t)view * H + py) * W + px;
+    if (best_t < 0) {
+        rast[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (db) db[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const RTri r = vs[best_t];
+    float A0 = edge(r.a.x, r.b.x, r.k.x, sx, sy);
+    float A1 = edge(r.a.y, r.b.y, r.k.y, sx, sy);
+    float A2 = edge(r.a.z, r.b.z, r.k.z, sx, sy);
+    float D = add(add(A0, A1), A2);
+    float u = dvd(A0, D), v = dvd(A1, D);
+    rast[pix] = make_float4(u, v, best_z, (float)(best_t + 1));
+    if (db) {
+        const float4* cv = clip + (size_t)view * nv;
+        float4 c0 = cv[tri[3 * (size_t)best_t]], c1 = cv[tri[3 * (size_t)best_t + 1]], c2 = cv[tri[3 * (size_t)best_t + 2]];
+        db[pix] = db_eval(c0, c1, c2, dvd(2.f, (float)W), dvd(2.f, (float)H), u, v);
+    }
+}
+
+// rasterize.cu:84-141: dL/d(x, y, w) of the three clip-space vertices from
+// dL/d(u, v); one vector atomic per vertex (z receives +0).
+__global__ void k_raster_bwd(const float* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W,
+                             int H, long long npix, const float4* __restrict__ rast, const float2* __restrict__ gb,
+                             float* __restrict__ gclip) {
+    long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pidx >= npix) return;
+    float4 r = rast[pidx];
+    int idx = rast_id(r.w);
+    if (idx < 0 || idx >= nt) return;
+    float2 g = gb[pidx];
+    if (((__float_as_uint(g.x) | __float_as_uint(g.y)) << 1) == 0u) return;
+    long long hw = (long long)W * H;
+    int view = (int)(pidx / hw);
+    int rem = (int)(pidx - view * hw);
+    int py = rem / W, px = rem - py * W;
+    const float xs = 2.f / (float)W, ys = 2.f / (float)H;
+    float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
+    float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
+    uint32_t i0 = tri[3 * (size_t)idx], i1 = tri[3 * (size_t)idx + 1], i2 = tri[3 * (size_t)idx + 2];
+    if (i0 >= (uint32_t)nv || i1 >= (uint32_t)nv || i2 >= (uint32_t)nv) return;
+    const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * nv;
+    float4 c0 = cv[i0], c1 = cv[i1], c2 = cv[i2];
+    float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
+    float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
+    float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
+    float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
+    float a = e0x * e1y - e0y * e1x;
+    float ia = 1.f / (a + (a > 0 ? 1e-6f : -1e-6f));
+    float kuv = r.x * g.x + r.y * g.y;
+    float gx0 = (g.y * p2y + kuv * e1y) * ia;
+    float gy0 = (-g.y * p2x - kuv * e1x) * ia;
+    float gw0 = -gx0 * pxn - gy0 * pyn;
+    float gx1 = (-g.x * p2y - kuv * e0y) * ia;
+    float gy1 = (g.x * p2x + kuv * e0x) * ia;
+    float gw1 = -gx1 * pxn - gy1 * pyn;
+    float gx2 = ((-g.y * p0y + g.x * p1y) - kuv * (-p0y + p1y)) * ia;
+    float gy2 = ((g.y * p0x - g.x * p1x) - kuv * (p0x - p1x)) * ia;
+    float gw2 = -gx2 * pxn - gy2 * pyn;
+    float* gv = gclip + (size_t)view * nv * 4;
+    red_add4(gv + (size_t)i0 * 4, gx0, gy0, 0.f, gw0);
+    red_add4(gv + (size_t)i1 * 4, gx1, gy1, 0.f, gw1);
+    red_add4(gv + (size_t)i2 * 4, gx2, gy2, 0.f, gw2);
+}
+
+struct RasterWS {
+    RTri* setup;
+    int* count;
+    int* offset;
+    int* cursor;
+    int* list;
+    long long cap;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+long long auto_capacity(long long views, long long nt, int W, int H, int tile) {
+    long long ntiles = (long long)((W + tile - 1) / tile) * ((H + tile - 1) / tile) * views;
+    long long c = views * nt * 6 + ntiles * 4 + (1 << 20);
+    return c > (1ll << 31) - 1 ? (1ll << 31) - 1 : c;
+}
+
+size_t ws_bytes(long long views, long long nt, long long ntiles, long long cap) {
+    return align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1)) + 3 * align256(sizeof(int) * (size_t)ntiles) +
+           align256(sizeof(int) * (size_t)cap);
+}
+
+RasterWS carve(void* base, long long views, long long nt, long long ntiles, long long cap) {
+    char* p = (char*)base;
+    RasterWS w;
+    w.setup = (RTri*)p; p += align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1));
+    w.count = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
+    w.offset = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
+    w.cursor = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
+    w.list = (int*)p;
+    w.cap = cap;
+    return w;
+}
+
+}  // namespace
+
+extern "C" {
+
+VCL_API vcl_status vcl_reserve_raster(vcl_ctx* ctx, int W, int H, int views, int nt) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nt >= 0, "bad raster reservation sizes");
+    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity(views, nt, W, H, ctx->tile);
+    int ts[3] = {8, 16, 32};
+    size_t need = 0;
+    for (int t : ts) {
+        long long ntiles = (long long)((W + t - 1) / t) * ((H + t - 1) / t) * views;
+        size_t b = ws_bytes(views, nt, ntiles, cap);
+        if (b > need) need = b;
+    }
+    return vcl_ws_reserve(ctx, need);
+}
+
+VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W,
+                                     int H, int views, float* rast, float* db, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nv >= 0 && nt >= 0, "bad raster sizes W=%d H=%d views=%d nv=%d nt=%d",
+                W, H, views, nv, nt);
+    VCL_REQUIRE(rast, "rast output is null");
+    VCL_REQUIRE(nt == 0 || (clip && tri), "clip/tri is null");
+    VCL_REQUIRE(((uintptr_t)clip & 15) == 0 && ((uintptr_t)rast & 15) == 0 && ((uintptr_t)db & 15) == 0,
+                "clip/rast/db must be 16-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int T = ctx->tile;
+    const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
+    const long long ntiles_view = (long long)tiles_x * tiles_y;
+    const long long ntiles = ntiles_view * views;
+    VCL_REQUIRE(ntiles < (1ll << 31), "too many tiles");
+    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity(views, nt, W, H, T);
+    vcl_status st = vcl_ws_reserve(ctx, ws_bytes(views, nt, ntiles, cap));
+    if (st) return st;
+    RasterWS w = carve(ctx->ws, views, nt, ntiles, cap);
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
+    if (st) return st;
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.cursor, 0, sizeof(int) * ntiles, s), "raster memset");
+    if (st) return st;
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(ctx->dev_flags, 0, sizeof(int), s), "raster memset");
+    if (st) return st;
+    long long work = (long long)views * nt;
+    if (work > 0) {
+        k_setup<<<vcl_blocks(work, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
+                                                       (int)ntiles_view, w.setup, w.count, ctx->dev_flags);
+    }
+    k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
+    if (work > 0) {
+        k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, T, tiles_x, (int)ntiles_view, w.offset,
+                                                      w.cursor, w.list, cap);
+    }
+    dim3 grid((unsigned)ntiles_view, (unsigned)views);
+    const float4* c4 = (const float4*)clip;
+    if (T == 8)
+        k_fine<8><<<grid, dim3(8, 8), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
+                                             (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+    else if (T == 16)
+        k_fine<16><<<grid, dim3(16, 16), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
+                                               (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+    else
+        k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
+                                               (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+    return vcl_launch_check(ctx, "rasterize_fwd");
+}
+
+VCL_API vcl_status vcl_rasterize_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W, int H,
+                                     int views, const float* rast, const float* grad_bary, float* grad_clip,
+                                     void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0, "bad raster sizes");
+    VCL_REQUIRE(clip && tri && rast && grad_bary && grad_clip, "null buffer");
+    VCL_REQUIRE(((uintptr_t)clip & 15) == 0 && ((uintptr_t)grad_clip & 15) == 0 && ((uintptr_t)rast & 15) == 0 &&
+                    ((uintptr_t)grad_bary & 7) == 0, "misaligned buffer");
+    long long npix = (long long)W * H * views;
+    k_raster_bwd<<<vcl_blocks(npix, 256), 256, 0, (cudaStream_t)stream>>>(
+        clip, nv, tri, nt, W, H, npix, (const float4*)rast, (const float2*)grad_bary, grad_clip);
+    return vcl_launch_check(ctx, "rasterize_bwd");
+}
+
+}  // extern "C"
