@@ -37,7 +37,7 @@ SIGS = {
     "interpolate_fwd": "iiiiipppppp",
     "interpolate_bwd": "iiiiipppppp",
     "texture_fwd": "iiiiiiippppp",
-    "texture_bwd": "iiiiiiipppppppp",
+    "texture_bwd": "iiiiiiiipppppppp",
     "mip_build": "iiiip",
     "mip_pushdown": "iiiiip",
     "clamp": "zpff",

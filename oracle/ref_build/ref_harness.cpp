@@ -120,7 +120,7 @@ void ref_texture_fwd(int W, int H, int views, int tw, int th, int C, int L, cons
     p.kernel.out = out;
     Texturemap::forward(p);
 }
-void ref_texture_bwd(int W, int H, int views, int tw, int th, int C, int L, const float* pyr,
+void ref_texture_bwd(int /*mode*/, int W, int H, int views, int tw, int th, int C, int L, const float* pyr,
                      const float* rast, const float* uv, const float* uv_da, const float* g_out,
                      float* g_pyr, float* g_uv, float* g_uv_da) {
     TexturemapGradParams p{};

@@ -486,7 +486,7 @@ void orc_texture_fwd(int W, int H, int views, int tw, int th, int C, int L,
 }
 
 /* texturemap.cu:229-319 */
-void orc_texture_bwd(int W, int H, int views, int tw, int th, int C, int L,
+void orc_texture_bwd(int mode, int W, int H, int views, int tw, int th, int C, int L,
                      const float* pyr, const float* rast, const float* uv,
                      const float* uv_da, const float* g_out, float* g_pyr,
                      float* g_uv, float* g_uv_da) {
@@ -496,7 +496,7 @@ void orc_texture_bwd(int W, int H, int views, int tw, int th, int C, int L,
         f2 u = F2(uv[pidx * 2], uv[pidx * 2 + 1]);
         if (L > 1) {
             int l0 = 0, l1 = 0; float fl = 0.f, dl[4];
-            calc_level_jacob(0, tw, th, L, uv_da + pidx * 4, &l0, &l1, &fl, dl);
+            calc_level_jacob(mode, tw, th, L, uv_da + pidx * 4, &l0, &l1, &fl, dl);
             int i0[4], i1[4]; f2 t0, t1;
             index_fetch(tw, th, l0, u, i0, &t0);
             index_fetch(tw, th, l1, u, i1, &t1);

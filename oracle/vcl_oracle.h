@@ -54,7 +54,7 @@ size_t orc_tex_level_offset(int tw, int th, int C, int level);
 void orc_texture_fwd(int W, int H, int views, int tw, int th, int C, int levels,
                      const float* pyramid, const float* rast, const float* uv,
                      const float* uv_da, float* out);
-void orc_texture_bwd(int W, int H, int views, int tw, int th, int C, int levels,
+void orc_texture_bwd(int mode, int W, int H, int views, int tw, int th, int C, int levels,
                      const float* pyramid, const float* rast, const float* uv,
                      const float* uv_da, const float* grad_out, float* grad_pyramid,
                      float* grad_uv, float* grad_uv_da);

@@ -87,7 +87,7 @@ def run_chain(lib, scene, mode=0, target=None, rast=None, db=None, pos=None, pyr
     lib.sg_specular_bwd(W, H, V, rast, normal, view, rough, S.ior, g_sam, g_ssh, g_rough)
     r["g_rough"] = g_rough
     g_pyr = np.zeros_like(pyr); g_uv = f32((N, 2)); g_uv_da = f32((N, 4))
-    lib.texture_bwd(W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, uv, uv_da, g_diffuse, g_pyr, g_uv, g_uv_da)
+    lib.texture_bwd(mode, W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, uv, uv_da, g_diffuse, g_pyr, g_uv, g_uv_da)
     r["g_pyr"], r["g_uv"], r["g_uv_da"] = g_pyr, g_uv, g_uv_da
     g_uvattr = f32((S.nv, 2)); g_bary = f32((N, 2))
     lib.interpolate_bwd(mode, W, H, V, 2, rast, S.uv, S.tri, g_uv, g_uvattr, g_bary)
@@ -103,3 +103,44 @@ def run_chain(lib, scene, mode=0, target=None, rast=None, db=None, pos=None, pyr
     lib.adam(mode, n0, p, np.ascontiguousarray(g_pyr[:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, adam_step)
     r["adam_p"], r["adam_m"], r["adam_v"] = p, m, vv
     return r
+
+
+def oracle_fit(S, mode, steps, target, lr=None):
+    """Full fit iterations on the CPU oracle, as a fit job runs them:
+    forward/backward (run_chain), mip gradient push-down, Adam on texture
+    level 0 + clamp + mip rebuild, Adam on positions and on the lobes
+    (axis | sharpness | amplitude), all with persistent moments."""
+    lib = O.orc()
+    lr = S.lr if lr is None else lr
+    pos = S.pos.copy()
+    pyr = build_pyramid(S, S.tex_init)
+    lobes = np.concatenate([S.lobe_axis_init.reshape(-1), S.lobe_sharp_init.reshape(-1),
+                            S.lobe_amp_init.reshape(-1)]).astype(np.float32)
+    K, C = S.K, S.C
+    n0 = S.tex_w * S.tex_h * C
+    mt, vt = f32((n0,)), f32((n0,))
+    mp, vp = f32((S.nv * 3,)), f32((S.nv * 3,))
+    ml, vl = f32((lobes.size,)), f32((lobes.size,))
+    losses = []
+    for t in range(1, steps + 1):
+        ax = np.ascontiguousarray(lobes[:3 * K].reshape(K, 3))
+        sh = np.ascontiguousarray(lobes[3 * K:4 * K])
+        am = np.ascontiguousarray(lobes[4 * K:].reshape(K, C))
+        r = run_chain(lib, S, mode, target=target, pos=pos, pyr=pyr, lobes=(ax, sh, am))
+        n = S.W * S.H * S.views * C
+        losses.append(lib.mse(1, n, r["aa"], target, np.zeros(n, np.float32)))
+        g = r["g_pyr"].copy()
+        lib.mip_pushdown(mode, S.tex_w, S.tex_h, C, S.levels, g)
+        p0 = np.ascontiguousarray(pyr[:n0])
+        lib.adam(mode, n0, p0, np.ascontiguousarray(g[:n0]), mt, vt, lr, 0.9, 0.999, 1e-8, t)
+        lib.clamp(n0, p0, 0.0, 1.0)
+        pyr = pyr.copy(); pyr[:n0] = p0
+        lib.mip_build(S.tex_w, S.tex_h, C, S.levels, pyr)
+        pp = np.ascontiguousarray(pos.reshape(-1))
+        lib.adam(mode, pp.size, pp, np.ascontiguousarray(r["g_pos"].reshape(-1)), mp, vp, lr, 0.9, 0.999, 1e-8, t)
+        pos = pp.reshape(-1, 3)
+        gl = np.concatenate([r["g_axis"].reshape(-1), r["g_sharp"].reshape(-1), r["g_amp"].reshape(-1)]).astype(np.float32)
+        lib.adam(mode, lobes.size, lobes, gl, ml, vl, lr, 0.9, 0.999, 1e-8, t)
+    ax = lobes[:3 * K].reshape(K, 3); sh = lobes[3 * K:4 * K]; am = lobes[4 * K:].reshape(K, C)
+    return {"pos": pos, "tex": pyr[:n0].reshape(S.tex_h, S.tex_w, C), "axis": ax, "sharp": sh, "amp": am,
+            "losses": losses, "pyr": pyr}

@@ -1,0 +1,130 @@
+"""Fit jobs on the GPU (vcl_fit_*): the plain and fused strategies against
+full fit iterations of the CPU oracle, and against each other."""
+import numpy as np
+import pytest
+
+import chain
+from oracle import oracle as O
+from vcl_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).max(initial=0.0) / max(np.abs(b).max(initial=0.0), 1e-30)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from vcl_b200 import capi
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def _scene():
+    return scenes.small(seed=21, W=96, H=64, views=2, subdiv=3, tex=64, K=6)
+
+
+def _target(S):
+    return np.random.default_rng(S.seed + 3).random((S.W * S.H * S.views, S.C)).astype(np.float32)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("strategy", [0, 1])
+def test_fit_steps_match_oracle(ctx, mode, strategy):
+    from vcl_b200 import capi
+    S = _scene()
+    tgt = _target(S)
+    steps = 3
+    ref = chain.oracle_fit(S, mode, steps, tgt)
+    ctx.set_mode(mode)
+    fit = capi.Fit(ctx, S, strategy=strategy)
+    fit.set_target(tgt)
+    stream = torch.cuda.Stream()
+    losses = []
+    for _ in range(steps):
+        fit.step(stream.cuda_stream)
+        losses.append(fit.read_loss(stream.cuda_stream))
+    pos, tex, (ax, sh, am) = fit.read_params(stream.cuda_stream)
+    fit.close()
+    ctx.set_mode(0)
+    assert np.allclose(losses, ref["losses"], rtol=1e-5), (losses, ref["losses"])
+    # three Adam steps of size ~lr: parameters agree to far better than lr
+    for name, got, want in (("tex", tex, ref["tex"]), ("pos", pos, ref["pos"]), ("axis", ax, ref["axis"]),
+                            ("sharp", sh, ref["sharp"]), ("amp", am, ref["amp"])):
+        assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max()), (name, np.abs(got - want).max())
+
+
+def test_fused_equals_plain_over_many_steps(ctx):
+    from vcl_b200 import capi
+    S = _scene()
+    tgt = _target(S)
+    stream = torch.cuda.Stream()
+    res = []
+    for strategy in (capi.FIT_PLAIN, capi.FIT_FUSED):
+        fit = capi.Fit(ctx, S, strategy=strategy)
+        fit.set_target(tgt)
+        ls = []
+        for _ in range(10):
+            fit.step(stream.cuda_stream)
+            ls.append(fit.read_loss(stream.cuda_stream))
+        res.append((ls, fit.read_params(stream.cuda_stream)))
+        fit.close()
+    (l0, (p0, t0, lb0)), (l1, (p1, t1, lb1)) = res
+    assert np.allclose(l0, l1, rtol=1e-5)
+    assert rel_err(t1, t0) <= 1e-4 and rel_err(p1, p0) <= 1e-4
+    for a, b in zip(lb0, lb1):
+        assert rel_err(b, a) <= 1e-4
+    assert l1[-1] < l1[0]       # the fit makes progress
+
+
+def test_fused_graph_and_direct_launch_agree(ctx):
+    from vcl_b200 import capi
+    S = _scene()
+    tgt = _target(S)
+    out = []
+    for use_stream in (False, True):
+        fit = capi.Fit(ctx, S, strategy=capi.FIT_FUSED)
+        fit.set_target(tgt)
+        st = torch.cuda.Stream() if use_stream else None
+        h = st.cuda_stream if st else None
+        for _ in range(4):
+            fit.step(h)
+        torch.cuda.synchronize()
+        out.append(fit.read_params(h))
+        fit.close()
+    for a, b in zip(out[0][:2], out[1][:2]):
+        assert rel_err(a, b) <= 1e-5
+
+
+def test_render_is_deterministic_and_switching_strategy_keeps_step_count(ctx):
+    from vcl_b200 import capi
+    S = _scene()
+    fit = capi.Fit(ctx, S)
+    img = [torch.zeros(S.W * S.H * S.views * S.C, device="cuda") for _ in range(2)]
+    fit.render(img[0]); fit.render(img[1])
+    torch.cuda.synchronize()
+    assert torch.equal(img[0], img[1])
+    tgt = _target(S)
+    fit.set_target(tgt)
+    stream = torch.cuda.Stream()
+    fit.step(stream.cuda_stream)
+    fit.set_strategy(capi.FIT_FUSED)
+    fit.step(stream.cuda_stream)
+    fit.set_strategy(capi.FIT_PLAIN)
+    fit.step(stream.cuda_stream)
+    p_mixed = fit.read_params(stream.cuda_stream)
+    fit.close()
+    ref = capi.Fit(ctx, S)
+    ref.set_target(tgt)
+    for _ in range(3):
+        ref.step(stream.cuda_stream)
+    p_plain = ref.read_params(stream.cuda_stream)
+    ref.close()
+    assert rel_err(p_mixed[1], p_plain[1]) <= 1e-4

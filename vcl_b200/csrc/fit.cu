@@ -124,7 +124,8 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
         return vcl_fail(ctx, VCL_ERR_NOMEM, "fit arena of %zu bytes: %s", L.total, cudaGetErrorString(e));
     }
     f->arena_bytes = L.total;
-    plan(f->d, f, L);
+    Layout L2;
+    plan(f->d, f, L2);
     const vcl_fit_desc& d = f->d;
     const size_t N = (size_t)d.W * d.H * d.views;
     const size_t n0 = (size_t)d.tex_w * d.tex_h * d.C;
@@ -175,6 +176,11 @@ VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* f, int strategy) {
     if (!f) return VCL_ERR_ARG;
     vcl_ctx* ctx = f->ctx;
     VCL_REQUIRE(strategy == VCL_FIT_PLAIN || strategy == VCL_FIT_FUSED, "unknown strategy %d", strategy);
+    VCL_REQUIRE(strategy == VCL_FIT_PLAIN || f->d.C == 4, "the fused strategy needs C = 4 channels");
+    if (strategy == VCL_FIT_FUSED && f->strategy != VCL_FIT_FUSED) {
+        vcl_status st = fit_fused_sync_counter(f, true);
+        if (st) return st;
+    }
     f->strategy = strategy;
     return VCL_OK;
 }

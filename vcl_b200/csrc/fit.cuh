@@ -29,3 +29,4 @@ vcl_status fit_forward(vcl_fit* f, float* out, cudaStream_t s);
 int fit_plain_launches(const vcl_fit* f);
 int fit_fused_launches(const vcl_fit* f);
 void fit_fused_release(vcl_fit* f);
+vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device);

@@ -1,8 +1,615 @@
-// Fused fit iteration (placeholder until the fused kernels land).
+// Fused fit iteration.  Same operators and arithmetic as the plain path
+// (fit_plain.cu), regrouped so that per-pixel intermediates stay in
+// registers instead of round-tripping through HBM:
+//
+//   begin        device step counter, Adam bias corrections, loss := 0
+//   project      clip-space positions
+//   raster       setup / scan / emit / fine (own workspace)
+//   shade_fwd    interpolate(uv, DA) + texture + NormalAxis + ViewAxis +
+//                SGSpecular + SG per pixel -> color (and the AA input copy)
+//   aa edges     silhouette blending (atomics)
+//   mse_init     grad = aa - target, loss, and the AA-backward input copy
+//   aa edges bwd colour and clip-position gradients at silhouettes
+//   fused_bwd    per pixel: recompute the shading inputs, SG backward (lobe
+//                gradients block-reduced), texture backward (texel atomics),
+//                interpolate backward, raster backward (clip atomics)
+//   project bwd  position gradients
+//   adam_tex     mip gradient push-down + Adam + clamp on texture level 0,
+//                gradient clear, and mip levels 1..5 of each 32x32 tile
+//   mips         remaining coarse levels
+//   adam_small   Adam on positions and lobes, gradient clear
+//
+// On a non-default stream the whole step is captured once into a CUDA
+// graph and replayed (the step index lives in device memory, so the graph
+// never changes).
 #include "fit.cuh"
+#include "sg_math.cuh"
+#include "tex_math.cuh"
+#include "adam_math.cuh"
+#include "ops_internal.cuh"
 
-vcl_status fit_step_fused(vcl_fit* f, cudaStream_t) {
-    return vcl_fail(f->ctx, VCL_ERR_STATE, "fused strategy not built");
+namespace {
+
+struct Fused {
+    void* raster_ws = nullptr;
+    int tile = 16;
+    long long cap = 0;
+    int* d_step = nullptr;
+    double* d_corr = nullptr;    // 1 - beta1^t', 1 - beta2^t'
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    int graph_mode = -1;
+};
+
+DEV float mulr(float a, float b) { return __fmul_rn(a, b); }
+DEV float addr(float a, float b) { return __fadd_rn(a, b); }
+
+__global__ void k_begin(int* step, double* corr, double b1, double b2, int compat, float* loss) {
+    int t = ++*step;
+    double c1 = compat ? b1 : 1.0, c2 = compat ? b2 : 1.0;
+    for (int k = 0; k < t; ++k) { c1 *= b1; c2 *= b2; }
+    corr[0] = 1.0 - c1;
+    corr[1] = 1.0 - c2;
+    *loss = 0.f;
 }
-int fit_fused_launches(const vcl_fit*) { return 0; }
-void fit_fused_release(vcl_fit*) {}
+
+struct ShadeIn {
+    const float4* rast; const float4* db; const float* uvattr; const uint32_t* tri; int nt, nv;
+    const float* pyr; const float* rot; const float* nrm; const float* pvinv;
+    int W, H; long long npix; float rough, ior;
+    const float* axis; const float* sharp; const float* amp; int K, C;
+};
+
+// Everything the SG stage needs at one covered pixel, recomputed from the
+// raster output the way the plain operators compute it.
+struct PixIn {
+    float2 uv; float4 uvda; float4 dfs; float3 n, pax; float ss, sa;
+    uint32_t i0, i1, i2; float4 r;
+};
+
+template <int C4>
+DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o) {
+    float4 r = a.rast[p];
+    o.r = r;
+    int idx = rast_id(r.w);
+    if (idx < 0 || idx >= a.nt) return false;
+    uint32_t i0 = a.tri[3 * (size_t)idx], i1 = a.tri[3 * (size_t)idx + 1], i2 = a.tri[3 * (size_t)idx + 2];
+    if (i0 >= (uint32_t)a.nv || i1 >= (uint32_t)a.nv || i2 >= (uint32_t)a.nv) return false;
+    o.i0 = i0; o.i1 = i1; o.i2 = i2;
+    // interpolate.cu:38 and :40-47 (uv with screen derivatives)
+    float4 d = a.db[p];
+    double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
+    float u[2], dx[2], dy[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        float a0 = a.uvattr[2 * i0 + i], a1 = a.uvattr[2 * i1 + i], a2 = a.uvattr[2 * i2 + i];
+        u[i] = (float)__dadd_rn((double)addr(mulr(a0, r.x), mulr(a1, r.y)), __dmul_rn((double)a2, l2));
+        float dadu = a0 - a2, dadv = a1 - a2;
+        dx[i] = addr(mulr(dadu, d.x), mulr(dadv, d.z));
+        dy[i] = addr(mulr(dadu, d.y), mulr(dadv, d.w));
+    }
+    o.uv = make_float2(u[0], u[1]);
+    o.uvda = make_float4(dx[0], dy[0], dx[1], dy[1]);
+    // texturemap.cu:67-95
+    int l0 = 0, l1 = 0;
+    float fl = 0.f;
+    if (td.L > 1) calc_level(td, o.uvda, l0, l1, fl, nullptr, 0);
+    int q0[4];
+    float2 f0;
+    index_fetch(td, l0, o.uv, q0, f0);
+    const float* T0 = a.pyr + td.off[l0];
+    float4 c = bilerp4(ld4(T0, q0[0]), ld4(T0, q0[1]), ld4(T0, q0[2]), ld4(T0, q0[3]), f0);
+    if (td.L > 1 && fl > 0) {
+        int q1[4];
+        float2 f1;
+        index_fetch(td, l1, o.uv, q1, f1);
+        const float* T1 = a.pyr + td.off[l1];
+        float4 c1 = bilerp4(ld4(T1, q1[0]), ld4(T1, q1[1]), ld4(T1, q1[2]), ld4(T1, q1[3]), f1);
+        c = make_float4(lerpf_(c.x, c1.x, fl), lerpf_(c.y, c1.y, fl), lerpf_(c.z, c1.z, fl), lerpf_(c.w, c1.w, fl));
+    }
+    o.dfs = c;
+    // material.cu:36-47 (NormalAxis)
+    float3 n2 = ld3(a.nrm, i2);
+    float3 n0 = ld3(a.nrm, i0) - n2, n1 = ld3(a.nrm, i1) - n2;
+    float3 N = normalize3(n0 * r.x + n1 * r.y + n2);
+    const float* R = a.rot;
+    o.n = f3(R[0] * N.x + R[4] * N.y + R[8] * N.z, R[1] * N.x + R[5] * N.y + R[9] * N.z,
+             R[2] * N.x + R[6] * N.y + R[10] * N.z);
+    // material.cu:99-107 (ViewAxis)
+    long long hw = (long long)a.W * a.H;
+    int view = (int)(p / hw);
+    int rem = (int)(p - view * hw);
+    int py = rem / a.W, px = rem - py * a.W;
+    const float* M = a.pvinv + (size_t)view * 9;
+    float sx = (float)px / (float)a.W * 2.f - 1.f, sy = (float)py / (float)a.H * 2.f - 1.f;
+    float3 vw = normalize3(f3(M[0], M[1], M[2]) * sx + f3(M[3], M[4], M[5]) * sy + f3(M[6], M[7], M[8]));
+    // material.cu:155-182 (SGSpecular)
+    SpecLobe s = spec_eval(o.n, vw, a.rough, a.ior);
+    o.pax = s.p;
+    o.sa = s.F * s.Gp * s.Gv * s.pn / fmaxf(s.m2, 1e-6f);
+    o.ss = .5f / fmaxf(s.m2 * s.vn, 1e-6f);
+    return true;
+}
+
+// Forward shading of every pixel; writes the color and the antialias input
+// copy (antialias.cu:62-65).  C = 4 texture/lobe channels.
+__global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
+                                                   float4* __restrict__ aa) {
+    extern __shared__ float sm[];
+    const SGLobes L = sg_stage_lobes(sm, a.K, 4, a.axis, a.sharp, a.amp);
+    __syncthreads();
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.npix) return;
+    PixIn q;
+    if (!shade_inputs<1>(a, td, p, q)) {
+        color[p] = aa[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    float de[SG_CMAX], se[SG_CMAX];
+    sg_env<4>(L, a.K, 4, q.n, q.pax, q.ss, q.sa, de, se);
+    float4 c = make_float4(q.dfs.x * de[0] + se[0], q.dfs.y * de[1] + se[1], q.dfs.z * de[2] + se[2],
+                           q.dfs.w * de[3] + se[3]);
+    color[p] = c;
+    aa[p] = c;
+}
+
+// loss.cu:22-30 plus the antialias-backward input copy (antialias.cu:267-269).
+__global__ void k_mse_init(const float4* __restrict__ aa, const float4* __restrict__ tgt, long long n4,
+                           float4* __restrict__ g_aa, float4* __restrict__ g_color, float* __restrict__ loss) {
+    __shared__ double part[32];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        float4 a = aa[i], t = tgt[i];
+        float4 g = make_float4(a.x - t.x, a.y - t.y, a.z - t.z, a.w - t.w);
+        g_aa[i] = g;
+        g_color[i] = g;
+        acc += (double)g.x * g.x + (double)g.y * g.y + (double)g.z * g.z + (double)g.w * g.w;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (threadIdx.x == 0) atomicAdd(loss, (float)(acc * 0.5));
+    }
+}
+
+constexpr int FP = 2;   // pixels per thread in the fused backward
+
+// material.cu:369-438 -> texturemap.cu:229-284 -> interpolate.cu:114-143 ->
+// rasterize.cu:84-141 for the pixels of each thread, gradients scattered
+// with vector reductions.
+__global__ void __launch_bounds__(256, 2) k_fused_bwd(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+                                                   float* __restrict__ g_pyr, const float* __restrict__ clip,
+                                                   float* __restrict__ g_clip, float* __restrict__ g_axis,
+                                                   float* __restrict__ g_sharp, float* __restrict__ g_amp, int nacc,
+                                                   int want_tex, int want_geom) {
+    extern __shared__ float sm[];
+    const int nwarps = blockDim.x >> 5;
+    const int K = a.K;
+    const SGLobes L = sg_stage_lobes(sm, K, 4, a.axis, a.sharp, a.amp);
+    float* s_acc = sm + 8 * K;
+    const bool lobe_grads = g_axis != nullptr;
+    if (lobe_grads)
+        for (int i = threadIdx.x; i < nwarps * K * nacc; i += blockDim.x) s_acc[i] = 0.f;
+    __syncthreads();
+    float* wacc = s_acc + (size_t)(threadIdx.x >> 5) * K * nacc;
+    const long long span = (long long)blockDim.x * FP;
+    for (long long base = (long long)blockIdx.x * span; base < a.npix; base += (long long)gridDim.x * span) {
+        SGPix q[FP];
+        PixIn in[FP];
+        bool live[FP];
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < FP; ++j) {
+            long long p = base + threadIdx.x + (long long)j * blockDim.x;
+            live[j] = p < a.npix && shade_inputs<1>(a, td, p, in[j]);
+            any |= live[j];
+            SGPix& z = q[j];
+            z.gsx = f3(0.f, 0.f, 0.f); z.gsh = 0.f;
+#pragma unroll
+            for (int k = 0; k < SG_CMAX; ++k) { z.dfs[k] = 0.f; z.go[k] = 0.f; z.gd[k] = 0.f; z.gsa[k] = 0.f; }
+            z.n = z.pax = f3(0.f, 0.f, 0.f); z.ss = z.sa = 0.f;
+            if (live[j]) {
+                z.n = in[j].n; z.pax = in[j].pax; z.ss = in[j].ss; z.sa = in[j].sa;
+                z.dfs[0] = in[j].dfs.x; z.dfs[1] = in[j].dfs.y; z.dfs[2] = in[j].dfs.z; z.dfs[3] = in[j].dfs.w;
+                float4 g = g_color[p];
+                z.go[0] = g.x; z.go[1] = g.y; z.go[2] = g.z; z.go[3] = g.w;
+            }
+        }
+        if (!__any_sync(0xffffffffu, any)) continue;
+        sg_bwd_block<FP, 4>(L, K, 4, 0, q, live, wacc, nacc, lobe_grads, false);
+        if (!want_tex && !want_geom) continue;
+#pragma unroll
+        for (int j = 0; j < FP; ++j) {
+            if (!live[j]) continue;
+            const long long p = base + threadIdx.x + (long long)j * blockDim.x;
+            const PixIn& I = in[j];
+            const float4 g = make_float4(q[j].gd[0], q[j].gd[1], q[j].gd[2], q[j].gd[3]);
+            // texture backward (texturemap.cu:229-284)
+            int l0 = 0, l1 = 0;
+            float fl = 0.f;
+            if (td.L > 1) calc_level(td, I.uvda, l0, l1, fl, nullptr, 0);
+            const bool mip = td.L > 1;
+            int q0[4], q1[4];
+            float2 f0, f1 = make_float2(0.f, 0.f);
+            index_fetch(td, l0, I.uv, q0, f0);
+            const bool tri = mip && fl > 0;
+            if (tri) index_fetch(td, l1, I.uv, q1, f1);
+            const float wl0 = mip ? 1.f - fl : 1.f;
+            if (want_tex) {
+                float* G0 = g_pyr + td.off[l0];
+                float w00 = wl0 * (1.f - f0.x) * (1.f - f0.y), w01 = wl0 * f0.x * (1.f - f0.y);
+                float w10 = wl0 * (1.f - f0.x) * f0.y, w11 = wl0 * f0.x * f0.y;
+                red_add4(G0 + 4 * q0[0], w00 * g.x, w00 * g.y, w00 * g.z, w00 * g.w);
+                red_add4(G0 + 4 * q0[1], w01 * g.x, w01 * g.y, w01 * g.z, w01 * g.w);
+                red_add4(G0 + 4 * q0[2], w10 * g.x, w10 * g.y, w10 * g.z, w10 * g.w);
+                red_add4(G0 + 4 * q0[3], w11 * g.x, w11 * g.y, w11 * g.z, w11 * g.w);
+                if (tri) {
+                    float* G1 = g_pyr + td.off[l1];
+                    float v00 = fl * (1.f - f1.x) * (1.f - f1.y), v01 = fl * f1.x * (1.f - f1.y);
+                    float v10 = fl * (1.f - f1.x) * f1.y, v11 = fl * f1.x * f1.y;
+                    red_add4(G1 + 4 * q1[0], v00 * g.x, v00 * g.y, v00 * g.z, v00 * g.w);
+                    red_add4(G1 + 4 * q1[1], v01 * g.x, v01 * g.y, v01 * g.z, v01 * g.w);
+                    red_add4(G1 + 4 * q1[2], v10 * g.x, v10 * g.y, v10 * g.z, v10 * g.w);
+                    red_add4(G1 + 4 * q1[3], v11 * g.x, v11 * g.y, v11 * g.z, v11 * g.w);
+                }
+            }
+            if (!want_geom) continue;
+            const float* T0 = a.pyr + td.off[l0];
+            const float* T1 = a.pyr + td.off[l1];
+            const float s0x = (float)(td.tw >> l0), s0y = (float)(td.th >> l0);
+            const float s1x = (float)(td.tw >> l1), s1y = (float)(td.th >> l1);
+            float4 a00 = ld4(T0, q0[0]), a01 = ld4(T0, q0[1]), a10 = ld4(T0, q0[2]), a11 = ld4(T0, q0[3]);
+            float4 b00 = a00, b01 = a00, b10 = a00, b11 = a00;
+            if (tri) { b00 = ld4(T1, q1[0]); b01 = ld4(T1, q1[1]); b10 = ld4(T1, q1[2]); b11 = ld4(T1, q1[3]); }
+            float gu = 0.f, gv = 0.f;
+            const float ga[4] = {g.x, g.y, g.z, g.w};
+            const float A00[4] = {a00.x, a00.y, a00.z, a00.w}, A01[4] = {a01.x, a01.y, a01.z, a01.w};
+            const float A10[4] = {a10.x, a10.y, a10.z, a10.w}, A11[4] = {a11.x, a11.y, a11.z, a11.w};
+            const float B00[4] = {b00.x, b00.y, b00.z, b00.w}, B01[4] = {b01.x, b01.y, b01.z, b01.w};
+            const float B10[4] = {b10.x, b10.y, b10.z, b10.w}, B11[4] = {b11.x, b11.y, b11.z, b11.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], f0.y) * s0x;
+                float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], f0.x) * s0y;
+                if (tri) {
+                    du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], f1.y) * s1x, fl);
+                    dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], f1.x) * s1y, fl);
+                }
+                gu += du * ga[i];
+                gv += dv * ga[i];
+            }
+            // interpolate backward to the barycentrics (interpolate.cu:133-141)
+            float gbu = 0.f, gbv = 0.f;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                float gi = i == 0 ? gu : gv;
+                float a2 = a.uvattr[2 * I.i2 + i];
+                gbu += gi * (a.uvattr[2 * I.i0 + i] - a2);
+                gbv += gi * (a.uvattr[2 * I.i1 + i] - a2);
+            }
+            if (((__float_as_uint(gbu) | __float_as_uint(gbv)) << 1) == 0u) continue;
+            // raster backward (rasterize.cu:84-141)
+            long long hw = (long long)a.W * a.H;
+            int view = (int)(p / hw);
+            int rem = (int)(p - view * hw);
+            int py = rem / a.W, px = rem - py * a.W;
+            const float xs = 2.f / (float)a.W, ys = 2.f / (float)a.H;
+            float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
+            float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
+            const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * a.nv;
+            float4 c0 = cv[I.i0], c1 = cv[I.i1], c2 = cv[I.i2];
+            float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
+            float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
+            float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
+            float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
+            float ar = e0x * e1y - e0y * e1x;
+            float ia = 1.f / (ar + (ar > 0 ? 1e-6f : -1e-6f));
+            float kuv = I.r.x * gbu + I.r.y * gbv;
+            float gx0 = (gbv * p2y + kuv * e1y) * ia, gy0 = (-gbv * p2x - kuv * e1x) * ia;
+            float gx1 = (-gbu * p2y - kuv * e0y) * ia, gy1 = (gbu * p2x + kuv * e0x) * ia;
+            float gx2 = ((-gbv * p0y + gbu * p1y) - kuv * (-p0y + p1y)) * ia;
+            float gy2 = ((gbv * p0x - gbu * p1x) - kuv * (p0x - p1x)) * ia;
+            float* gcv = g_clip + (size_t)view * a.nv * 4;
+            red_add4(gcv + (size_t)I.i0 * 4, gx0, gy0, 0.f, -gx0 * pxn - gy0 * pyn);
+            red_add4(gcv + (size_t)I.i1 * 4, gx1, gy1, 0.f, -gx1 * pxn - gy1 * pyn);
+            red_add4(gcv + (size_t)I.i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
+        }
+    }
+    if (!lobe_grads) return;
+    __syncthreads();
+    sg_flush_lobes(s_acc, nwarps, K, 4, nacc, g_axis, g_sharp, g_amp, nullptr);
+}
+
+DEV float4 nan_add4(float4 a, float4 b) {
+    add_nan_check(a.x, b.x); add_nan_check(a.y, b.y); add_nan_check(a.z, b.z); add_nan_check(a.w, b.w);
+    return a;
+}
+DEV float4 mul4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+DEV float4 avg4(float4 a, float4 b, float4 c, float4 d) {
+    return make_float4(addr(addr(addr(a.x, b.x), c.x), d.x) * 0.25f, addr(addr(addr(a.y, b.y), c.y), d.y) * 0.25f,
+                       addr(addr(addr(a.z, b.z), c.z), d.z) * 0.25f, addr(addr(addr(a.w, b.w), c.w), d.w) * 0.25f);
+}
+DEV float clamp01(float x) { return x < 0.f ? 0.f : x > 1.f ? 1.f : x; }
+
+struct AdamArgs {
+    double b1, b2, lr, eps;
+    const double* corr;
+};
+
+// TextureGrad::gradSumup (buffer.cu:615-648) folded into level 0, Adam
+// (optimize.cu:95-106), clamp (buffer.cu:65-72), gradient clear, and the
+// 2x2 mip chain (buffer.cu:449-472) of each 32x32 level-0 tile up to level
+// `top` (<= 5).  One thread per 2x2 level-0 quad; C = 4.
+__global__ void __launch_bounds__(256) k_adam_tex_tile(TexDesc td, float* __restrict__ pyr, float* __restrict__ gpyr,
+                                                       float* __restrict__ m, float* __restrict__ v, AdamArgs aa,
+                                                       float wpush, int top) {
+    __shared__ float4 s_lvl[16][16];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x = blockIdx.x * 16 + tx, y = blockIdx.y * 16 + ty;     // level-1 texel = level-0 quad
+    const int W0 = td.tw, L = td.L;
+    // pushed-down gradient of the quad's level-1 ancestor chain
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (L > 1) {
+        t = ld4(gpyr + td.off[L - 1], (y >> (L - 2)) * (td.tw >> (L - 1)) + (x >> (L - 2)));
+        for (int k = L - 2; k >= 1; --k)
+            t = nan_add4(ld4(gpyr + td.off[k], (y >> (k - 1)) * (td.tw >> k) + (x >> (k - 1))), mul4(t, wpush));
+    }
+    const double c1 = aa.corr[0], c2 = aa.corr[1];
+    float4 out[4];
+#pragma unroll
+    for (int qd = 0; qd < 4; ++qd) {
+        const int X = 2 * x + (qd & 1), Y = 2 * y + (qd >> 1);
+        const size_t ti = (size_t)Y * W0 + X;
+        float4 g = ld4(gpyr, (int)ti);
+        if (L > 1) g = nan_add4(g, mul4(t, wpush));
+        float4 P = ld4(pyr, (int)ti), M = ld4(m, (int)ti), V = ld4(v, (int)ti);
+        adam_one(P.x, g.x, M.x, V.x, aa.b1, aa.b2, aa.lr, aa.eps, c1, c2);
+        adam_one(P.y, g.y, M.y, V.y, aa.b1, aa.b2, aa.lr, aa.eps, c1, c2);
+        adam_one(P.z, g.z, M.z, V.z, aa.b1, aa.b2, aa.lr, aa.eps, c1, c2);
+        adam_one(P.w, g.w, M.w, V.w, aa.b1, aa.b2, aa.lr, aa.eps, c1, c2);
+        P = make_float4(clamp01(P.x), clamp01(P.y), clamp01(P.z), clamp01(P.w));
+        reinterpret_cast<float4*>(pyr)[ti] = P;
+        reinterpret_cast<float4*>(m)[ti] = M;
+        reinterpret_cast<float4*>(v)[ti] = V;
+        reinterpret_cast<float4*>(gpyr)[ti] = make_float4(0.f, 0.f, 0.f, 0.f);
+        out[qd] = P;
+    }
+    if (top < 1) return;
+    float4 l1 = avg4(out[0], out[1], out[2], out[3]);
+    reinterpret_cast<float4*>(pyr + td.off[1])[(size_t)y * (W0 >> 1) + x] = l1;
+    s_lvl[ty][tx] = l1;
+    __syncthreads();
+    for (int k = 2, n = 8; k <= top; ++k, n >>= 1) {
+        float4 r;
+        const bool act = tx < n && ty < n;
+        if (act) r = avg4(s_lvl[2 * ty][2 * tx], s_lvl[2 * ty][2 * tx + 1], s_lvl[2 * ty + 1][2 * tx],
+                          s_lvl[2 * ty + 1][2 * tx + 1]);
+        __syncthreads();
+        if (act) {
+            s_lvl[ty][tx] = r;
+            const int X = blockIdx.x * n + tx, Y = blockIdx.y * n + ty;
+            reinterpret_cast<float4*>(pyr + td.off[k])[(size_t)Y * (W0 >> k) + X] = r;
+        }
+        __syncthreads();
+    }
+}
+
+// The same optimizer pass for any channel count / size, one thread per
+// level-0 texel channel (no mip chain).
+__global__ void k_adam_tex_generic(TexDesc td, float* __restrict__ pyr, float* __restrict__ gpyr, float* __restrict__ m,
+                                   float* __restrict__ v, AdamArgs aa, float wpush) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int C = td.C;
+    long long n0 = (long long)td.tw * td.th * C;
+    if (i >= n0) return;
+    int c = (int)(i % C);
+    long long t = i / C;
+    int X = (int)(t % td.tw), Y = (int)(t / td.tw);
+    float g = gpyr[i];
+    if (td.L > 1) {
+        int L = td.L;
+        float tv = gpyr[td.off[L - 1] + ((long long)(Y >> (L - 1)) * (td.tw >> (L - 1)) + (X >> (L - 1))) * C + c];
+        for (int k = L - 2; k >= 1; --k) {
+            float gk = gpyr[td.off[k] + ((long long)(Y >> k) * (td.tw >> k) + (X >> k)) * C + c];
+            add_nan_check(gk, tv * wpush);
+            tv = gk;
+        }
+        add_nan_check(g, tv * wpush);
+    }
+    float P = pyr[i], M = m[i], V = v[i];
+    adam_one(P, g, M, V, aa.b1, aa.b2, aa.lr, aa.eps, aa.corr[0], aa.corr[1]);
+    pyr[i] = clamp01(P);
+    m[i] = M;
+    v[i] = V;
+    gpyr[i] = 0.f;
+}
+
+// Adam on positions then lobes (one flat index space), gradient clear.
+__global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, float* __restrict__ mv0, long long n0,
+                             float* __restrict__ p1, float* __restrict__ g1, float* __restrict__ mv1, long long n1,
+                             AdamArgs aa) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float *p, *g, *m, *v;
+    long long j;
+    if (i < n0) { p = p0; g = g0; m = mv0; v = mv0 + n0; j = i; }
+    else if (i < n0 + n1) { p = p1; g = g1; m = mv1; v = mv1 + n1; j = i - n0; }
+    else return;
+    float P = p[j], M = m[j], V = v[j];
+    adam_one(P, g[j], M, V, aa.b1, aa.b2, aa.lr, aa.eps, aa.corr[0], aa.corr[1]);
+    p[j] = P; m[j] = M; v[j] = V; g[j] = 0.f;
+}
+
+#define TRY(x) do { vcl_status _s = (x); if (_s) return _s; } while (0)
+
+size_t shade_smem(int K) { return sizeof(float) * (size_t)K * 8; }
+size_t bwd_smem(int K, int nacc) { return sizeof(float) * ((size_t)K * 8 + (size_t)8 * K * nacc); }
+
+vcl_status fused_init(vcl_fit* f) {
+    if (f->fused) return VCL_OK;
+    vcl_ctx* ctx = f->ctx;
+    const vcl_fit_desc& d = f->d;
+    Fused* F = new Fused();
+    F->tile = ctx->tile;
+    F->cap = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(d.views, d.nt, d.W, d.H, F->tile);
+    size_t ws = raster_ws_size(d.W, d.H, d.views, d.nt, F->tile, F->cap);
+    cudaError_t e = cudaMalloc(&F->raster_ws, ws);
+    if (e == cudaSuccess) e = cudaMalloc(&F->d_step, 64);
+    if (e == cudaSuccess) e = cudaMalloc(&F->d_corr, 64);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        if (F->raster_ws) cudaFree(F->raster_ws);
+        if (F->d_step) cudaFree(F->d_step);
+        delete F;
+        return vcl_fail(ctx, VCL_ERR_NOMEM, "fused fit state: %s", cudaGetErrorString(e));
+    }
+    f->fused = F;
+    const int nacc = 4 + 4 + 1;
+    size_t sb = bwd_smem(d.K, nacc);
+    if (sb > 48 * 1024) cudaFuncSetAttribute(k_fused_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    size_t sf = shade_smem(d.K);
+    if (sf > 48 * 1024) cudaFuncSetAttribute(k_shade_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
+    return vcl_cuda_check(ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice), "fused init");
+}
+
+vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
+    vcl_ctx* ctx = f->ctx;
+    Fused* F = (Fused*)f->fused;
+    const vcl_fit_desc& d = f->d;
+    const int W = d.W, H = d.H, V = d.views;
+    const long long N = (long long)W * H * V;
+    const size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, 4, d.levels);
+    const size_t n0 = (size_t)d.tex_w * d.tex_h * 4;
+    const int compat = ctx->mode == VCL_MODE_COMPAT;
+    k_begin<<<1, 1, 0, s>>>(F->d_step, F->d_corr, d.beta1, d.beta2, compat, f->loss);
+    TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_clip, 0, sizeof(float) * V * d.nv * 4, s), "clear"));
+    if (npyr > n0) TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_pyr + n0, 0, sizeof(float) * (npyr - n0), s), "clear"));
+    TRY(vcl_project_fwd(ctx, f->mvp, V, f->pos, d.nv, 4, f->clip, s));
+    TRY(raster_fwd_ws(ctx, F->raster_ws, F->tile, F->cap, f->clip, d.nv, f->tri, d.nt, W, H, V, f->rast, f->db, s));
+    ShadeIn a;
+    a.rast = (const float4*)f->rast; a.db = (const float4*)f->db; a.uvattr = f->uvattr; a.tri = f->tri;
+    a.nt = d.nt; a.nv = d.nv; a.pyr = f->pyr; a.rot = f->rot; a.nrm = f->nrmattr; a.pvinv = f->pvinv;
+    a.W = W; a.H = H; a.npix = N; a.rough = d.roughness; a.ior = d.ior;
+    a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
+    TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
+    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->aa);
+    TRY(vcl_launch_check(ctx, "fused shade"));
+    TRY(aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
+    int grid = ctx->sm_count * 4;
+    k_mse_init<<<grid, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N, (float4*)f->g_aa,
+                                    (float4*)f->g_color, f->loss);
+    TRY(vcl_launch_check(ctx, "fused mse"));
+    TRY(aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
+                     d.learn_pos ? f->g_clip : nullptr, s));
+    const bool lobes = d.learn_lobes && d.K;
+    const int nacc = 4 + 4 + 1;
+    long long blocks = (N + 256 * FP - 1) / (256 * FP);
+    int bgrid = (int)(blocks < ctx->sm_count * 2 ? (blocks < 1 ? 1 : blocks) : ctx->sm_count * 2);
+    k_fused_bwd<<<bgrid, 256, bwd_smem(d.K, nacc), s>>>(a, td, (const float4*)f->g_color, f->g_pyr, f->clip, f->g_clip,
+                                                        lobes ? f->g_axis : nullptr, lobes ? f->g_sharp : nullptr,
+                                                        lobes ? f->g_amp : nullptr, nacc, d.learn_tex, d.learn_pos);
+    TRY(vcl_launch_check(ctx, "fused backward"));
+    if (d.learn_pos) TRY(vcl_project_bwd(ctx, f->mvp, V, f->g_clip, d.nv, 4, f->g_pos, s));
+    AdamArgs aa{d.beta1, d.beta2, d.lr, d.eps, F->d_corr};
+    const float wpush = ctx->mode == VCL_MODE_EXACT ? 0.25f : 1.f;
+    if (d.learn_tex) {
+        const bool tile = d.tex_w % 32 == 0 && d.tex_h % 32 == 0 && d.levels >= 2;
+        if (tile) {
+            int top = d.levels - 1 < 5 ? d.levels - 1 : 5;
+            dim3 g(d.tex_w / 32, d.tex_h / 32);
+            k_adam_tex_tile<<<g, 256, 0, s>>>(td, f->pyr, f->g_pyr, f->mv_tex, f->mv_tex + n0, aa, wpush, top);
+            TRY(vcl_launch_check(ctx, "fused adam texture"));
+            for (int l = top + 1; l < d.levels; ++l)
+                launch_mip_down(f->pyr + vcl_tex_level_offset(d.tex_w, d.tex_h, 4, l - 1),
+                                f->pyr + vcl_tex_level_offset(d.tex_w, d.tex_h, 4, l), d.tex_w >> l, d.tex_h >> l, 4, s);
+        } else {
+            k_adam_tex_generic<<<vcl_blocks((long long)n0, 256), 256, 0, s>>>(td, f->pyr, f->g_pyr, f->mv_tex,
+                                                                               f->mv_tex + n0, aa, wpush);
+            for (int l = 1; l < d.levels; ++l)
+                launch_mip_down(f->pyr + vcl_tex_level_offset(d.tex_w, d.tex_h, 4, l - 1),
+                                f->pyr + vcl_tex_level_offset(d.tex_w, d.tex_h, 4, l), d.tex_w >> l, d.tex_h >> l, 4, s);
+        }
+        TRY(vcl_launch_check(ctx, "fused mips"));
+    }
+    long long np = d.learn_pos ? (long long)d.nv * 3 : 0;
+    long long nl = lobes ? (long long)d.K * 8 : 0;
+    if (np + nl > 0) {
+        k_adam_small<<<vcl_blocks(np + nl, 256), 256, 0, s>>>(f->pos, f->g_pos, f->mv_pos, np, f->lobe, f->g_lobe,
+                                                              f->mv_lobe, nl, aa);
+        TRY(vcl_launch_check(ctx, "fused adam"));
+    }
+    return VCL_OK;
+}
+
+}  // namespace
+
+vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(f->d.C == 4, "the fused strategy needs C = 4 channels (got %d)", f->d.C);
+    vcl_status st = fused_init(f);
+    if (st) return st;
+    Fused* F = (Fused*)f->fused;
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+        st = enqueue(f, s);
+        if (!st) ++f->step_count;
+        return st;
+    }
+    if (!F->graph || F->graph_stream != s || F->graph_mode != ctx->mode) {
+        if (F->graph) { cudaGraphExecDestroy(F->graph); F->graph = nullptr; }
+        st = vcl_cuda_check(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        if (st) return st;
+        vcl_status est = enqueue(f, s);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (est) { if (g) cudaGraphDestroy(g); return est; }
+        st = vcl_cuda_check(ctx, e, "graph capture end");
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        e = cudaGraphInstantiate(&F->graph, g, 0);
+        cudaGraphDestroy(g);
+        st = vcl_cuda_check(ctx, e, "graph instantiate");
+        if (st) { F->graph = nullptr; return st; }
+        F->graph_stream = s;
+        F->graph_mode = ctx->mode;
+    }
+    st = vcl_cuda_check(ctx, cudaGraphLaunch(F->graph, s), "graph launch");
+    if (!st) ++f->step_count;
+    return st;
+}
+
+int fit_fused_launches(const vcl_fit* f) {
+    const vcl_fit_desc& d = f->d;
+    int n = 1 /* begin */ + 1 /* project */ + raster_fwd_launches() + 1 /* shade */ + 1 /* aa */ + 1 /* mse */ +
+            1 /* aa bwd */ + 1 /* fused bwd */;
+    if (d.learn_pos) n += 1;
+    if (d.learn_tex) {
+        const bool tile = d.tex_w % 32 == 0 && d.tex_h % 32 == 0 && d.levels >= 2;
+        int top = d.levels - 1 < 5 ? d.levels - 1 : 5;
+        n += 1 + (tile ? d.levels - 1 - top : d.levels - 1);
+    }
+    if (d.learn_pos || (d.learn_lobes && d.K)) n += 1;
+    return n;
+}
+
+void fit_fused_release(vcl_fit* f) {
+    Fused* F = (Fused*)f->fused;
+    if (!F) return;
+    if (F->graph) cudaGraphExecDestroy(F->graph);
+    if (F->raster_ws) cudaFree(F->raster_ws);
+    if (F->d_step) cudaFree(F->d_step);
+    if (F->d_corr) cudaFree(F->d_corr);
+    delete F;
+    f->fused = nullptr;
+}
+
+// Keeps the device step counter of the fused path and the host counter of
+// the plain path in agreement when the strategy changes.
+vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device) {
+    Fused* F = (Fused*)f->fused;
+    if (!F) return VCL_OK;
+    if (to_device)
+        return vcl_cuda_check(f->ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice),
+                              "step counter");
+    return VCL_OK;
+}

@@ -5,6 +5,9 @@
 // count allows.  Gradient scatters use FP32 vector reductions
 // (red.global.add.v4.f32 / .v2.f32, sm_90+).
 #include "common.cuh"
+#include "tex_math.cuh"
+#include "adam_math.cuh"
+#include "ops_internal.cuh"
 
 namespace {
 
@@ -22,7 +25,9 @@ __global__ void k_project_fwd(const float* __restrict__ mats, int views, const f
     const float* m = mats + (size_t)view * 16;
     float x = pos[3 * (size_t)p], y = pos[3 * (size_t)p + 1], z = pos[3 * (size_t)p + 2];
     float* o = out + (size_t)gid * dim;
-    for (int i = 0; i < dim; ++i) o[i] = m[i] * x + m[4 + i] * y + m[8 + i] * z + m[12 + i];
+    // exactly rounded, as the CPU restatement: triangle ids downstream are
+    // sensitive to the last bit of clip-space positions
+    for (int i = 0; i < dim; ++i) o[i] = add(add(add(mul(m[i], x), mul(m[4 + i], y)), mul(m[8 + i], z)), m[12 + i]);
 }
 
 // project.cu:71-88; one thread per vertex sums its views (no atomics)
@@ -120,70 +125,6 @@ __global__ void k_interp_bwd(const float4* __restrict__ rast, const float* __res
         else gbary[p] = make_float2(gu, gv);
     }
 }
-
-// -------------------------------------------------------------- texture
-struct TexDesc {
-    int tw, th, C, L;
-    long long off[16];
-};
-
-// texturemap.cu:22-47 (level) and :160-197 (level + Jacobian); the level
-// arithmetic is rounded exactly like the CPU restatement so that the same
-// mip levels are chosen.
-DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, float4* dl, int exact) {
-    float dsdx = mul(da.x, (float)t.tw), dsdy = mul(da.y, (float)t.tw);
-    float dtdx = mul(da.z, (float)t.th), dtdy = mul(da.w, (float)t.th);
-    float s2 = add(mul(dsdx, dsdx), mul(dsdy, dsdy));
-    float t2 = add(mul(dtdx, dtdx), mul(dtdy, dtdy));
-    float a = sub(mul(dsdx, dtdy), mul(dtdx, dsdy));
-    float b = mul(.5f, add(s2, t2));
-    float c2 = sub(mul(b, b), mul(a, a));
-    float c = sqrtf(c2);
-    float level = mul(.5f, log2f(add(b, c)));
-    const int L = t.L;
-    l0 = level <= 0 ? 0 : (float)(L - 2) <= level ? L - 2 : (int)floorf(level);
-    l1 = level <= 1 ? 1 : (float)(L - 1) <= level ? L - 1 : (int)floorf(level) + 1;
-    fl = level <= 0 ? 0.f : (float)(L - 1) <= level ? 1.f : level - floorf(level);
-    if (dl) {
-        float d = b * c + c2;
-        if ((double)fabsf(d) > 1e-6) {
-            d = 0.72134752f / d;
-            float bc = b + c;
-            *dl = make_float4(d * (bc * dsdx - a * dtdy), d * (bc * dsdy + a * dtdx), bc * dtdx + a * dsdy,
-                              bc * dtdy - a * dsdx);
-            if (exact) { dl->z *= d; dl->w *= d; }
-        } else if ((double)fabsf(b) > 1e-6) {
-            d = 1 / b;
-            *dl = make_float4(d * dsdx, d * dsdy, d * dtdx, d * dtdy);
-        } else {
-            *dl = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    }
-}
-
-// texturemap.cu:49-65
-DEV void index_fetch(const TexDesc& t, int level, float2 uv, int idx[4], float2& f) {
-    int sx = t.tw >> level, sy = t.th >> level;
-    float tx = uv.x * (float)sx, ty = uv.y * (float)sy;
-    int u0 = tx < 0 ? 0 : tx > (float)(sx - 1) ? sx - 1 : (int)tx;
-    int u1 = tx < 1 ? 0 : tx > (float)(sx - 2) ? sx - 1 : (int)tx + 1;
-    int v0 = ty < 0 ? 0 : ty > (float)(sy - 1) ? sy - 1 : (int)ty;
-    int v1 = ty < 1 ? 0 : ty > (float)(sy - 2) ? sy - 1 : (int)ty + 1;
-    idx[0] = v0 * sx + u0; idx[1] = v0 * sx + u1; idx[2] = v1 * sx + u0; idx[3] = v1 * sx + u1;
-    f.x = tx < 0 ? 0.f : (float)sx < tx ? 1.f : tx - floorf(tx);
-    f.y = ty < 0 ? 0.f : (float)sy < ty ? 1.f : ty - floorf(ty);
-}
-
-DEV float4 ld4(const float* p, int i) { return reinterpret_cast<const float4*>(p)[i]; }
-DEV float4 bilerp4(float4 a, float4 b, float4 c, float4 d, float2 t) {
-    float4 r;
-    r.x = lerpf_(lerpf_(a.x, b.x, t.x), lerpf_(c.x, d.x, t.x), t.y);
-    r.y = lerpf_(lerpf_(a.y, b.y, t.x), lerpf_(c.y, d.y, t.x), t.y);
-    r.z = lerpf_(lerpf_(a.z, b.z, t.x), lerpf_(c.z, d.z, t.x), t.y);
-    r.w = lerpf_(lerpf_(a.w, b.w, t.x), lerpf_(c.w, d.w, t.x), t.y);
-    return r;
-}
-DEV float bilerp1(float a, float b, float c, float d, float2 t) { return lerpf_(lerpf_(a, b, t.x), lerpf_(c, d, t.x), t.y); }
 
 // texturemap.cu:67-114
 template <int C4>
@@ -548,16 +489,6 @@ __global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ 
 }
 
 // ----------------------------------------------------------------- adam
-// optimize.cu:95-106: moments rounded to FP32, update in FP64, NaN-guarded.
-DEV void adam_one(float& p, float g, float& m, float& v, double b1, double b2, double lr, double eps, double c1,
-                  double c2) {
-    m = (float)__dadd_rn(__dmul_rn(b1, (double)m), __dmul_rn(1.0 - b1, (double)g));
-    v = (float)__dadd_rn(__dmul_rn(b2, (double)v), __dmul_rn(__dmul_rn(1.0 - b2, (double)g), (double)g));
-    double mh = (double)m / c1;
-    double vh = (double)v / c2;
-    add_nan_check(p, (float)(-mh * lr / (sqrt(vh) + eps)));
-}
-
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
                        long long n, double b1, double b2, double lr, double eps, double c1, double c2, int vec) {
     long long n4 = vec ? n / 4 : 0;
@@ -577,17 +508,6 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
-TexDesc make_desc(int tw, int th, int C, int L) {
-    TexDesc d;
-    d.tw = tw; d.th = th; d.C = C; d.L = L;
-    long long off = 0;
-    for (int l = 0; l < 16; ++l) {
-        d.off[l] = off;
-        if (l < L) off += (long long)(tw >> l) * (th >> l) * C;
-    }
-    return d;
-}
-
 int grid_for(long long n, int threads, int sm) {
     long long b = (n + threads - 1) / threads;
     long long cap = (long long)sm * 8;
@@ -595,6 +515,36 @@ int grid_for(long long n, int threads, int sm) {
 }
 
 }  // namespace
+
+vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
+                        int H, int views, int C, const float* in, float* out, cudaStream_t s) {
+    long long npix = (long long)W * H * views;
+    if (C == 4 && aligned16(in) && aligned16(out))
+        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, out, ctx->dev_flags);
+    else
+        k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, out, ctx->dev_flags);
+    return vcl_launch_check(ctx, "antialias_fwd");
+}
+
+vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
+                        int H, int views, int C, const float* in, const float* grad_out, float* grad_in,
+                        float* grad_clip, cudaStream_t s) {
+    long long npix = (long long)W * H * views;
+    int exact = ctx->mode == VCL_MODE_EXACT;
+    if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in))
+        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+    else
+        k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
+                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+    return vcl_launch_check(ctx, "antialias_bwd");
+}
+
+void launch_mip_down(const float* src, float* dst, int w, int h, int C, cudaStream_t s) {
+    k_mip_down<<<vcl_blocks((long long)w * h, 256), 256, 0, s>>>(src, dst, w, h, C);
+}
 
 extern "C" {
 
@@ -754,13 +704,7 @@ VCL_API vcl_status vcl_antialias_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(out, in, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s),
                                    "antialias copy");
     if (st) return st;
-    if (C == 4 && aligned16(in) && aligned16(out))
-        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, out, ctx->dev_flags);
-    else
-        k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, out, ctx->dev_flags);
-    return vcl_launch_check(ctx, "antialias_fwd");
+    return aa_edges_fwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, out, s);
 }
 
 VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
@@ -776,14 +720,7 @@ VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, co
     vcl_status st = vcl_cuda_check(
         ctx, cudaMemcpyAsync(grad_in, grad_out, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s), "antialias copy");
     if (st) return st;
-    int exact = ctx->mode == VCL_MODE_EXACT;
-    if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in))
-        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
-    else
-        k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
-    return vcl_launch_check(ctx, "antialias_bwd");
+    return aa_edges_bwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, grad_out, grad_in, grad_clip, s);
 }
 
 VCL_API vcl_status vcl_mse(vcl_ctx* ctx, const float* pred, const float* target, size_t n, float* grad, float* loss_dev,

@@ -1,0 +1,21 @@
+// Internal launchers shared by the C-ABI operators and the fused fit path.
+#pragma once
+#include "common.cuh"
+
+// Antialias edge passes only (the caller has already initialised `out` /
+// `grad_in`, antialias.cu:62-65 / :267-269).
+vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
+                        int H, int views, int C, const float* in, float* out, cudaStream_t s);
+vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
+                        int H, int views, int C, const float* in, const float* grad_out, float* grad_in,
+                        float* grad_clip, cudaStream_t s);
+// Mip level l from level l-1 (buffer.cu:449-472).
+void launch_mip_down(const float* src, float* dst, int w, int h, int C, cudaStream_t s);
+
+// Rasterizer with a caller-owned workspace (a fit job owns one, so that a
+// captured graph never points into a workspace that another call regrows).
+long long raster_auto_capacity(long long views, long long nt, int W, int H, int tile);
+size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap);
+vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int tile, long long cap, const float* clip, int nv,
+                         const uint32_t* tri, int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s);
+int raster_fwd_launches();

@@ -23,6 +23,7 @@
 // restatement of the same rules: triangle ids, barycentrics and depth match
 // exactly.
 #include "common.cuh"
+#include "ops_internal.cuh"
 
 namespace {
 
@@ -208,14 +209,15 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
     const RTri* vs = setup + (size_t)view * nt;
     float best_z = 1.f;
     int best_t = -1;
-    for (int i0 = 0; i0 < n_iter; i0 += CHUNK) {
-        if (tid < CHUNK && i0 + tid < n_iter) {
+    constexpr int CH = T * T < CHUNK ? T * T : CHUNK;   // records staged per pass (<= threads)
+    for (int i0 = 0; i0 < n_iter; i0 += CH) {
+        if (tid < CH && i0 + tid < n_iter) {
             int t = overflow ? i0 + tid : list[off + i0 + tid];
             s_id[tid] = t;
             s_tri[tid] = vs[t];
         }
         __syncthreads();
-        const int m = min(CHUNK, n_iter - i0);
+        const int m = min(CH, n_iter - i0);
         if (inside) {
             for (int j = 0; j < m; ++j) {
                 const int4 box = s_tri[j].box;
@@ -316,7 +318,7 @@ struct RasterWS {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-long long auto_capacity(long long views, long long nt, int W, int H, int tile) {
+long long auto_capacity_(long long views, long long nt, int W, int H, int tile) {
     long long ntiles = (long long)((W + tile - 1) / tile) * ((H + tile - 1) / tile) * views;
     long long c = views * nt * 6 + ntiles * 4 + (1 << 20);
     return c > (1ll << 31) - 1 ? (1ll << 31) - 1 : c;
@@ -341,42 +343,24 @@ RasterWS carve(void* base, long long views, long long nt, long long ntiles, long
 
 }  // namespace
 
-extern "C" {
-
-VCL_API vcl_status vcl_reserve_raster(vcl_ctx* ctx, int W, int H, int views, int nt) {
-    VCL_CTX_CHECK();
-    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nt >= 0, "bad raster reservation sizes");
-    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity(views, nt, W, H, ctx->tile);
-    int ts[3] = {8, 16, 32};
-    size_t need = 0;
-    for (int t : ts) {
-        long long ntiles = (long long)((W + t - 1) / t) * ((H + t - 1) / t) * views;
-        size_t b = ws_bytes(views, nt, ntiles, cap);
-        if (b > need) need = b;
-    }
-    return vcl_ws_reserve(ctx, need);
+long long raster_auto_capacity(long long views, long long nt, int W, int H, int tile) {
+    return auto_capacity_(views, nt, W, H, tile);
 }
 
-VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W,
-                                     int H, int views, float* rast, float* db, void* stream) {
-    VCL_CTX_CHECK();
-    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nv >= 0 && nt >= 0, "bad raster sizes W=%d H=%d views=%d nv=%d nt=%d",
-                W, H, views, nv, nt);
-    VCL_REQUIRE(rast, "rast output is null");
-    VCL_REQUIRE(nt == 0 || (clip && tri), "clip/tri is null");
-    VCL_REQUIRE(((uintptr_t)clip & 15) == 0 && ((uintptr_t)rast & 15) == 0 && ((uintptr_t)db & 15) == 0,
-                "clip/rast/db must be 16-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    const int T = ctx->tile;
+size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap) {
+    long long ntiles = (long long)((W + tile - 1) / tile) * ((H + tile - 1) / tile) * views;
+    return ws_bytes(views, nt, ntiles, cap);
+}
+
+int raster_fwd_launches() { return 4; }
+
+vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const float* clip, int nv, const uint32_t* tri,
+                         int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s) {
     const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
     const long long ntiles_view = (long long)tiles_x * tiles_y;
     const long long ntiles = ntiles_view * views;
-    VCL_REQUIRE(ntiles < (1ll << 31), "too many tiles");
-    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity(views, nt, W, H, T);
-    vcl_status st = vcl_ws_reserve(ctx, ws_bytes(views, nt, ntiles, cap));
-    if (st) return st;
-    RasterWS w = carve(ctx->ws, views, nt, ntiles, cap);
-    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
+    RasterWS w = carve(ws, views, nt, ntiles, cap);
+    vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
     st = vcl_cuda_check(ctx, cudaMemsetAsync(w.cursor, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
@@ -404,6 +388,43 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
                                                (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
     return vcl_launch_check(ctx, "rasterize_fwd");
+}
+
+extern "C" {
+
+VCL_API vcl_status vcl_reserve_raster(vcl_ctx* ctx, int W, int H, int views, int nt) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nt >= 0, "bad raster reservation sizes");
+    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity_(views, nt, W, H, ctx->tile);
+    int ts[3] = {8, 16, 32};
+    size_t need = 0;
+    for (int t : ts) {
+        long long ntiles = (long long)((W + t - 1) / t) * ((H + t - 1) / t) * views;
+        size_t b = ws_bytes(views, nt, ntiles, cap);
+        if (b > need) need = b;
+    }
+    return vcl_ws_reserve(ctx, need);
+}
+
+VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W,
+                                     int H, int views, float* rast, float* db, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nv >= 0 && nt >= 0, "bad raster sizes W=%d H=%d views=%d nv=%d nt=%d",
+                W, H, views, nv, nt);
+    VCL_REQUIRE(rast, "rast output is null");
+    VCL_REQUIRE(nt == 0 || (clip && tri), "clip/tri is null");
+    VCL_REQUIRE(((uintptr_t)clip & 15) == 0 && ((uintptr_t)rast & 15) == 0 && ((uintptr_t)db & 15) == 0,
+                "clip/rast/db must be 16-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int T = ctx->tile;
+    const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
+    const long long ntiles_view = (long long)tiles_x * tiles_y;
+    const long long ntiles = ntiles_view * views;
+    VCL_REQUIRE(ntiles < (1ll << 31), "too many tiles");
+    long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity_(views, nt, W, H, T);
+    vcl_status st = vcl_ws_reserve(ctx, ws_bytes(views, nt, ntiles, cap));
+    if (st) return st;
+    return raster_fwd_ws(ctx, ctx->ws, T, cap, clip, nv, tri, nt, W, H, views, rast, db, s);
 }
 
 VCL_API vcl_status vcl_rasterize_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W, int H,

@@ -1,0 +1,295 @@
+// Spherical-Gaussian lobe arithmetic shared by the per-operator kernels and
+// the fused fit kernels (reference material.cu:285-323 forward, :369-438
+// backward).
+//
+// Per (pixel, lobe) the reference evaluates the SG inner product of the
+// pixel's diffuse lobe (axis n, sharpness 2.133, amplitude 2.34) and of its
+// specular lobe (axis p, sharpness ss, amplitude sa) with an environment
+// lobe (axis a_k, sharpness s_k):
+//     l = |lambda1 mu1 + lambda2 mu2|,
+//     term = (e^(l - lambda1 - lambda2) - e^(-l - lambda1 - lambda2)) / max(l, 1e-6) * amp.
+// Here 1/l comes from one reciprocal square root of |.|^2 (and l = |.|^2 / l),
+// so a lobe costs two rsqrt and four exp instead of two sqrt, two
+// divisions and four exp.
+#pragma once
+#include "common.cuh"
+
+constexpr float SG_DIFF_SHARP = 2.133f;
+constexpr float SG_DIFF_AMP = 2.34f;
+constexpr int SG_CMAX = 8;
+
+// 1/max(|v|, 1e-6) and |v| from |v|^2.
+DEV void sg_len(float d2, float& l, float& il) {
+    il = rsqrtf(fmaxf(d2, 1e-12f));
+    l = d2 * il;
+}
+
+// Forward terms of one lobe for one pixel: diffuse-lobe and specular-lobe
+// SG inner products (without the environment amplitude).
+DEV void sg_terms(float3 dn, float3 sn, float3 g, float gs, float ss, float sa, float& dg, float& sg) {
+    float3 d = dn + g;
+    float l, il;
+    sg_len(dot3(d, d), l, il);
+    dg = (expf(l - SG_DIFF_SHARP - gs) - expf(-l - SG_DIFF_SHARP - gs)) * il * SG_DIFF_AMP;
+    float3 s = sn + g;
+    sg_len(dot3(s, s), l, il);
+    sg = (expf(l - ss - gs) - expf(-l - ss - gs)) * il * sa;
+}
+
+// Backward terms of one lobe (material.cu:398-418).
+struct SGB {
+    float dg, sgv, ddgs, dsgs, dsgss, sil_e;   // sil_e = (e- - e+) / max(l,1e-6) of the specular term
+    float3 ddg, dsg;
+};
+
+DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa) {
+    SGB r;
+    float3 dsum = dn + sgn;
+    float dl, il;
+    sg_len(dot3(dsum, dsum), dl, il);
+    float dotn = (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
+    float em = expf(dl - SG_DIFF_SHARP - gs), ep = expf(-dl - SG_DIFF_SHARP - gs);
+    r.dg = (em - ep) * il * SG_DIFF_AMP;
+    r.ddg = dsum * (((1.f - il) * em + (1.f + il) * ep) * il * il);
+    r.ddgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
+    float3 ssum = sn + sgn;
+    float sl;
+    sg_len(dot3(ssum, ssum), sl, il);
+    float sdot = dot3(sgn, pax);
+    dotn = (gs + ss * sdot) * il;
+    float dotp = (gs * sdot + ss) * il;
+    em = expf(sl - ss - gs); ep = expf(-sl - ss - gs);
+    r.sil_e = (em - ep) * il;
+    r.sgv = r.sil_e * sa;
+    r.dsg = ssum * (((1.f - il) * em + (1.f + il) * ep) * il * il);
+    r.dsgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
+    r.dsgss = ((dotp * (1.f - il) - 1.f) * em + (dotp * (1.f + il) + 1.f) * ep) * il;
+    return r;
+}
+
+DEV float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+DEV bool fin3(float3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+DEV float finite_or0(float v) { return isfinite(v) ? v : 0.f; }
+
+// Lobes staged in shared memory: axis pre-multiplied by sharpness.
+struct SGLobes {
+    const float* ax;   // [K][3] axis * sharpness
+    const float* sh;   // [K]
+    const float* am;   // [K][C]
+};
+
+DEV SGLobes sg_stage_lobes(float* sm, int K, int C, const float* axis, const float* sharp, const float* amp) {
+    float* s_ax = sm;
+    float* s_sh = sm + 3 * K;
+    float* s_am = sm + 4 * K;
+    for (int i = threadIdx.x; i < K; i += blockDim.x) {
+        float s = sharp[i];
+        s_sh[i] = s;
+        s_ax[3 * i] = axis[3 * i] * s; s_ax[3 * i + 1] = axis[3 * i + 1] * s; s_ax[3 * i + 2] = axis[3 * i + 2] * s;
+    }
+    for (int i = threadIdx.x; i < K * C; i += blockDim.x) s_am[i] = amp[i];
+    return SGLobes{s_ax, s_sh, s_am};
+}
+
+// Diffuse and specular environment sums of one pixel with the reference's
+// NaN-guarded accumulation (common.h:181): plain sums when they end finite
+// (then no partial sum was non-finite and every guarded add was a plain
+// add), else the guarded sequential loop.
+template <int CC>
+DEV void sg_env(const SGLobes& L, int K, int C, float3 n, float3 pax, float ss, float sa, float* de, float* se) {
+    const int Cn = CC ? CC : C;
+    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+#pragma unroll
+    for (int k = 0; k < SG_CMAX; ++k) { de[k] = 0.f; se[k] = 0.f; }
+    for (int i = 0; i < K; ++i) {
+        float dg, sg;
+        sg_terms(dn, sn, f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]), L.sh[i], ss, sa, dg, sg);
+#pragma unroll
+        for (int k = 0; k < SG_CMAX; ++k) {
+            if (k >= Cn) break;
+            float a = L.am[i * C + k];
+            de[k] += dg * a;
+            se[k] += sg * a;
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < SG_CMAX; ++k)
+        if (k < Cn) ok = ok && isfinite(de[k]) && isfinite(se[k]);
+    if (ok) return;
+#pragma unroll
+    for (int k = 0; k < SG_CMAX; ++k) { de[k] = 0.f; se[k] = 0.f; }
+    for (int i = 0; i < K; ++i) {
+        float dg, sg;
+        sg_terms(dn, sn, f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]), L.sh[i], ss, sa, dg, sg);
+        for (int k = 0; k < Cn; ++k) {
+            float a = L.am[i * C + k];
+            add_nan_check(de[k], dg * a);
+            add_nan_check(se[k], sg * a);
+        }
+    }
+}
+
+// Specular lobe of a pixel (material.cu:155-178 / :213-240).
+struct SpecLobe { float3 p; float vn, pn, m, m2, Gv, Gp, F, iGv, iGp; };
+
+// material.cu:155-178 / :213-240
+DEV SpecLobe spec_eval(float3 n, float3 vw, float m, float ior) {
+    SpecLobe s;
+    float3 v = f3(-vw.x, -vw.y, -vw.z);
+    s.p = n * (2.f * dot3(v, n)) - v;
+    s.m = m; s.m2 = m * m;
+    s.vn = fmaxf(dot3(v, n), 0.f);
+    float vn2 = s.vn * s.vn;
+    s.iGv = sqrtf(vn2 + s.m2 * (1.f - vn2));
+    s.Gv = 1.f / fmaxf(s.vn + s.iGv, 1e-6f);
+    s.pn = fmaxf(dot3(s.p, n), 0.f);
+    float pn2 = s.pn * s.pn;
+    s.iGp = sqrtf(pn2 + s.m2 * (1.f - pn2));
+    s.Gp = 1.f / fmaxf(s.pn + s.iGp, 1e-6f);
+    float g = sqrtf(ior * ior - 1.f + pn2);
+    float gp = g + s.pn, gm = g - s.pn;
+    float f0 = gm / gp;
+    float f1 = (s.pn * gp - 1.f) / (s.pn * gm + 1.f);
+    s.F = f0 * f0 * (1.f + f1 * f1);
+    return s;
+}
+
+
+// Per-pixel state of the SG backward.
+struct SGPix {
+    float3 n, pax, gsx;
+    float ss, sa, gsh;
+    float dfs[SG_CMAX], go[SG_CMAX], gd[SG_CMAX], gsa[SG_CMAX];
+};
+
+// The guarded (reference-order) per-pixel accumulation, used only when the
+// plain sums of a pixel end non-finite.
+template <int CC>
+DEV void sg_bwd_pixel_slow(const SGLobes& L, int K, int C, int exact, SGPix& q, const float* gd0, const float* gsa0,
+                           float3 gsx0, float gsh0) {
+    const int Cn = CC ? CC : C;
+    for (int k = 0; k < Cn; ++k) { q.gd[k] = gd0[k]; q.gsa[k] = gsa0[k]; }
+    float gsx[3] = {gsx0.x, gsx0.y, gsx0.z};
+    q.gsh = gsh0;
+    const float3 dn = q.n * SG_DIFF_SHARP, sn = q.pax * q.ss;
+    for (int i = 0; i < K; ++i) {
+        float gs = L.sh[i];
+        float3 sgn = f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]);
+        SGB t = sg_bwd_terms(q.n, dn, q.pax, sn, sgn, gs, q.ss, q.sa);
+        float sum = 0.f, sum_sa = 0.f;
+        for (int k = 0; k < Cn; ++k) {
+            float a = L.am[i * C + k], g = q.go[k];
+            sum += g * a;
+            add_nan_check(q.gd[k], g * t.dg * a);
+            if (!exact) add_nan_check(q.gsa[k], g * t.sgv * a);
+            else sum_sa += g * t.sil_e * a;
+        }
+        if (exact) add_nan_check(q.gsa[0], sum_sa);
+        float3 csx = ((t.dsg * sum) * q.sa) * q.ss;
+        add_nan_check3(gsx, csx.x, csx.y, csx.z);
+        if (exact) add_nan_check(q.gsh, sum * t.dsgss * q.sa);
+    }
+    q.gsx = f3(gsx[0], gsx[1], gsx[2]);
+}
+
+// SG backward of P pixels per thread (material.cu:369-438).  Lobe
+// gradients are summed over the thread's P pixels, then over the warp
+// (shuffles), into the warp's shared accumulators `wacc` [K][nacc]:
+// axis xyz, sharpness, amplitude[C], then (compat) the lobe-indexed
+// specular sharpness.  Per-pixel gradients stay in `q`.
+template <int P, int CC>
+DEV void sg_bwd_block(const SGLobes& L, int K, int C, int exact, SGPix (&q)[P], const bool (&live)[P], float* wacc,
+                      int nacc, bool lobe_grads, bool ssh_lobe) {
+    const int Cn = CC ? CC : C;
+    const int lane = threadIdx.x & 31;
+    float gd0[P][SG_CMAX], gsa0[P][SG_CMAX], gsh0[P];
+    float3 gsx0[P], dn[P], sn[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+#pragma unroll
+        for (int k = 0; k < SG_CMAX; ++k) { gd0[j][k] = q[j].gd[k]; gsa0[j][k] = q[j].gsa[k]; }
+        gsh0[j] = q[j].gsh;
+        gsx0[j] = q[j].gsx;
+        dn[j] = q[j].n * SG_DIFF_SHARP;
+        sn[j] = q[j].pax * q[j].ss;
+    }
+    for (int i = 0; i < K; ++i) {
+        const float gs = L.sh[i];
+        const float3 sgn = f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]);
+        float c_ax0 = 0.f, c_ax1 = 0.f, c_ax2 = 0.f, c_sh = 0.f, c_ssh = 0.f;
+        float c_am[SG_CMAX];
+#pragma unroll
+        for (int k = 0; k < SG_CMAX; ++k) c_am[k] = 0.f;
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            if (!live[j]) continue;
+            SGB t = sg_bwd_terms(q[j].n, dn[j], q[j].pax, sn[j], sgn, gs, q[j].ss, q[j].sa);
+            float sum = 0.f, sumd = 0.f, sum_sa = 0.f;
+#pragma unroll
+            for (int k = 0; k < SG_CMAX; ++k) {
+                if (k >= Cn) break;
+                float a = L.am[i * C + k];
+                float g = q[j].go[k];
+                sum += g * a;
+                sumd += g * a * q[j].dfs[k];
+                c_am[k] += finite_or0(g * (t.dg * q[j].dfs[k] + t.sgv));
+                q[j].gd[k] += g * t.dg * a;
+                if (!exact) q[j].gsa[k] += g * t.sgv * a;
+                else sum_sa += g * t.sil_e * a;
+            }
+            if (exact) q[j].gsa[0] += sum_sa;
+            float3 cax = ((t.ddg * sumd) * SG_DIFF_AMP + (t.dsg * sum) * q[j].sa) * gs;
+            if (fin3(cax)) { c_ax0 += cax.x; c_ax1 += cax.y; c_ax2 += cax.z; }
+            c_sh += finite_or0(sumd * t.ddgs * SG_DIFF_AMP + sum * t.dsgs * q[j].sa);
+            q[j].gsx = q[j].gsx + ((t.dsg * sum) * q[j].sa) * q[j].ss;
+            float cssh = sum * t.dsgss * q[j].sa;
+            if (exact) q[j].gsh += cssh;
+            else c_ssh += finite_or0(cssh);
+        }
+        if (lobe_grads) {
+            float* a = wacc + (size_t)i * nacc;
+            float v;
+            v = warp_sum(c_ax0); if (lane == 0) a[0] += v;
+            v = warp_sum(c_ax1); if (lane == 0) a[1] += v;
+            v = warp_sum(c_ax2); if (lane == 0) a[2] += v;
+            v = warp_sum(c_sh); if (lane == 0) a[3] += v;
+#pragma unroll
+            for (int k = 0; k < SG_CMAX; ++k) {
+                if (k >= Cn) break;
+                v = warp_sum(c_am[k]);
+                if (lane == 0) a[4 + k] += v;
+            }
+            if (ssh_lobe) { v = warp_sum(c_ssh); if (lane == 0) a[4 + Cn] += v; }
+        }
+    }
+    // per-pixel sums that did not end finite: redo them in reference order
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        if (!live[j]) continue;
+        bool ok = fin3(q[j].gsx) && isfinite(q[j].gsh);
+        for (int k = 0; k < Cn; ++k) ok = ok && isfinite(q[j].gd[k]) && isfinite(q[j].gsa[k]);
+        if (!ok) sg_bwd_pixel_slow<CC>(L, K, C, exact, q[j], gd0[j], gsa0[j], gsx0[j], gsh0[j]);
+    }
+}
+
+// Flushes the per-warp accumulators of a block to the global lobe gradients.
+DEV void sg_flush_lobes(const float* s_acc, int nwarps, int K, int C, int nacc, float* gaxis, float* gsharp, float* gamp,
+                        float* gssh_lobe) {
+    for (int j = threadIdx.x; j < K * nacc; j += blockDim.x) {
+        float v = 0.f;
+        for (int w = 0; w < nwarps; ++w) v += s_acc[(size_t)w * K * nacc + j];
+        if (v == 0.f) continue;
+        int i = j / nacc, q = j % nacc;
+        if (q < 3) { if (gaxis) atomicAdd(&gaxis[3 * i + q], v); }
+        else if (q == 3) { if (gsharp) atomicAdd(&gsharp[i], v); }
+        else if (q < 4 + C) { if (gamp) atomicAdd(&gamp[i * C + (q - 4)], v); }
+        else if (gssh_lobe) atomicAdd(&gssh_lobe[i], v);
+    }
+}
+

@@ -6,12 +6,11 @@
 // atomic per block and lobe parameter -- the reference accumulates them
 // with unsynchronised adds from every thread (material.cu:428-436).
 #include "common.cuh"
+#include "sg_math.cuh"
 
 namespace {
 
-constexpr int CMAX = 8;
-constexpr float DIFF_SHARP = 2.133f;
-constexpr float DIFF_AMP = 2.34f;
+constexpr int CMAX = SG_CMAX;
 
 // material.cu:25-48 (the branch taken with a normal map bound)
 __global__ void k_normal_axis(const float4* __restrict__ rast, long long npix, const float* __restrict__ rot,
@@ -52,30 +51,6 @@ __global__ void k_view_axis(int W, int H, long long npix, const float* __restric
     st3(out, p, normalize3(f3(M[0], M[1], M[2]) * sx + f3(M[3], M[4], M[5]) * sy + f3(M[6], M[7], M[8])));
 }
 
-struct SpecLobe { float3 p; float vn, pn, m, m2, Gv, Gp, F, iGv, iGp; };
-
-// material.cu:155-178 / :213-240
-DEV SpecLobe spec_eval(float3 n, float3 vw, float m, float ior) {
-    SpecLobe s;
-    float3 v = f3(-vw.x, -vw.y, -vw.z);
-    s.p = n * (2.f * dot3(v, n)) - v;
-    s.m = m; s.m2 = m * m;
-    s.vn = fmaxf(dot3(v, n), 0.f);
-    float vn2 = s.vn * s.vn;
-    s.iGv = sqrtf(vn2 + s.m2 * (1.f - vn2));
-    s.Gv = 1.f / fmaxf(s.vn + s.iGv, 1e-6f);
-    s.pn = fmaxf(dot3(s.p, n), 0.f);
-    float pn2 = s.pn * s.pn;
-    s.iGp = sqrtf(pn2 + s.m2 * (1.f - pn2));
-    s.Gp = 1.f / fmaxf(s.pn + s.iGp, 1e-6f);
-    float g = sqrtf(ior * ior - 1.f + pn2);
-    float gp = g + s.pn, gm = g - s.pn;
-    float f0 = gm / gp;
-    float f1 = (s.pn * gp - 1.f) / (s.pn * gm + 1.f);
-    s.F = f0 * f0 * (1.f + f1 * f1);
-    return s;
-}
-
 __global__ void k_sg_spec_fwd(const float4* __restrict__ rast, long long npix, const float* __restrict__ normal,
                               const float* __restrict__ view, const float* __restrict__ rough, float ior,
                               float* __restrict__ oax, float* __restrict__ osh, float* __restrict__ oam) {
@@ -109,227 +84,108 @@ __global__ void k_sg_spec_bwd(const float4* __restrict__ rast, long long npix, c
     grough[p] = g;
 }
 
-// SG inner-product term (e^(l-a-b) - e^(-l-a-b)) / max(l, 1e-6) * amp,
-// material.cu:309/311.
-DEV float sg_term(float l, float a, float b, float amp) {
-    return (expf(l - a - b) - expf(-l - a - b)) / fmaxf(l, 1e-6f) * amp;
-}
-
 // material.cu:285-323
+template <int CC>
 __global__ void k_sg_fwd(int C, int K, const float* __restrict__ axis, const float* __restrict__ sharp,
                          const float* __restrict__ amp, const float4* __restrict__ rast, long long npix,
                          const float* __restrict__ normal, const float* __restrict__ diffuse, const float* __restrict__ sax,
                          const float* __restrict__ ssh, const float* __restrict__ sam, float* __restrict__ out,
                          float* __restrict__ odiff, float* __restrict__ ospec) {
     extern __shared__ float sm[];
-    float* s_ax = sm;             // [K][3], pre-multiplied by sharpness
-    float* s_sh = sm + 3 * K;     // [K]
-    float* s_am = sm + 4 * K;     // [K][C]
-    for (int i = threadIdx.x; i < K; i += blockDim.x) {
-        float s = sharp[i];
-        s_sh[i] = s;
-        s_ax[3 * i] = axis[3 * i] * s; s_ax[3 * i + 1] = axis[3 * i + 1] * s; s_ax[3 * i + 2] = axis[3 * i + 2] * s;
-    }
-    for (int i = threadIdx.x; i < K * C; i += blockDim.x) s_am[i] = amp[i];
+    const SGLobes L = sg_stage_lobes(sm, K, C, axis, sharp, amp);
     __syncthreads();
+    const int Cn = CC ? CC : C;
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npix) return;
     if (rast_id(rast[p].w) < 0) {
-        for (int k = 0; k < C; ++k) {
-            out[p * C + k] = 0.f;
-            if (odiff) odiff[p * C + k] = 0.f;
-            if (ospec) ospec[p * C + k] = 0.f;
+        for (int k = 0; k < Cn; ++k) {
+            out[p * Cn + k] = 0.f;
+            if (odiff) odiff[p * Cn + k] = 0.f;
+            if (ospec) ospec[p * Cn + k] = 0.f;
         }
         return;
     }
-    float3 dn = ld3(normal, p) * DIFF_SHARP;
-    float ss = ssh[p], sa = sam[p];
-    float3 sn = ld3(sax, p) * ss;
-    float de[CMAX], se[CMAX];
+    float de[SG_CMAX], se[SG_CMAX];
+    sg_env<CC>(L, K, C, ld3(normal, p), ld3(sax, p), ssh[p], sam[p], de, se);
 #pragma unroll
-    for (int k = 0; k < CMAX; ++k) { de[k] = 0.f; se[k] = 0.f; }
-    for (int i = 0; i < K; ++i) {
-        float gs = s_sh[i];
-        float3 g = f3(s_ax[3 * i], s_ax[3 * i + 1], s_ax[3 * i + 2]);
-        float dg = sg_term(len3(dn + g), DIFF_SHARP, gs, DIFF_AMP);
-        float sg = sg_term(len3(sn + g), ss, gs, sa);
-#pragma unroll
-        for (int k = 0; k < CMAX; ++k) {
-            if (k >= C) break;
-            float a = s_am[i * C + k];
-            add_nan_check(de[k], dg * a);
-            add_nan_check(se[k], sg * a);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < CMAX; ++k) {
-        if (k >= C) break;
-        out[p * C + k] = diffuse[p * C + k] * de[k] + se[k];
-        if (odiff) odiff[p * C + k] = de[k];
-        if (ospec) ospec[p * C + k] = se[k];
+    for (int k = 0; k < SG_CMAX; ++k) {
+        if (k >= Cn) break;
+        out[p * Cn + k] = diffuse[p * Cn + k] * de[k] + se[k];
+        if (odiff) odiff[p * Cn + k] = de[k];
+        if (ospec) ospec[p * Cn + k] = se[k];
     }
 }
 
-DEV float warp_sum(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
+constexpr int SGB_P = 2;
 
-DEV bool fin3(float3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
-
-// material.cu:369-438.  Accumulator layout per lobe: axis xyz, sharpness,
-// amplitude[C], then (compat only) the specular sharpness the reference
-// indexes by lobe.
-__global__ void k_sg_bwd(int C, int K, int nacc, const float* __restrict__ axis, const float* __restrict__ sharp,
-                         const float* __restrict__ amp, const float4* __restrict__ rast, long long npix,
-                         const float* __restrict__ normal, const float* __restrict__ diffuse, const float* __restrict__ sax,
-                         const float* __restrict__ ssh, const float* __restrict__ sam, const float* __restrict__ gout,
-                         float* __restrict__ gdiff, float* __restrict__ gaxis, float* __restrict__ gsharp,
-                         float* __restrict__ gamp, float* __restrict__ gsax, float* __restrict__ gssh,
-                         float* __restrict__ gsam, int exact) {
+template <int CC>
+__global__ void __launch_bounds__(256) k_sg_bwd(int C, int K, int nacc, const float* __restrict__ axis,
+                                                const float* __restrict__ sharp, const float* __restrict__ amp,
+                                                const float4* __restrict__ rast, long long npix,
+                                                const float* __restrict__ normal, const float* __restrict__ diffuse,
+                                                const float* __restrict__ sax, const float* __restrict__ ssh,
+                                                const float* __restrict__ sam, const float* __restrict__ gout,
+                                                float* __restrict__ gdiff, float* __restrict__ gaxis,
+                                                float* __restrict__ gsharp, float* __restrict__ gamp,
+                                                float* __restrict__ gsax, float* __restrict__ gssh,
+                                                float* __restrict__ gsam, int exact) {
     extern __shared__ float sm[];
     const int nwarps = blockDim.x >> 5;
-    float* s_ax = sm;
-    float* s_sh = sm + 3 * K;
-    float* s_am = sm + 4 * K;
-    float* s_acc = sm + (4 + C) * K;   // [nwarps][K][nacc]
+    const int Cn = CC ? CC : C;
+    const SGLobes L = sg_stage_lobes(sm, K, C, axis, sharp, amp);
+    float* s_acc = sm + (4 + C) * K;
     const bool lobe_grads = gaxis || gsharp || gamp || (!exact && gssh);
-    for (int i = threadIdx.x; i < K; i += blockDim.x) {
-        float s = sharp[i];
-        s_sh[i] = s;
-        s_ax[3 * i] = axis[3 * i] * s; s_ax[3 * i + 1] = axis[3 * i + 1] * s; s_ax[3 * i + 2] = axis[3 * i + 2] * s;
-    }
-    for (int i = threadIdx.x; i < K * C; i += blockDim.x) s_am[i] = amp[i];
     if (lobe_grads)
         for (int i = threadIdx.x; i < nwarps * K * nacc; i += blockDim.x) s_acc[i] = 0.f;
     __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    float* wacc = s_acc + (size_t)wid * K * nacc;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long npad = (npix + 31) / 32 * 32;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npad; p += stride) {
-        bool live = p < npix && rast_id(rast[p].w) >= 0;
-        if (!lobe_grads && !live) continue;
-        float3 n = f3(0.f, 0.f, 0.f), pax = n;
-        float ss = 0.f, sa = 0.f;
-        float dfs[CMAX], go[CMAX], gd[CMAX], gsa[CMAX];
-        float3 gsx = f3(0.f, 0.f, 0.f);
-        float gsh_p = 0.f;
+    float* wacc = s_acc + (size_t)(threadIdx.x >> 5) * K * nacc;
+    const long long span = (long long)blockDim.x * SGB_P;
+    for (long long base = (long long)blockIdx.x * span; base < npix; base += (long long)gridDim.x * span) {
+        SGPix q[SGB_P];
+        bool live[SGB_P];
+        bool any = false;
 #pragma unroll
-        for (int k = 0; k < CMAX; ++k) { dfs[k] = 0.f; go[k] = 0.f; gd[k] = 0.f; gsa[k] = 0.f; }
-        if (live) {
-            n = ld3(normal, p);
-            pax = ld3(sax, p);
-            ss = ssh[p]; sa = sam[p];
+        for (int j = 0; j < SGB_P; ++j) {
+            long long p = base + threadIdx.x + (long long)j * blockDim.x;
+            live[j] = p < npix && rast_id(rast[p].w) >= 0;
+            any |= live[j];
+            SGPix& z = q[j];
+            z.gsx = f3(0.f, 0.f, 0.f); z.gsh = 0.f;
 #pragma unroll
-            for (int k = 0; k < CMAX; ++k) {
-                if (k >= C) break;
-                dfs[k] = diffuse[p * C + k];
-                go[k] = gout[p * C + k];
-                if (gdiff) gd[k] = gdiff[p * C + k];
-                if (gsam && !exact) gsa[k] = gsam[p * C + k];
-            }
-            if (gsax) gsx = ld3(gsax, p);
-            if (gsam && exact) gsa[0] = gsam[p];
-            if (gssh && exact) gsh_p = gssh[p];
-        }
-        const float3 diffn = n * DIFF_SHARP, specn = pax * ss;
-        for (int i = 0; i < K; ++i) {
-            float gs = s_sh[i];
-            float3 sgn = f3(s_ax[3 * i], s_ax[3 * i + 1], s_ax[3 * i + 2]);
-            float c_ax0 = 0.f, c_ax1 = 0.f, c_ax2 = 0.f, c_sh = 0.f, c_ssh = 0.f;
-            float c_am[CMAX];
-#pragma unroll
-            for (int k = 0; k < CMAX; ++k) c_am[k] = 0.f;
-            if (live) {
-                float3 dsum = diffn + sgn;
-                float dl = len3(dsum);
-                float il = 1.f / fmaxf(dl, 1e-6f);
-                float dotn = (gs + DIFF_SHARP * dot3(sgn, n)) * il;
-                float em = expf(dl - DIFF_SHARP - gs), ep = expf(-dl - DIFF_SHARP - gs);
-                float dg = (em - ep) * il * DIFF_AMP;
-                float3 ddg = dsum * (((1.f - il) * em + (1.f + il) * ep) * il) * il;
-                float ddgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
-                float3 ssum = specn + sgn;
-                float sl = len3(ssum);
-                il = 1.f / fmaxf(sl, 1e-6f);
-                float sdot = dot3(sgn, pax);
-                dotn = (gs + ss * sdot) * il;
-                float dotp = (gs * sdot + ss) * il;
-                em = expf(sl - ss - gs); ep = expf(-sl - ss - gs);
-                float sgv = (em - ep) * il * sa;
-                float3 dsg = ssum * (((1.f - il) * em + (1.f + il) * ep) * il) * il;
-                float dsgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
-                float dsgss = ((dotp * (1.f - il) - 1.f) * em + (dotp * (1.f + il) + 1.f) * ep) * il;
-                float sum = 0.f, sumd = 0.f, sum_sa = 0.f;
-#pragma unroll
-                for (int k = 0; k < CMAX; ++k) {
-                    if (k >= C) break;
-                    float a = s_am[i * C + k];
-                    float g = go[k];
-                    sum += g * a;
-                    sumd += g * a * dfs[k];
-                    c_am[k] = g * (dg * dfs[k] + sgv);
-                    add_nan_check(gd[k], g * dg * a);
-                    if (!exact) add_nan_check(gsa[k], g * sgv * a);
-                    else sum_sa += g * (em - ep) * il * a;
+            for (int k = 0; k < SG_CMAX; ++k) { z.dfs[k] = 0.f; z.go[k] = 0.f; z.gd[k] = 0.f; z.gsa[k] = 0.f; }
+            if (live[j]) {
+                z.n = ld3(normal, p); z.pax = ld3(sax, p); z.ss = ssh[p]; z.sa = sam[p];
+                for (int k = 0; k < Cn; ++k) {
+                    z.dfs[k] = diffuse[p * Cn + k];
+                    z.go[k] = gout[p * Cn + k];
+                    if (gdiff) z.gd[k] = gdiff[p * Cn + k];
+                    if (gsam && !exact) z.gsa[k] = gsam[p * Cn + k];
                 }
-                if (exact) add_nan_check(gsa[0], sum_sa);
-                float3 t = (ddg * sumd) * DIFF_AMP + (dsg * sum) * sa;
-                float3 cax = t * gs;
-                if (fin3(cax)) { c_ax0 = cax.x; c_ax1 = cax.y; c_ax2 = cax.z; }
-                c_sh = sumd * ddgs * DIFF_AMP + sum * dsgs * sa;
-                if (!isfinite(c_sh)) c_sh = 0.f;
-                float3 csx = ((dsg * sum) * sa) * ss;
-                add_nan_check3(&gsx.x, csx.x, csx.y, csx.z);
-                float cssh = sum * dsgss * sa;
-                if (exact) add_nan_check(gsh_p, cssh);
-                else c_ssh = isfinite(cssh) ? cssh : 0.f;
-#pragma unroll
-                for (int k = 0; k < CMAX; ++k)
-                    if (!isfinite(c_am[k])) c_am[k] = 0.f;
-            }
-            if (lobe_grads) {
-                float* a = wacc + (size_t)i * nacc;
-                float v;
-                v = warp_sum(c_ax0); if (lane == 0) a[0] += v;
-                v = warp_sum(c_ax1); if (lane == 0) a[1] += v;
-                v = warp_sum(c_ax2); if (lane == 0) a[2] += v;
-                v = warp_sum(c_sh); if (lane == 0) a[3] += v;
-#pragma unroll
-                for (int k = 0; k < CMAX; ++k) {
-                    if (k >= C) break;
-                    v = warp_sum(c_am[k]);
-                    if (lane == 0) a[4 + k] += v;
-                }
-                if (!exact && gssh) { v = warp_sum(c_ssh); if (lane == 0) a[4 + C] += v; }
+                if (gsax) z.gsx = ld3(gsax, p);
+                if (gsam && exact) z.gsa[0] = gsam[p];
+                if (gssh && exact) z.gsh = gssh[p];
+            } else {
+                z.n = z.pax = f3(0.f, 0.f, 0.f); z.ss = z.sa = 0.f;
             }
         }
-        if (live) {
+        if (!__any_sync(0xffffffffu, any)) continue;
+        sg_bwd_block<SGB_P, CC>(L, K, C, exact, q, live, wacc, nacc, lobe_grads, !exact && gssh);
 #pragma unroll
-            for (int k = 0; k < CMAX; ++k) {
-                if (k >= C) break;
-                if (gdiff) gdiff[p * C + k] = gd[k];
-                if (gsam && !exact) gsam[p * C + k] = gsa[k];
+        for (int j = 0; j < SGB_P; ++j) {
+            if (!live[j]) continue;
+            long long p = base + threadIdx.x + (long long)j * blockDim.x;
+            for (int k = 0; k < Cn; ++k) {
+                if (gdiff) gdiff[p * Cn + k] = q[j].gd[k];
+                if (gsam && !exact) gsam[p * Cn + k] = q[j].gsa[k];
             }
-            if (gsax) st3(gsax, p, gsx);
-            if (gsam && exact) gsam[p] = gsa[0];
-            if (gssh && exact) gssh[p] = gsh_p;
+            if (gsax) st3(gsax, p, q[j].gsx);
+            if (gsam && exact) gsam[p] = q[j].gsa[0];
+            if (gssh && exact) gssh[p] = q[j].gsh;
         }
     }
     if (!lobe_grads) return;
     __syncthreads();
-    for (int j = threadIdx.x; j < K * nacc; j += blockDim.x) {
-        float v = 0.f;
-        for (int w = 0; w < nwarps; ++w) v += s_acc[(size_t)w * K * nacc + j];
-        if (v == 0.f) continue;
-        int i = j / nacc, q = j % nacc;
-        if (q < 3) { if (gaxis) atomicAdd(&gaxis[3 * i + q], v); }
-        else if (q == 3) { if (gsharp) atomicAdd(&gsharp[i], v); }
-        else if (q < 4 + C) { if (gamp) atomicAdd(&gamp[i * C + (q - 4)], v); }
-        else if (gssh) atomicAdd(&gssh[i], v);
-    }
+    sg_flush_lobes(s_acc, nwarps, K, C, nacc, gaxis, gsharp, gamp, exact ? nullptr : gssh);
 }
 
 size_t sg_fwd_smem(int K, int C) { return sizeof(float) * (size_t)K * (4 + C); }
@@ -399,12 +255,12 @@ VCL_API vcl_status vcl_sg_fwd(vcl_ctx* ctx, const float* rast, int W, int H, int
     VCL_REQUIRE(K >= 0 && K <= 1024 && (K == 0 || (axis && sharpness && amplitude)), "bad lobe count %d", K);
     long long npix = (long long)W * H * views;
     size_t smem = sg_fwd_smem(K, C);
-    static bool attr_set = false;
-    if (!attr_set) { cudaFuncSetAttribute(k_sg_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); attr_set = true; }
-    k_sg_fwd<<<vcl_blocks(npix, 256), 256, smem, (cudaStream_t)stream>>>(C, K, axis, sharpness, amplitude,
-                                                                        (const float4*)rast, npix, normal, diffuse,
-                                                                        spec_axis, spec_sharpness, spec_amplitude, out,
-                                                                        out_diffenv, out_specenv);
+    auto kern = C == 4 ? k_sg_fwd<4> : k_sg_fwd<0>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<vcl_blocks(npix, 256), 256, smem, (cudaStream_t)stream>>>(C, K, axis, sharpness, amplitude,
+                                                                    (const float4*)rast, npix, normal, diffuse,
+                                                                    spec_axis, spec_sharpness, spec_amplitude, out,
+                                                                    out_diffenv, out_specenv);
     return vcl_launch_check(ctx, "sg_fwd");
 }
 
@@ -425,12 +281,13 @@ VCL_API vcl_status vcl_sg_bwd(vcl_ctx* ctx, const float* rast, int W, int H, int
     const int nacc = 4 + C + 1;
     size_t smem = sg_bwd_smem(K, C, nacc, threads);
     VCL_REQUIRE(smem <= 200 * 1024, "too many lobes for the shared-memory reduction (K=%d)", K);
-    static bool attr_set = false;
-    if (!attr_set) { cudaFuncSetAttribute(k_sg_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024); attr_set = true; }
-    long long blocks = (npix + threads - 1) / threads;
+    VCL_REQUIRE(C == 4 || C <= CMAX, "channel count");
+    auto kern = C == 4 ? k_sg_bwd<4> : k_sg_bwd<0>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    long long blocks = (npix + threads * SGB_P - 1) / (threads * SGB_P);
     long long cap = (long long)ctx->sm_count * 4;
     int grid = (int)(blocks < cap ? (blocks < 1 ? 1 : blocks) : cap);
-    k_sg_bwd<<<grid, threads, smem, (cudaStream_t)stream>>>(
+    kern<<<grid, threads, smem, (cudaStream_t)stream>>>(
         C, K, nacc, axis, sharpness, amplitude, (const float4*)rast, npix, normal, diffuse, spec_axis, spec_sharpness,
         spec_amplitude, grad_out, grad_diffuse, grad_axis, grad_sharpness, grad_amplitude, grad_spec_axis,
         grad_spec_sharpness, grad_spec_amplitude, exact);
