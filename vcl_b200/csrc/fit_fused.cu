@@ -39,6 +39,8 @@ struct Fused {
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
     int graph_mode = -1;
+    cudaStream_t side = nullptr;               // lobe-gradient branch
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 DEV float mulr(float a, float b) { return __fmul_rn(a, b); }
@@ -134,7 +136,7 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
 // Forward shading of every pixel; writes the color and the antialias input
 // copy (antialias.cu:62-65).  C = 4 texture/lobe channels.
 __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
-                                                   float4* __restrict__ aa) {
+                                                   float4* __restrict__ aa, float4* __restrict__ diffenv) {
     extern __shared__ float sm[];
     const SGLobes L = sg_stage_lobes(sm, a.K, 4, a.axis, a.sharp, a.amp);
     __syncthreads();
@@ -142,11 +144,12 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
     if (p >= a.npix) return;
     PixIn q;
     if (!shade_inputs<1>(a, td, p, q)) {
-        color[p] = aa[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        color[p] = aa[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
     float de[SG_CMAX], se[SG_CMAX];
     sg_env<4>(L, a.K, 4, q.n, q.pax, q.ss, q.sa, de, se);
+    diffenv[p] = make_float4(de[0], de[1], de[2], de[3]);
     float4 c = make_float4(q.dfs.x * de[0] + se[0], q.dfs.y * de[1] + se[1], q.dfs.z * de[2] + se[2],
                            q.dfs.w * de[3] + se[3]);
     color[p] = c;
@@ -175,152 +178,165 @@ __global__ void k_mse_init(const float4* __restrict__ aa, const float4* __restri
     }
 }
 
-constexpr int FP = 2;   // pixels per thread in the fused backward
-
-// material.cu:369-438 -> texturemap.cu:229-284 -> interpolate.cu:114-143 ->
-// rasterize.cu:84-141 for the pixels of each thread, gradients scattered
-// with vector reductions.
-__global__ void __launch_bounds__(256, 2) k_fused_bwd(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
-                                                   float* __restrict__ g_pyr, const float* __restrict__ clip,
-                                                   float* __restrict__ g_clip, float* __restrict__ g_axis,
-                                                   float* __restrict__ g_sharp, float* __restrict__ g_amp, int nacc,
-                                                   int want_tex, int want_geom) {
-    extern __shared__ float sm[];
-    const int nwarps = blockDim.x >> 5;
-    const int K = a.K;
-    const SGLobes L = sg_stage_lobes(sm, K, 4, a.axis, a.sharp, a.amp);
-    float* s_acc = sm + 8 * K;
-    const bool lobe_grads = g_axis != nullptr;
-    if (lobe_grads)
-        for (int i = threadIdx.x; i < nwarps * K * nacc; i += blockDim.x) s_acc[i] = 0.f;
-    __syncthreads();
-    float* wacc = s_acc + (size_t)(threadIdx.x >> 5) * K * nacc;
-    const long long span = (long long)blockDim.x * FP;
-    for (long long base = (long long)blockIdx.x * span; base < a.npix; base += (long long)gridDim.x * span) {
-        SGPix q[FP];
-        PixIn in[FP];
-        bool live[FP];
-        bool any = false;
+// Per-pixel backward below the SG stage: the diffuse gradient is
+// grad ⊙ diffenv (material.cu:429 summed over the lobes), then texture
+// backward (texturemap.cu:229-284), interpolate backward to the
+// barycentrics (interpolate.cu:114-143) and raster backward
+// (rasterize.cu:84-141), scattered with vector reductions.
+__global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+                                                 const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
+                                                 const float* __restrict__ clip, float* __restrict__ g_clip,
+                                                 int want_tex, int want_geom) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.npix) return;
+    const float4 r = a.rast[p];
+    const int idx = rast_id(r.w);
+    if (idx < 0 || idx >= a.nt) return;
+    const uint32_t i0 = a.tri[3 * (size_t)idx], i1 = a.tri[3 * (size_t)idx + 1], i2 = a.tri[3 * (size_t)idx + 2];
+    if (i0 >= (uint32_t)a.nv || i1 >= (uint32_t)a.nv || i2 >= (uint32_t)a.nv) return;
+    const float4 gc = g_color[p], de = diffenv[p];
+    const float4 g = make_float4(gc.x * de.x, gc.y * de.y, gc.z * de.z, gc.w * de.w);
+    // uv and its screen derivatives (interpolate.cu:20-49)
+    const float4 d = a.db[p];
+    const double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
+    float u[2], dx[2], dy[2];
 #pragma unroll
-        for (int j = 0; j < FP; ++j) {
-            long long p = base + threadIdx.x + (long long)j * blockDim.x;
-            live[j] = p < a.npix && shade_inputs<1>(a, td, p, in[j]);
-            any |= live[j];
-            SGPix& z = q[j];
-            z.gsx = f3(0.f, 0.f, 0.f); z.gsh = 0.f;
-#pragma unroll
-            for (int k = 0; k < SG_CMAX; ++k) { z.dfs[k] = 0.f; z.go[k] = 0.f; z.gd[k] = 0.f; z.gsa[k] = 0.f; }
-            z.n = z.pax = f3(0.f, 0.f, 0.f); z.ss = z.sa = 0.f;
-            if (live[j]) {
-                z.n = in[j].n; z.pax = in[j].pax; z.ss = in[j].ss; z.sa = in[j].sa;
-                z.dfs[0] = in[j].dfs.x; z.dfs[1] = in[j].dfs.y; z.dfs[2] = in[j].dfs.z; z.dfs[3] = in[j].dfs.w;
-                float4 g = g_color[p];
-                z.go[0] = g.x; z.go[1] = g.y; z.go[2] = g.z; z.go[3] = g.w;
-            }
-        }
-        if (!__any_sync(0xffffffffu, any)) continue;
-        sg_bwd_block<FP, 4>(L, K, 4, 0, q, live, wacc, nacc, lobe_grads, false);
-        if (!want_tex && !want_geom) continue;
-#pragma unroll
-        for (int j = 0; j < FP; ++j) {
-            if (!live[j]) continue;
-            const long long p = base + threadIdx.x + (long long)j * blockDim.x;
-            const PixIn& I = in[j];
-            const float4 g = make_float4(q[j].gd[0], q[j].gd[1], q[j].gd[2], q[j].gd[3]);
-            // texture backward (texturemap.cu:229-284)
-            int l0 = 0, l1 = 0;
-            float fl = 0.f;
-            if (td.L > 1) calc_level(td, I.uvda, l0, l1, fl, nullptr, 0);
-            const bool mip = td.L > 1;
-            int q0[4], q1[4];
-            float2 f0, f1 = make_float2(0.f, 0.f);
-            index_fetch(td, l0, I.uv, q0, f0);
-            const bool tri = mip && fl > 0;
-            if (tri) index_fetch(td, l1, I.uv, q1, f1);
-            const float wl0 = mip ? 1.f - fl : 1.f;
-            if (want_tex) {
-                float* G0 = g_pyr + td.off[l0];
-                float w00 = wl0 * (1.f - f0.x) * (1.f - f0.y), w01 = wl0 * f0.x * (1.f - f0.y);
-                float w10 = wl0 * (1.f - f0.x) * f0.y, w11 = wl0 * f0.x * f0.y;
-                red_add4(G0 + 4 * q0[0], w00 * g.x, w00 * g.y, w00 * g.z, w00 * g.w);
-                red_add4(G0 + 4 * q0[1], w01 * g.x, w01 * g.y, w01 * g.z, w01 * g.w);
-                red_add4(G0 + 4 * q0[2], w10 * g.x, w10 * g.y, w10 * g.z, w10 * g.w);
-                red_add4(G0 + 4 * q0[3], w11 * g.x, w11 * g.y, w11 * g.z, w11 * g.w);
-                if (tri) {
-                    float* G1 = g_pyr + td.off[l1];
-                    float v00 = fl * (1.f - f1.x) * (1.f - f1.y), v01 = fl * f1.x * (1.f - f1.y);
-                    float v10 = fl * (1.f - f1.x) * f1.y, v11 = fl * f1.x * f1.y;
-                    red_add4(G1 + 4 * q1[0], v00 * g.x, v00 * g.y, v00 * g.z, v00 * g.w);
-                    red_add4(G1 + 4 * q1[1], v01 * g.x, v01 * g.y, v01 * g.z, v01 * g.w);
-                    red_add4(G1 + 4 * q1[2], v10 * g.x, v10 * g.y, v10 * g.z, v10 * g.w);
-                    red_add4(G1 + 4 * q1[3], v11 * g.x, v11 * g.y, v11 * g.z, v11 * g.w);
-                }
-            }
-            if (!want_geom) continue;
-            const float* T0 = a.pyr + td.off[l0];
-            const float* T1 = a.pyr + td.off[l1];
-            const float s0x = (float)(td.tw >> l0), s0y = (float)(td.th >> l0);
-            const float s1x = (float)(td.tw >> l1), s1y = (float)(td.th >> l1);
-            float4 a00 = ld4(T0, q0[0]), a01 = ld4(T0, q0[1]), a10 = ld4(T0, q0[2]), a11 = ld4(T0, q0[3]);
-            float4 b00 = a00, b01 = a00, b10 = a00, b11 = a00;
-            if (tri) { b00 = ld4(T1, q1[0]); b01 = ld4(T1, q1[1]); b10 = ld4(T1, q1[2]); b11 = ld4(T1, q1[3]); }
-            float gu = 0.f, gv = 0.f;
-            const float ga[4] = {g.x, g.y, g.z, g.w};
-            const float A00[4] = {a00.x, a00.y, a00.z, a00.w}, A01[4] = {a01.x, a01.y, a01.z, a01.w};
-            const float A10[4] = {a10.x, a10.y, a10.z, a10.w}, A11[4] = {a11.x, a11.y, a11.z, a11.w};
-            const float B00[4] = {b00.x, b00.y, b00.z, b00.w}, B01[4] = {b01.x, b01.y, b01.z, b01.w};
-            const float B10[4] = {b10.x, b10.y, b10.z, b10.w}, B11[4] = {b11.x, b11.y, b11.z, b11.w};
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], f0.y) * s0x;
-                float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], f0.x) * s0y;
-                if (tri) {
-                    du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], f1.y) * s1x, fl);
-                    dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], f1.x) * s1y, fl);
-                }
-                gu += du * ga[i];
-                gv += dv * ga[i];
-            }
-            // interpolate backward to the barycentrics (interpolate.cu:133-141)
-            float gbu = 0.f, gbv = 0.f;
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                float gi = i == 0 ? gu : gv;
-                float a2 = a.uvattr[2 * I.i2 + i];
-                gbu += gi * (a.uvattr[2 * I.i0 + i] - a2);
-                gbv += gi * (a.uvattr[2 * I.i1 + i] - a2);
-            }
-            if (((__float_as_uint(gbu) | __float_as_uint(gbv)) << 1) == 0u) continue;
-            // raster backward (rasterize.cu:84-141)
-            long long hw = (long long)a.W * a.H;
-            int view = (int)(p / hw);
-            int rem = (int)(p - view * hw);
-            int py = rem / a.W, px = rem - py * a.W;
-            const float xs = 2.f / (float)a.W, ys = 2.f / (float)a.H;
-            float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
-            float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
-            const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * a.nv;
-            float4 c0 = cv[I.i0], c1 = cv[I.i1], c2 = cv[I.i2];
-            float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
-            float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
-            float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
-            float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
-            float ar = e0x * e1y - e0y * e1x;
-            float ia = 1.f / (ar + (ar > 0 ? 1e-6f : -1e-6f));
-            float kuv = I.r.x * gbu + I.r.y * gbv;
-            float gx0 = (gbv * p2y + kuv * e1y) * ia, gy0 = (-gbv * p2x - kuv * e1x) * ia;
-            float gx1 = (-gbu * p2y - kuv * e0y) * ia, gy1 = (gbu * p2x + kuv * e0x) * ia;
-            float gx2 = ((-gbv * p0y + gbu * p1y) - kuv * (-p0y + p1y)) * ia;
-            float gy2 = ((gbv * p0x - gbu * p1x) - kuv * (p0x - p1x)) * ia;
-            float* gcv = g_clip + (size_t)view * a.nv * 4;
-            red_add4(gcv + (size_t)I.i0 * 4, gx0, gy0, 0.f, -gx0 * pxn - gy0 * pyn);
-            red_add4(gcv + (size_t)I.i1 * 4, gx1, gy1, 0.f, -gx1 * pxn - gy1 * pyn);
-            red_add4(gcv + (size_t)I.i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
+    for (int i = 0; i < 2; ++i) {
+        float a0 = a.uvattr[2 * i0 + i], a1 = a.uvattr[2 * i1 + i], a2 = a.uvattr[2 * i2 + i];
+        u[i] = (float)__dadd_rn((double)addr(mulr(a0, r.x), mulr(a1, r.y)), __dmul_rn((double)a2, l2));
+        float dadu = a0 - a2, dadv = a1 - a2;
+        dx[i] = addr(mulr(dadu, d.x), mulr(dadv, d.z));
+        dy[i] = addr(mulr(dadu, d.y), mulr(dadv, d.w));
+    }
+    const float2 uv = make_float2(u[0], u[1]);
+    int l0 = 0, l1 = 0;
+    float fl = 0.f;
+    const bool mip = td.L > 1;
+    if (mip) calc_level(td, make_float4(dx[0], dy[0], dx[1], dy[1]), l0, l1, fl, nullptr, 0);
+    int q0[4], q1[4];
+    float2 f0, f1 = make_float2(0.f, 0.f);
+    index_fetch(td, l0, uv, q0, f0);
+    const bool tri = mip && fl > 0;
+    if (tri) index_fetch(td, l1, uv, q1, f1);
+    const float wl0 = mip ? 1.f - fl : 1.f;
+    if (want_tex) {
+        float* G0 = g_pyr + td.off[l0];
+        float w00 = wl0 * (1.f - f0.x) * (1.f - f0.y), w01 = wl0 * f0.x * (1.f - f0.y);
+        float w10 = wl0 * (1.f - f0.x) * f0.y, w11 = wl0 * f0.x * f0.y;
+        red_add4(G0 + 4 * q0[0], w00 * g.x, w00 * g.y, w00 * g.z, w00 * g.w);
+        red_add4(G0 + 4 * q0[1], w01 * g.x, w01 * g.y, w01 * g.z, w01 * g.w);
+        red_add4(G0 + 4 * q0[2], w10 * g.x, w10 * g.y, w10 * g.z, w10 * g.w);
+        red_add4(G0 + 4 * q0[3], w11 * g.x, w11 * g.y, w11 * g.z, w11 * g.w);
+        if (tri) {
+            float* G1 = g_pyr + td.off[l1];
+            float v00 = fl * (1.f - f1.x) * (1.f - f1.y), v01 = fl * f1.x * (1.f - f1.y);
+            float v10 = fl * (1.f - f1.x) * f1.y, v11 = fl * f1.x * f1.y;
+            red_add4(G1 + 4 * q1[0], v00 * g.x, v00 * g.y, v00 * g.z, v00 * g.w);
+            red_add4(G1 + 4 * q1[1], v01 * g.x, v01 * g.y, v01 * g.z, v01 * g.w);
+            red_add4(G1 + 4 * q1[2], v10 * g.x, v10 * g.y, v10 * g.z, v10 * g.w);
+            red_add4(G1 + 4 * q1[3], v11 * g.x, v11 * g.y, v11 * g.z, v11 * g.w);
         }
     }
-    if (!lobe_grads) return;
+    if (!want_geom) return;
+    const float* T0 = a.pyr + td.off[l0];
+    const float* T1 = a.pyr + td.off[l1];
+    const float s0x = (float)(td.tw >> l0), s0y = (float)(td.th >> l0);
+    const float s1x = (float)(td.tw >> l1), s1y = (float)(td.th >> l1);
+    const float4 a00 = ld4(T0, q0[0]), a01 = ld4(T0, q0[1]), a10 = ld4(T0, q0[2]), a11 = ld4(T0, q0[3]);
+    float4 b00 = a00, b01 = a00, b10 = a00, b11 = a00;
+    if (tri) { b00 = ld4(T1, q1[0]); b01 = ld4(T1, q1[1]); b10 = ld4(T1, q1[2]); b11 = ld4(T1, q1[3]); }
+    const float ga[4] = {g.x, g.y, g.z, g.w};
+    const float A00[4] = {a00.x, a00.y, a00.z, a00.w}, A01[4] = {a01.x, a01.y, a01.z, a01.w};
+    const float A10[4] = {a10.x, a10.y, a10.z, a10.w}, A11[4] = {a11.x, a11.y, a11.z, a11.w};
+    const float B00[4] = {b00.x, b00.y, b00.z, b00.w}, B01[4] = {b01.x, b01.y, b01.z, b01.w};
+    const float B10[4] = {b10.x, b10.y, b10.z, b10.w}, B11[4] = {b11.x, b11.y, b11.z, b11.w};
+    float gu = 0.f, gv = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], f0.y) * s0x;
+        float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], f0.x) * s0y;
+        if (tri) {
+            du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], f1.y) * s1x, fl);
+            dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], f1.x) * s1y, fl);
+        }
+        gu += du * ga[i];
+        gv += dv * ga[i];
+    }
+    float gbu = 0.f, gbv = 0.f;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        float gi = i == 0 ? gu : gv;
+        float a2 = a.uvattr[2 * i2 + i];
+        gbu += gi * (a.uvattr[2 * i0 + i] - a2);
+        gbv += gi * (a.uvattr[2 * i1 + i] - a2);
+    }
+    if (((__float_as_uint(gbu) | __float_as_uint(gbv)) << 1) == 0u) return;
+    const long long hw = (long long)a.W * a.H;
+    const int view = (int)(p / hw);
+    const int rem = (int)(p - view * hw);
+    const int py = rem / a.W, px = rem - py * a.W;
+    const float xs = 2.f / (float)a.W, ys = 2.f / (float)a.H;
+    const float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
+    const float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
+    const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * a.nv;
+    const float4 c0 = cv[i0], c1 = cv[i1], c2 = cv[i2];
+    float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
+    float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
+    float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
+    float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
+    float ar = e0x * e1y - e0y * e1x;
+    float ia = 1.f / (ar + (ar > 0 ? 1e-6f : -1e-6f));
+    float kuv = r.x * gbu + r.y * gbv;
+    float gx0 = (gbv * p2y + kuv * e1y) * ia, gy0 = (-gbv * p2x - kuv * e1x) * ia;
+    float gx1 = (-gbu * p2y - kuv * e0y) * ia, gy1 = (gbu * p2x + kuv * e0x) * ia;
+    float gx2 = ((-gbv * p0y + gbu * p1y) - kuv * (-p0y + p1y)) * ia;
+    float gy2 = ((gbv * p0x - gbu * p1x) - kuv * (p0x - p1x)) * ia;
+    float* gcv = g_clip + (size_t)view * a.nv * 4;
+    red_add4(gcv + (size_t)i0 * 4, gx0, gy0, 0.f, -gx0 * pxn - gy0 * pyn);
+    red_add4(gcv + (size_t)i1 * 4, gx1, gy1, 0.f, -gx1 * pxn - gy1 * pyn);
+    red_add4(gcv + (size_t)i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
+}
+
+// Lobe gradients (material.cu:428-433): lobe-parallel over staged pixels whose
+// shading inputs are recomputed from the raster output.  C = 4.
+template <int NL>
+__global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
+                                                  int nacc, float* __restrict__ g_axis, float* __restrict__ g_sharp,
+                                                  float* __restrict__ g_amp) {
+    extern __shared__ float sm[];
+    const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int K = a.K;
+    float* s_acc = sm;
+    SPix* s_pix = reinterpret_cast<SPix*>(sm + (size_t)K * nacc);
+    for (int i = threadIdx.x; i < K * nacc; i += blockDim.x) s_acc[i] = 0.f;
     __syncthreads();
-    sg_flush_lobes(s_acc, nwarps, K, 4, nacc, g_axis, g_sharp, g_amp, nullptr);
+    const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
+    LaneLobes<NL, 4> LL;
+    lane_lobes_load<NL, 4>(LL, li, Kp, K, 4, a.axis, a.sharp, a.amp);
+    SPix* st = s_pix + wid * 32;
+    const long long nchunks = (a.npix + 31) / 32;
+    for (long long chunk = (long long)blockIdx.x * nwarps + wid; chunk < nchunks; chunk += (long long)gridDim.x * nwarps) {
+        const long long p = chunk * 32 + lane;
+        PixIn q;
+        const bool live = p < a.npix && shade_inputs<1>(a, td, p, q);
+        const unsigned ball = __ballot_sync(0xffffffffu, live);
+        const int m = __popc(ball);
+        if (live) {
+            SPix& z = st[__popc(ball & ((1u << lane) - 1u))];
+            z.n[0] = q.n.x; z.n[1] = q.n.y; z.n[2] = q.n.z;
+            z.pax[0] = q.pax.x; z.pax[1] = q.pax.y; z.pax[2] = q.pax.z;
+            z.ss = q.ss; z.sa = q.sa;
+            z.dfs[0] = q.dfs.x; z.dfs[1] = q.dfs.y; z.dfs[2] = q.dfs.z; z.dfs[3] = q.dfs.w;
+            const float4 gc = g_color[p];
+            z.go[0] = gc.x; z.go[1] = gc.y; z.go[2] = gc.z; z.go[3] = gc.w;
+        }
+        __syncwarp();
+        if (m > 0) sg_bwd_lanes<NL, 4, false>(LL, 4, 0, st, nullptr, m, Kp, g, G, li);
+        __syncwarp();
+    }
+    lane_lobes_flush<NL, 4>(LL, 4, Kp, li, s_acc, nacc, false);
+    __syncthreads();
+    sg_flush_block(s_acc, K, 4, nacc, g_axis, g_sharp, g_amp, nullptr);
 }
 
 DEV float4 nan_add4(float4 a, float4 b) {
@@ -445,7 +461,9 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
 #define TRY(x) do { vcl_status _s = (x); if (_s) return _s; } while (0)
 
 size_t shade_smem(int K) { return sizeof(float) * (size_t)K * 8; }
-size_t bwd_smem(int K, int nacc) { return sizeof(float) * ((size_t)K * 8 + (size_t)8 * K * nacc); }
+size_t lobes_smem(int K, int nacc, int threads) {
+    return sizeof(float) * (size_t)K * nacc + (size_t)(threads / 32) * 32 * sizeof(SPix);
+}
 
 vcl_status fused_init(vcl_fit* f) {
     if (f->fused) return VCL_OK;
@@ -466,9 +484,10 @@ vcl_status fused_init(vcl_fit* f) {
         return vcl_fail(ctx, VCL_ERR_NOMEM, "fused fit state: %s", cudaGetErrorString(e));
     }
     f->fused = F;
-    const int nacc = 4 + 4 + 1;
-    size_t sb = bwd_smem(d.K, nacc);
-    if (sb > 48 * 1024) cudaFuncSetAttribute(k_fused_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+    e = cudaStreamCreateWithFlags(&F->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F->join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "fused streams");
     size_t sf = shade_smem(d.K);
     if (sf > 48 * 1024) cudaFuncSetAttribute(k_shade_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
     return vcl_cuda_check(ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice), "fused init");
@@ -494,7 +513,8 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     a.W = W; a.H = H; a.npix = N; a.rough = d.roughness; a.ior = d.ior;
     a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
     TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
-    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->aa);
+    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->aa,
+                                                                   (float4*)f->diffuse);
     TRY(vcl_launch_check(ctx, "fused shade"));
     TRY(aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
     int grid = ctx->sm_count * 4;
@@ -505,12 +525,36 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
                      d.learn_pos ? f->g_clip : nullptr, s));
     const bool lobes = d.learn_lobes && d.K;
     const int nacc = 4 + 4 + 1;
-    long long blocks = (N + 256 * FP - 1) / (256 * FP);
-    int bgrid = (int)(blocks < ctx->sm_count * 2 ? (blocks < 1 ? 1 : blocks) : ctx->sm_count * 2);
-    k_fused_bwd<<<bgrid, 256, bwd_smem(d.K, nacc), s>>>(a, td, (const float4*)f->g_color, f->g_pyr, f->clip, f->g_clip,
-                                                        lobes ? f->g_axis : nullptr, lobes ? f->g_sharp : nullptr,
-                                                        lobes ? f->g_amp : nullptr, nacc, d.learn_tex, d.learn_pos);
-    TRY(vcl_launch_check(ctx, "fused backward"));
+    // the lobe gradients run beside the per-pixel backward on a forked stream
+    if (lobes) {
+        TRY(vcl_cuda_check(ctx, cudaEventRecord(F->fork, s), "fork"));
+        TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(F->side, F->fork, 0), "fork"));
+        const int Kp = sg_lobe_group(d.K);
+        const int NL = (d.K + 31) / 32;
+        const int lthreads = 128;
+        long long chunks = (N + 31) / 32;
+        long long want = (chunks + 3) / 4;
+        long long capg = (long long)ctx->sm_count * 6;
+        int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
+        size_t lsm = lobes_smem(d.K, nacc, lthreads);
+        if (NL <= 1)
+            k_sg_lobes<1><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+                                                               f->g_sharp, f->g_amp);
+        else if (NL <= 2)
+            k_sg_lobes<2><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+                                                               f->g_sharp, f->g_amp);
+        else
+            k_sg_lobes<4><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+                                                               f->g_sharp, f->g_amp);
+        TRY(vcl_launch_check(ctx, "fused lobe gradients"));
+        TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));
+    }
+    if (d.learn_tex || d.learn_pos) {
+        k_bwd_pix<<<vcl_blocks(N, 256), 256, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
+                                                     f->g_pyr, f->clip, f->g_clip, d.learn_tex, d.learn_pos);
+        TRY(vcl_launch_check(ctx, "fused backward"));
+    }
+    if (lobes) TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join"));
     if (d.learn_pos) TRY(vcl_project_bwd(ctx, f->mvp, V, f->g_clip, d.nv, 4, f->g_pos, s));
     AdamArgs aa{d.beta1, d.beta2, d.lr, d.eps, F->d_corr};
     const float wpush = ctx->mode == VCL_MODE_EXACT ? 0.25f : 1.f;
@@ -581,7 +625,9 @@ vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
 int fit_fused_launches(const vcl_fit* f) {
     const vcl_fit_desc& d = f->d;
     int n = 1 /* begin */ + 1 /* project */ + raster_fwd_launches() + 1 /* shade */ + 1 /* aa */ + 1 /* mse */ +
-            1 /* aa bwd */ + 1 /* fused bwd */;
+            1 /* aa bwd */;
+    if (d.learn_tex || d.learn_pos) n += 1; /* per-pixel backward */
+    if (d.learn_lobes && d.K) n += 1;       /* lobe gradients */
     if (d.learn_pos) n += 1;
     if (d.learn_tex) {
         const bool tile = d.tex_w % 32 == 0 && d.tex_h % 32 == 0 && d.levels >= 2;
@@ -599,6 +645,9 @@ void fit_fused_release(vcl_fit* f) {
     if (F->raster_ws) cudaFree(F->raster_ws);
     if (F->d_step) cudaFree(F->d_step);
     if (F->d_corr) cudaFree(F->d_corr);
+    if (F->side) cudaStreamDestroy(F->side);
+    if (F->fork) cudaEventDestroy(F->fork);
+    if (F->join) cudaEventDestroy(F->join);
     delete F;
     f->fused = nullptr;
 }

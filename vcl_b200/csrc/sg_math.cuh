@@ -293,3 +293,167 @@ DEV void sg_flush_lobes(const float* s_acc, int nwarps, int K, int C, int nacc, 
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Lobe-parallel SG backward.  A warp stages up to 32 covered pixels in shared
+// memory, then its lanes walk those pixels with one lobe per lane: the
+// per-lobe gradient sums (axis, sharpness, amplitude -- sums over all
+// pixels) accumulate in registers with no reduction per pixel, and the
+// per-pixel gradients (sums over lobes) are reduced across the lanes of a
+// lobe group only when they are requested.  With K <= 16 the warp splits
+// into 32/Kp groups (Kp = next power of two >= K) that take different
+// pixels; with K > 32 each lane carries NL lobes.
+struct SPix {
+    float n[3], pax[3], ss, sa;
+    float dfs[SG_CMAX], go[SG_CMAX];
+};
+
+struct SPixOut { float gd[SG_CMAX], gsa[SG_CMAX], gsx[3], gsh; };
+
+template <int NL, int CC>
+struct LaneLobes {
+    bool valid[NL];
+    float gs[NL];
+    float3 sgn[NL];
+    float a[NL][CC ? CC : SG_CMAX];
+    float acc_ax[NL][3], acc_sh[NL], acc_ssh[NL];
+    float acc_am[NL][CC ? CC : SG_CMAX];
+};
+
+template <int NL, int CC>
+DEV void lane_lobes_load(LaneLobes<NL, CC>& LL, int li, int Kp, int K, int C, const float* axis, const float* sharp,
+                         const float* amp) {
+    const int Cn = CC ? CC : C;
+#pragma unroll
+    for (int s = 0; s < NL; ++s) {
+        int i = li + s * Kp;
+        LL.valid[s] = i < K;
+        int ii = LL.valid[s] ? i : 0;
+        float gs = K ? sharp[ii] : 0.f;
+        LL.gs[s] = gs;
+        LL.sgn[s] = K ? f3(axis[3 * ii] * gs, axis[3 * ii + 1] * gs, axis[3 * ii + 2] * gs) : f3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) LL.a[s][k] = (k < Cn && K) ? amp[ii * C + k] : 0.f;
+        LL.acc_ax[s][0] = LL.acc_ax[s][1] = LL.acc_ax[s][2] = 0.f;
+        LL.acc_sh[s] = LL.acc_ssh[s] = 0.f;
+#pragma unroll
+        for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) LL.acc_am[s][k] = 0.f;
+    }
+}
+
+// Sum over the lanes of one lobe group (offsets below Kp).
+DEV float group_sum(float v, int Kp) {
+    for (int o = Kp >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Processes the m staged pixels of this warp.  PIX: also produce the
+// per-pixel gradients into `out` (diffuse, specular amplitude/axis/sharpness).
+template <int NL, int CC, bool PIX>
+DEV void sg_bwd_lanes(LaneLobes<NL, CC>& LL, int C, int exact, const SPix* st, SPixOut* out, int m, int Kp, int g,
+                      int G, int li) {
+    const int Cn = CC ? CC : C;
+    const int rounds = (m + G - 1) / G;
+    for (int rr = 0; rr < rounds; ++rr) {
+        const int j = rr * G + g;
+        const bool ok = j < m;
+        const SPix& P = st[ok ? j : 0];
+        float pgd[CC ? CC : SG_CMAX], pgsa[CC ? CC : SG_CMAX], pgsx[3] = {0.f, 0.f, 0.f}, pgsh = 0.f;
+#pragma unroll
+        for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) { pgd[k] = 0.f; pgsa[k] = 0.f; }
+        if (ok) {
+            const float3 n = f3(P.n[0], P.n[1], P.n[2]), pax = f3(P.pax[0], P.pax[1], P.pax[2]);
+            const float ss = P.ss, sa = P.sa;
+            const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+#pragma unroll
+            for (int s = 0; s < NL; ++s) {
+                if (!LL.valid[s]) continue;
+                SGB t = sg_bwd_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa);
+                float sum = 0.f, sumd = 0.f, sum_sa = 0.f;
+#pragma unroll
+                for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
+                    if (k >= Cn) break;
+                    const float a = LL.a[s][k], gk = P.go[k], dk = P.dfs[k];
+                    sum += gk * a;
+                    sumd += gk * a * dk;
+                    LL.acc_am[s][k] += finite_or0(gk * (t.dg * dk + t.sgv));
+                    if (PIX) {
+                        pgd[k] += gk * t.dg * a;
+                        if (!exact) pgsa[k] += gk * t.sgv * a;
+                        else sum_sa += gk * t.sil_e * a;
+                    }
+                }
+                float3 cax = ((t.ddg * sumd) * SG_DIFF_AMP + (t.dsg * sum) * sa) * LL.gs[s];
+                if (fin3(cax)) { LL.acc_ax[s][0] += cax.x; LL.acc_ax[s][1] += cax.y; LL.acc_ax[s][2] += cax.z; }
+                LL.acc_sh[s] += finite_or0(sumd * t.ddgs * SG_DIFF_AMP + sum * t.dsgs * sa);
+                const float cssh = sum * t.dsgss * sa;
+                if (!exact) LL.acc_ssh[s] += finite_or0(cssh);
+                if (PIX) {
+                    if (exact) { pgsa[0] += sum_sa; pgsh += cssh; }
+                    float3 csx = ((t.dsg * sum) * sa) * ss;
+                    pgsx[0] += csx.x; pgsx[1] += csx.y; pgsx[2] += csx.z;
+                }
+            }
+        }
+        if (PIX) {
+#pragma unroll
+            for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
+                if (k >= Cn) break;
+                pgd[k] = group_sum(pgd[k], Kp);
+                pgsa[k] = group_sum(pgsa[k], Kp);
+            }
+            pgsx[0] = group_sum(pgsx[0], Kp); pgsx[1] = group_sum(pgsx[1], Kp); pgsx[2] = group_sum(pgsx[2], Kp);
+            pgsh = group_sum(pgsh, Kp);
+            if (ok && li == 0) {
+                SPixOut& o = out[j];
+                for (int k = 0; k < Cn; ++k) { o.gd[k] = pgd[k]; o.gsa[k] = pgsa[k]; }
+                o.gsx[0] = pgsx[0]; o.gsx[1] = pgsx[1]; o.gsx[2] = pgsx[2];
+                o.gsh = pgsh;
+            }
+        }
+    }
+}
+
+// Adds this lane's lobe sums into the block accumulator s_acc [K][nacc]
+// (after folding the lobe groups of the warp together).
+template <int NL, int CC>
+DEV void lane_lobes_flush(LaneLobes<NL, CC>& LL, int C, int Kp, int li, float* s_acc, int nacc, bool ssh_lobe) {
+    const int Cn = CC ? CC : C;
+#pragma unroll
+    for (int s = 0; s < NL; ++s) {
+        float v[3 + 1 + SG_CMAX + 1];
+        v[0] = LL.acc_ax[s][0]; v[1] = LL.acc_ax[s][1]; v[2] = LL.acc_ax[s][2]; v[3] = LL.acc_sh[s];
+        for (int k = 0; k < SG_CMAX; ++k) v[4 + k] = k < Cn ? LL.acc_am[s][k] : 0.f;
+        v[4 + SG_CMAX] = LL.acc_ssh[s];
+        for (int q = 0; q < 4 + SG_CMAX + 1; ++q)
+            for (int o = 16; o >= Kp; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        const int lane = threadIdx.x & 31;
+        if (lane < Kp && LL.valid[s]) {
+            const int i = li + s * Kp;
+            float* a = s_acc + (size_t)i * nacc;
+            atomicAdd(&a[0], v[0]); atomicAdd(&a[1], v[1]); atomicAdd(&a[2], v[2]); atomicAdd(&a[3], v[3]);
+            for (int k = 0; k < Cn; ++k) atomicAdd(&a[4 + k], v[4 + k]);
+            if (ssh_lobe) atomicAdd(&a[4 + Cn], v[4 + SG_CMAX]);
+        }
+    }
+}
+
+// Block accumulator [K][nacc] -> global lobe gradients.
+DEV void sg_flush_block(const float* s_acc, int K, int C, int nacc, float* gaxis, float* gsharp, float* gamp,
+                        float* gssh_lobe) {
+    for (int j = threadIdx.x; j < K * nacc; j += blockDim.x) {
+        float v = s_acc[j];
+        if (v == 0.f) continue;
+        int i = j / nacc, q = j % nacc;
+        if (q < 3) { if (gaxis) atomicAdd(&gaxis[3 * i + q], v); }
+        else if (q == 3) { if (gsharp) atomicAdd(&gsharp[i], v); }
+        else if (q < 4 + C) { if (gamp) atomicAdd(&gamp[i * C + (q - 4)], v); }
+        else if (gssh_lobe) atomicAdd(&gssh_lobe[i], v);
+    }
+}
+
+inline int sg_lobe_group(int K) {
+    int kp = 1;
+    while (kp < K && kp < 32) kp <<= 1;
+    return kp;
+}

@@ -188,6 +188,105 @@ __global__ void __launch_bounds__(256) k_sg_bwd(int C, int K, int nacc, const fl
     sg_flush_lobes(s_acc, nwarps, K, C, nacc, gaxis, gsharp, gamp, exact ? nullptr : gssh);
 }
 
+// Lobe-parallel SG backward (see sg_bwd_lanes): one lobe per lane, pixels
+// staged per warp in shared memory, per-lobe sums in registers.
+template <int NL, int CC>
+__global__ void __launch_bounds__(128) k_sg_bwd_lp(int C, int K, int Kp, int nacc, const float* __restrict__ axis,
+                                                   const float* __restrict__ sharp, const float* __restrict__ amp,
+                                                   const float4* __restrict__ rast, long long npix,
+                                                   const float* __restrict__ normal, const float* __restrict__ diffuse,
+                                                   const float* __restrict__ sax, const float* __restrict__ ssh,
+                                                   const float* __restrict__ sam, const float* __restrict__ gout,
+                                                   float* __restrict__ gdiff, float* __restrict__ gaxis,
+                                                   float* __restrict__ gsharp, float* __restrict__ gamp,
+                                                   float* __restrict__ gsax, float* __restrict__ gssh,
+                                                   float* __restrict__ gsam, int exact) {
+    extern __shared__ float sm[];
+    const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Cn = CC ? CC : C;
+    float* s_acc = sm;                                            // [K][nacc]
+    float* s_lob = sm + (size_t)K * nacc;                         // lobes for the guarded fallback
+    SPix* s_pix = reinterpret_cast<SPix*>(s_lob + (size_t)K * (4 + C));
+    SPixOut* s_out = reinterpret_cast<SPixOut*>(s_pix + nwarps * 32);
+    for (int i = threadIdx.x; i < K * nacc; i += blockDim.x) s_acc[i] = 0.f;
+    const SGLobes L = sg_stage_lobes(s_lob, K, C, axis, sharp, amp);
+    __syncthreads();
+    const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
+    LaneLobes<NL, CC> LL;
+    lane_lobes_load<NL, CC>(LL, li, Kp, K, C, axis, sharp, amp);
+    const bool pix_out = gdiff || gsax || gssh || gsam;
+    SPix* st = s_pix + wid * 32;
+    SPixOut* so = s_out + wid * 32;
+    const long long nchunks = (npix + 31) / 32;
+    for (long long chunk = (long long)blockIdx.x * nwarps + wid; chunk < nchunks; chunk += (long long)gridDim.x * nwarps) {
+        const long long p = chunk * 32 + lane;
+        const bool live = p < npix && rast_id(rast[p].w) >= 0;
+        const unsigned ball = __ballot_sync(0xffffffffu, live);
+        const int m = __popc(ball);
+        const int slot = __popc(ball & ((1u << lane) - 1u));
+        if (live) {
+            SPix& z = st[slot];
+            float3 n = ld3(normal, p), pa = ld3(sax, p);
+            z.n[0] = n.x; z.n[1] = n.y; z.n[2] = n.z;
+            z.pax[0] = pa.x; z.pax[1] = pa.y; z.pax[2] = pa.z;
+            z.ss = ssh[p]; z.sa = sam[p];
+            for (int k = 0; k < Cn; ++k) { z.dfs[k] = diffuse[p * Cn + k]; z.go[k] = gout[p * Cn + k]; }
+        }
+        __syncwarp();
+        if (m > 0) {
+            if (pix_out) sg_bwd_lanes<NL, CC, true>(LL, C, exact, st, so, m, Kp, g, G, li);
+            else sg_bwd_lanes<NL, CC, false>(LL, C, exact, st, so, m, Kp, g, G, li);
+        }
+        __syncwarp();
+        if (pix_out && live) {
+            const SPixOut& o = so[slot];
+            const SPix& z = st[slot];
+            float gd0[SG_CMAX], gsa0[SG_CMAX], gd[SG_CMAX], gsa[SG_CMAX];
+            float3 gsx0 = gsax ? ld3(gsax, p) : f3(0.f, 0.f, 0.f);
+            float gsh0 = (gssh && exact) ? gssh[p] : 0.f;
+            bool ok = true;
+            for (int k = 0; k < Cn; ++k) {
+                gd0[k] = gdiff ? gdiff[p * Cn + k] : 0.f;
+                gsa0[k] = (gsam && !exact) ? gsam[p * Cn + k] : 0.f;
+                gd[k] = gd0[k] + o.gd[k];
+                gsa[k] = gsa0[k] + o.gsa[k];
+                ok = ok && isfinite(o.gd[k]) && isfinite(gd[k]) && isfinite(o.gsa[k]) && isfinite(gsa[k]);
+            }
+            if (gsam && exact) { gsa0[0] = gsam[p]; gsa[0] = gsa0[0] + o.gsa[0]; ok = ok && isfinite(gsa[0]); }
+            float3 gsx = gsx0 + f3(o.gsx[0], o.gsx[1], o.gsx[2]);
+            float gsh = gsh0 + o.gsh;
+            ok = ok && fin3(gsx) && isfinite(gsh);
+            if (!ok) {
+                // some partial sum left the finite range: redo this pixel in the
+                // reference's guarded order
+                SGPix q;
+                q.n = f3(z.n[0], z.n[1], z.n[2]); q.pax = f3(z.pax[0], z.pax[1], z.pax[2]);
+                q.ss = z.ss; q.sa = z.sa;
+                for (int k = 0; k < SG_CMAX; ++k) { q.dfs[k] = k < Cn ? z.dfs[k] : 0.f; q.go[k] = k < Cn ? z.go[k] : 0.f; }
+                sg_bwd_pixel_slow<CC>(L, K, C, exact, q, gd0, gsa0, gsx0, gsh0);
+                for (int k = 0; k < Cn; ++k) { gd[k] = q.gd[k]; gsa[k] = q.gsa[k]; }
+                gsx = q.gsx; gsh = q.gsh;
+            }
+            for (int k = 0; k < Cn; ++k) {
+                if (gdiff) gdiff[p * Cn + k] = gd[k];
+                if (gsam && !exact) gsam[p * Cn + k] = gsa[k];
+            }
+            if (gsax) st3(gsax, p, gsx);
+            if (gsam && exact) gsam[p] = gsa[0];
+            if (gssh && exact) gssh[p] = gsh;
+        }
+        __syncwarp();
+    }
+    lane_lobes_flush<NL, CC>(LL, C, Kp, li, s_acc, nacc, !exact && gssh);
+    __syncthreads();
+    sg_flush_block(s_acc, K, C, nacc, gaxis, gsharp, gamp, exact ? nullptr : gssh);
+}
+
+size_t sg_bwd_lp_smem(int K, int C, int nacc, int threads) {
+    return sizeof(float) * ((size_t)K * nacc + (size_t)K * (4 + C)) +
+           (size_t)(threads / 32) * 32 * (sizeof(SPix) + sizeof(SPixOut));
+}
+
 size_t sg_fwd_smem(int K, int C) { return sizeof(float) * (size_t)K * (4 + C); }
 size_t sg_bwd_smem(int K, int C, int nacc, int threads) {
     return sizeof(float) * ((size_t)K * (4 + C) + (size_t)(threads / 32) * K * nacc);
@@ -282,6 +381,25 @@ VCL_API vcl_status vcl_sg_bwd(vcl_ctx* ctx, const float* rast, int W, int H, int
     size_t smem = sg_bwd_smem(K, C, nacc, threads);
     VCL_REQUIRE(smem <= 200 * 1024, "too many lobes for the shared-memory reduction (K=%d)", K);
     VCL_REQUIRE(C == 4 || C <= CMAX, "channel count");
+    if (K <= 128) {
+        const int Kp = sg_lobe_group(K > 0 ? K : 1);
+        const int NL = (K + 31) / 32;
+        const int lthreads = 128;
+        size_t lsmem = sg_bwd_lp_smem(K, C, nacc, lthreads);
+        decltype(&k_sg_bwd_lp<1, 4>) lk;
+        if (C == 4) lk = NL <= 1 ? k_sg_bwd_lp<1, 4> : NL <= 2 ? k_sg_bwd_lp<2, 4> : k_sg_bwd_lp<4, 4>;
+        else lk = NL <= 1 ? k_sg_bwd_lp<1, 0> : NL <= 2 ? k_sg_bwd_lp<2, 0> : k_sg_bwd_lp<4, 0>;
+        if (lsmem > 48 * 1024) cudaFuncSetAttribute(lk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem);
+        long long chunks = (npix + 31) / 32;
+        long long want = (chunks + lthreads / 32 - 1) / (lthreads / 32);
+        long long cap = (long long)ctx->sm_count * 8;
+        int lgrid = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
+        lk<<<lgrid, lthreads, lsmem, (cudaStream_t)stream>>>(
+            C, K, Kp, nacc, axis, sharpness, amplitude, (const float4*)rast, npix, normal, diffuse, spec_axis,
+            spec_sharpness, spec_amplitude, grad_out, grad_diffuse, grad_axis, grad_sharpness, grad_amplitude,
+            grad_spec_axis, grad_spec_sharpness, grad_spec_amplitude, exact);
+        return vcl_launch_check(ctx, "sg_bwd");
+    }
     auto kern = C == 4 ? k_sg_bwd<4> : k_sg_bwd<0>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     long long blocks = (npix + threads * SGB_P - 1) / (threads * SGB_P);
