@@ -6,13 +6,15 @@
 //   project      clip-space positions
 //   raster       setup / scan / emit / fine (own workspace)
 //   shade_fwd    interpolate(uv, DA) + texture + NormalAxis + ViewAxis +
-//                SGSpecular + SG per pixel -> color (and the AA input copy)
-//   aa edges     silhouette blending (atomics)
-//   mse_init     grad = aa - target, loss, and the AA-backward input copy
-//   aa edges bwd colour and clip-position gradients at silhouettes
-//   fused_bwd    per pixel: recompute the shading inputs, SG backward (lobe
-//                gradients block-reduced), texture backward (texel atomics),
-//                interpolate backward, raster backward (clip atomics)
+//                SGSpecular + SG per pixel -> color, diffuse environment sum
+//   antialias    silhouette blending (gather form, deterministic)
+//   mse          grad = aa - target and the loss
+//   aa bwd       colour and clip-position gradients at silhouettes
+//   bwd_pix      per pixel: diffuse gradient = grad * diffuse environment,
+//                texture backward (texel atomics), interpolate backward,
+//                raster backward (clip atomics)
+//   sg_lobes     lobe gradients, lobe-parallel, on a forked stream beside
+//                bwd_pix
 //   project bwd  position gradients
 //   adam_tex     mip gradient push-down + Adam + clamp on texture level 0,
 //                gradient clear, and mip levels 1..5 of each 32x32 tile
@@ -133,10 +135,10 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
     return true;
 }
 
-// Forward shading of every pixel; writes the color and the antialias input
-// copy (antialias.cu:62-65).  C = 4 texture/lobe channels.
+// Forward shading of every pixel; writes the color and the diffuse
+// environment sum (kept for the backward's diffuse gradient).  C = 4.
 __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
-                                                   float4* __restrict__ aa, float4* __restrict__ diffenv) {
+                                                   float4* __restrict__ diffenv) {
     extern __shared__ float sm[];
     const SGLobes L = sg_stage_lobes(sm, a.K, 4, a.axis, a.sharp, a.amp);
     __syncthreads();
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
     if (p >= a.npix) return;
     PixIn q;
     if (!shade_inputs<1>(a, td, p, q)) {
-        color[p] = aa[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        color[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
     float de[SG_CMAX], se[SG_CMAX];
@@ -153,19 +155,17 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
     float4 c = make_float4(q.dfs.x * de[0] + se[0], q.dfs.y * de[1] + se[1], q.dfs.z * de[2] + se[2],
                            q.dfs.w * de[3] + se[3]);
     color[p] = c;
-    aa[p] = c;
 }
 
-// loss.cu:22-30 plus the antialias-backward input copy (antialias.cu:267-269).
+// loss.cu:22-30: gradient and loss in one pass.
 __global__ void k_mse_init(const float4* __restrict__ aa, const float4* __restrict__ tgt, long long n4,
-                           float4* __restrict__ g_aa, float4* __restrict__ g_color, float* __restrict__ loss) {
+                           float4* __restrict__ g_aa, float* __restrict__ loss) {
     __shared__ double part[32];
     double acc = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
         float4 a = aa[i], t = tgt[i];
         float4 g = make_float4(a.x - t.x, a.y - t.y, a.z - t.z, a.w - t.w);
         g_aa[i] = g;
-        g_color[i] = g;
         acc += (double)g.x * g.x + (double)g.y * g.y + (double)g.z * g.z + (double)g.w * g.w;
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -513,13 +513,11 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     a.W = W; a.H = H; a.npix = N; a.rough = d.roughness; a.ior = d.ior;
     a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
     TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
-    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->aa,
-                                                                   (float4*)f->diffuse);
+    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse);
     TRY(vcl_launch_check(ctx, "fused shade"));
     TRY(aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
     int grid = ctx->sm_count * 4;
-    k_mse_init<<<grid, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N, (float4*)f->g_aa,
-                                    (float4*)f->g_color, f->loss);
+    k_mse_init<<<grid, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N, (float4*)f->g_aa, f->loss);
     TRY(vcl_launch_check(ctx, "fused mse"));
     TRY(aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
                      d.learn_pos ? f->g_clip : nullptr, s));

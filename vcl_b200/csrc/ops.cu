@@ -353,6 +353,38 @@ DEV bool aa_edge(float2 pa, float2 pb, float2 o, float& a, float& alpha, float& 
     return true;
 }
 
+// One horizontal (dir 0: o = q-1) or vertical (dir 1: o = q-W) pixel pair
+// as antialias.cu:66-92 / :273-296 evaluate it at pixel q: which side is
+// drawn in front (pp), the other side (op), and pp's triangle in pixel
+// units around the shared pixel edge.  `typo` reproduces :279 (the current
+// pixel's id used for both sides of a horizontal pair).
+struct AAPair {
+    long long pp, op;
+    float2 o;
+    AATri t;
+};
+
+DEV bool aa_pair(const float4* __restrict__ proj, int nv, const uint32_t* __restrict__ tri, int nt,
+                 const float4* __restrict__ rast, long long q, int qx, int qy, int W, int dir, bool typo, float2 s,
+                 AAPair& P, int* flags) {
+    const long long oidx = dir == 0 ? q - 1 : q - W;
+    const float4 tr = rast[q], to = rast[oidx];
+    if (to.w == tr.w) return false;
+    long long pp = (int)tr.w ? q : oidx;
+    long long op = (int)((dir == 0 && typo) ? tr.w : to.w) ? q : oidx;
+    if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
+    float2 f;
+    if (dir == 0) { f = make_float2((float)qx + (pp > op ? .5f : -.5f), (float)qy + .5f); P.o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
+    else { f = make_float2((float)qx + .5f, (float)qy + (pp > op ? .5f : -.5f)); P.o = make_float2(0.f, pp > op ? -1.f : 1.f); }
+    P.pp = pp;
+    P.op = op;
+    return aa_fetch(proj, nv, tri, nt, rast, pp, s, f, P.t, flags);
+}
+
+// Forward antialias as a gather: each pixel evaluates the (up to four)
+// pairs it belongs to and adds the edge terms the reference sends to it
+// (antialias.cu:28-34), in a fixed order -- deterministic, no atomics, and
+// out = in + terms in one pass (the reference's init store, :62-65).
 template <int C4>
 __global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
                          const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
@@ -366,36 +398,41 @@ __global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t
     int py = rem / W, px = rem - py * W;
     const float4* proj = clip + (size_t)view * nv;
     const float2 s = make_float2(W / 2.f, H / 2.f);
-    float4 tr = rast[pidx];
-    for (int dir = 0; dir < 2; ++dir) {
-        if (dir == 0 ? px == 0 : py == 0) continue;
-        long long oidx = dir == 0 ? pidx - 1 : pidx - W;
-        float4 to = rast[oidx];
-        if (to.w == tr.w) continue;
-        long long pp = (int)tr.w ? pidx : oidx;
-        long long op = (int)to.w ? pidx : oidx;
-        if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
-        float2 f, o;
-        if (dir == 0) { f = make_float2((float)px + (pp > op ? .5f : -.5f), (float)py + .5f); o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
-        else { f = make_float2((float)px + .5f, (float)py + (pp > op ? .5f : -.5f)); o = make_float2(0.f, pp > op ? -1.f : 1.f); }
-        AATri t;
-        if (!aa_fetch(proj, nv, tri, nt, rast, pp, s, f, t, flags)) continue;
+    float acc[8];
+    for (int i = 0; i < C && i < 8; ++i) acc[i] = in[pidx * C + i];
+    // pairs: (p-1,p) at p, (p,p+1) at p+1, (p-W,p) at p, (p,p+W) at p+W
+    for (int k = 0; k < 4; ++k) {
+        const int dir = k >> 1;
+        const bool self = (k & 1) == 0;
+        int qx = px, qy = py;
+        if (!self) { if (dir == 0) ++qx; else ++qy; }
+        if (dir == 0 ? (qx == 0 || qx >= W) : (qy == 0 || qy >= H)) continue;
+        const long long q = self ? pidx : (dir == 0 ? pidx + 1 : pidx + W);
+        AAPair P;
+        if (!aa_pair(proj, nv, tri, nt, rast, q, qx, qy, W, dir, false, s, P, flags)) continue;
+        if (P.pp != pidx && P.op != pidx) continue;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
+        for (int e = 0; e < 3; ++e) {
             float a, alpha, ia, n;
-            float2 e;
-            if (!aa_edge(t.v[k], t.v[(k + 1) % 3], o, a, alpha, ia, e, n)) continue;
-            long long tgt = alpha > 0 ? op : pp;
+            float2 ev;
+            if (!aa_edge(P.t.v[e], P.t.v[(e + 1) % 3], P.o, a, alpha, ia, ev, n)) continue;
+            if ((alpha > 0 ? P.op : P.pp) != pidx) continue;
             if (C4) {
-                float4 ip = reinterpret_cast<const float4*>(in)[pp], io = reinterpret_cast<const float4*>(in)[op];
-                red_add4(out + tgt * 4, alpha * (ip.x - io.x), alpha * (ip.y - io.y), alpha * (ip.z - io.z), alpha * (ip.w - io.w));
+                float4 ip = reinterpret_cast<const float4*>(in)[P.pp], io = reinterpret_cast<const float4*>(in)[P.op];
+                acc[0] += alpha * (ip.x - io.x); acc[1] += alpha * (ip.y - io.y);
+                acc[2] += alpha * (ip.z - io.z); acc[3] += alpha * (ip.w - io.w);
             } else {
-                for (int i = 0; i < C; ++i) atomicAdd(&out[tgt * C + i], alpha * (in[pp * C + i] - in[op * C + i]));
+                for (int i = 0; i < C && i < 8; ++i) acc[i] += alpha * (in[P.pp * C + i] - in[P.op * C + i]);
             }
         }
     }
+    if (C4) reinterpret_cast<float4*>(out)[pidx] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    else for (int i = 0; i < C && i < 8; ++i) out[pidx * C + i] = acc[i];
 }
 
+// Backward antialias: colour gradients gathered per pixel like the forward
+// (antialias.cu:216-220, deterministic); clip-position gradients scattered
+// once per pair, by the pair's own pixel q (antialias.cu:222-245).
 template <int C4>
 __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
                          const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
@@ -411,49 +448,51 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
     const float4* proj = clip + (size_t)view * nv;
     float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
-    float4 tr = rast[pidx];
-    for (int dir = 0; dir < 2; ++dir) {
-        if (dir == 0 ? px == 0 : py == 0) continue;
-        long long oidx = dir == 0 ? pidx - 1 : pidx - W;
-        float4 to = rast[oidx];
-        if (to.w == tr.w) continue;
-        long long pp = (int)tr.w ? pidx : oidx;
-        // antialias.cu:279 uses the current pixel's id here (horizontal pairs)
-        long long op = (int)((dir == 0 && !exact) ? tr.w : to.w) ? pidx : oidx;
-        if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
-        float2 f, o;
-        if (dir == 0) { f = make_float2((float)px + (pp > op ? .5f : -.5f), (float)py + .5f); o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
-        else { f = make_float2((float)px + .5f, (float)py + (pp > op ? .5f : -.5f)); o = make_float2(0.f, pp > op ? -1.f : 1.f); }
-        AATri t;
-        if (!aa_fetch(proj, nv, tri, nt, rast, pp, s, f, t, flags)) continue;
+    float acc[8];
+    for (int i = 0; i < C && i < 8; ++i) acc[i] = gout[pidx * C + i];
+    for (int k = 0; k < 4; ++k) {
+        const int dir = k >> 1;
+        const bool self = (k & 1) == 0;
+        int qx = px, qy = py;
+        if (!self) { if (dir == 0) ++qx; else ++qy; }
+        if (dir == 0 ? (qx == 0 || qx >= W) : (qy == 0 || qy >= H)) continue;
+        const long long q = self ? pidx : (dir == 0 ? pidx + 1 : pidx + W);
+        AAPair P;
+        if (!aa_pair(proj, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags)) continue;
+        const bool mine = P.pp == pidx || P.op == pidx;
+        if (!mine && !(self && gv)) continue;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
+        for (int e = 0; e < 3; ++e) {
+            const int ka = e, kb = (e + 1) % 3;
             float a, alpha, ia, n;
-            float2 e;
-            const int ka = k, kb = (k + 1) % 3;
-            if (!aa_edge(t.v[ka], t.v[kb], o, a, alpha, ia, e, n)) continue;
-            const long long src = alpha > 0 ? op : pp;
+            float2 ev;
+            if (!aa_edge(P.t.v[ka], P.t.v[kb], P.o, a, alpha, ia, ev, n)) continue;
+            const long long src = alpha > 0 ? P.op : P.pp;
+            const float sign = P.pp == pidx ? 1.f : -1.f;
             float d = 0.f;
             if (C4) {
                 float4 g = reinterpret_cast<const float4*>(gout)[src];
-                float4 ip = reinterpret_cast<const float4*>(in)[pp], io = reinterpret_cast<const float4*>(in)[op];
-                red_add4(gin + pp * 4, alpha * g.x, alpha * g.y, alpha * g.z, alpha * g.w);
-                red_add4(gin + op * 4, -alpha * g.x, -alpha * g.y, -alpha * g.z, -alpha * g.w);
-                d = g.x * (ip.x - io.x) + g.y * (ip.y - io.y) + g.z * (ip.z - io.z) + g.w * (ip.w - io.w);
+                if (mine) {
+                    acc[0] += sign * alpha * g.x; acc[1] += sign * alpha * g.y;
+                    acc[2] += sign * alpha * g.z; acc[3] += sign * alpha * g.w;
+                }
+                if (self && gv) {
+                    float4 ip = reinterpret_cast<const float4*>(in)[P.pp], io = reinterpret_cast<const float4*>(in)[P.op];
+                    d = g.x * (ip.x - io.x) + g.y * (ip.y - io.y) + g.z * (ip.z - io.z) + g.w * (ip.w - io.w);
+                }
             } else {
-                for (int i = 0; i < C; ++i) {
+                for (int i = 0; i < C && i < 8; ++i) {
                     float g = gout[src * C + i];
-                    atomicAdd(&gin[pp * C + i], alpha * g);
-                    atomicAdd(&gin[op * C + i], -alpha * g);
-                    d += g * (in[pp * C + i] - in[op * C + i]);
+                    if (mine) acc[i] += sign * alpha * g;
+                    d += g * (in[P.pp * C + i] - in[P.op * C + i]);
                 }
             }
-            if (gv) {
-                float2 pa = t.v[ka], pb = t.v[kb];
+            if (self && gv) {
+                float2 pa = P.t.v[ka], pb = P.t.v[kb];
                 d *= ia;
-                float2 da = make_float2(d * s.x * t.iw[ka], d * s.y * t.iw[ka]);
-                float2 dbv = make_float2(d * s.x * t.iw[kb], d * s.y * t.iw[kb]);
-                float r = (n > 0 ? e.x : -e.y) * ia;
+                float2 da = make_float2(d * s.x * P.t.iw[ka], d * s.y * P.t.iw[ka]);
+                float2 dbv = make_float2(d * s.x * P.t.iw[kb], d * s.y * P.t.iw[kb]);
+                float r = (n > 0 ? ev.x : -ev.y) * ia;
                 if (n > 0) {
                     da.x *= pb.y; da.y *= pb.y; da.y *= r;
                     dbv.x *= -pa.y; dbv.y *= -pa.y; dbv.y *= r;
@@ -461,11 +500,13 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
                     da.x *= -pb.x; da.y *= -pb.x; da.x *= r;
                     dbv.x *= pa.x; dbv.y *= pa.x; dbv.x *= r;
                 }
-                red_add4(gv + (size_t)t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * pa.x + da.y * pa.y));
-                red_add4(gv + (size_t)t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * pb.x + dbv.y * pb.y));
+                red_add4(gv + (size_t)P.t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * pa.x + da.y * pa.y));
+                red_add4(gv + (size_t)P.t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * pb.x + dbv.y * pb.y));
             }
         }
     }
+    if (C4) reinterpret_cast<float4*>(gin)[pidx] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    else for (int i = 0; i < C && i < 8; ++i) gin[pidx * C + i] = acc[i];
 }
 
 // ----------------------------------------------------------------- loss
@@ -699,12 +740,8 @@ VCL_API vcl_status vcl_antialias_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     VCL_REQUIRE(clip && tri && rast && in && out && W > 0 && H > 0 && views > 0 && C > 0, "bad antialias_fwd arguments");
     VCL_REQUIRE(aligned16(clip) && aligned16(rast), "misaligned buffer");
     VCL_REQUIRE(in != out, "antialias_fwd cannot run in place");
-    long long npix = (long long)W * H * views;
-    cudaStream_t s = (cudaStream_t)stream;
-    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(out, in, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s),
-                                   "antialias copy");
-    if (st) return st;
-    return aa_edges_fwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, out, s);
+    VCL_REQUIRE(C <= 8, "antialias supports up to 8 channels");
+    return aa_edges_fwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, out, (cudaStream_t)stream);
 }
 
 VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
@@ -715,12 +752,9 @@ VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, co
                 "bad antialias_bwd arguments");
     VCL_REQUIRE(aligned16(clip) && aligned16(rast) && aligned16(grad_clip), "misaligned buffer");
     VCL_REQUIRE(grad_in != grad_out, "antialias_bwd cannot run in place");
-    long long npix = (long long)W * H * views;
-    cudaStream_t s = (cudaStream_t)stream;
-    vcl_status st = vcl_cuda_check(
-        ctx, cudaMemcpyAsync(grad_in, grad_out, sizeof(float) * npix * C, cudaMemcpyDeviceToDevice, s), "antialias copy");
-    if (st) return st;
-    return aa_edges_bwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, grad_out, grad_in, grad_clip, s);
+    VCL_REQUIRE(C <= 8, "antialias supports up to 8 channels");
+    return aa_edges_bwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, grad_out, grad_in, grad_clip,
+                        (cudaStream_t)stream);
 }
 
 VCL_API vcl_status vcl_mse(vcl_ctx* ctx, const float* pred, const float* target, size_t n, float* grad, float* loss_dev,

@@ -2,8 +2,8 @@
 #pragma once
 #include "common.cuh"
 
-// Antialias edge passes only (the caller has already initialised `out` /
-// `grad_in`, antialias.cu:62-65 / :267-269).
+// Antialias forward / backward (gather form: `out` / `grad_in` are written
+// completely, the reference's initial copy included).
 vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
                         int H, int views, int C, const float* in, float* out, cudaStream_t s);
 vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,

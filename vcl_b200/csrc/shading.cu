@@ -381,7 +381,8 @@ VCL_API vcl_status vcl_sg_bwd(vcl_ctx* ctx, const float* rast, int W, int H, int
     size_t smem = sg_bwd_smem(K, C, nacc, threads);
     VCL_REQUIRE(smem <= 200 * 1024, "too many lobes for the shared-memory reduction (K=%d)", K);
     VCL_REQUIRE(C == 4 || C <= CMAX, "channel count");
-    if (K <= 128) {
+    const bool pix_out = grad_diffuse || grad_spec_axis || grad_spec_sharpness || grad_spec_amplitude;
+    if (K <= 128 && !pix_out) {
         const int Kp = sg_lobe_group(K > 0 ? K : 1);
         const int NL = (K + 31) / 32;
         const int lthreads = 128;
