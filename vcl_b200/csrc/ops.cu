@@ -459,6 +459,9 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
         const long long q = self ? pidx : (dir == 0 ? pidx + 1 : pidx + W);
         AAPair P;
         if (!aa_pair(proj, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags)) continue;
+        // the reference's horizontal typo can give pp == op: its two colour
+        // terms cancel and the clip term is zero (antialias.cu:279, :216-223)
+        if (P.pp == P.op) continue;
         const bool mine = P.pp == pidx || P.op == pidx;
         if (!mine && !(self && gv)) continue;
 #pragma unroll
