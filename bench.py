@@ -206,6 +206,8 @@ def run_vcl(args, rank, world):
             clk = clocks.stop()
         results[name] = ms
         launches[name] = fit.launches_per_step()
+        if strat == capi.FIT_FUSED:
+            out["raster_tuning"] = fit.raster_tuning()
         losses[name] = fit.read_loss(sh)
         fit.close()
     best = strategies[-1][0]
@@ -423,6 +425,9 @@ def main():
             "h2d_bytes_per_step": S.views * S.H * S.W * S.C * 4 + S.views * (16 + 9) * 4,
             "d2h_bytes_per_step": 4},
         "loss_last": r["losses"][r["best"]],
+        "raster_autotune": ({"tile": r["raster_tuning"][0],
+                             "ms_per_tile_8_16_32": [round(x, 4) for x in r["raster_tuning"][1]]}
+                            if "raster_tuning" in r else None),
     }
     if "stages" in r:
         st = r["stages"]

@@ -289,6 +289,11 @@ VCL_API vcl_status vcl_fit_read_loss(vcl_fit* fit, float* loss_host, void* strea
  * synchronizes `stream`. */
 VCL_API vcl_status vcl_fit_read_params(vcl_fit* fit, float* pos, float* tex_level0, float* lobe_axis,
                                        float* lobe_sharp, float* lobe_amp, void* stream);
+/* The raster tile size the fused strategy's autotuner picked for this job
+ * (tuned on first use by timing tiles 8, 16 and 32 on the job's geometry)
+ * and the measured milliseconds per raster call for each (ms_per_tile[3],
+ * may be NULL). */
+VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* fit, int* tile, float* ms_per_tile);
 /* Device bytes held by a job with this descriptor (for admission). */
 VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc);
 /* Number of kernel launches one vcl_fit_step issues with the current

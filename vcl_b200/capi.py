@@ -67,6 +67,7 @@ SIGNATURES = {
     "vcl_fit_read_loss": (c_int, [P, P, P]),
     "vcl_fit_read_params": (c_int, [P, P, P, P, P, P, P]),
     "vcl_fit_footprint": (c_size, [P]),
+    "vcl_fit_raster_tuning": (c_int, [P, P, P]),
     "vcl_fit_launches_per_step": (c_int, [P]),
 }
 
@@ -248,6 +249,12 @@ class Fit:
 
     def loss_address(self):
         return self.ctx.lib.vcl_fit_loss_device(self.h)
+
+    def raster_tuning(self):
+        t = ctypes.c_int()
+        ms = (ctypes.c_float * 3)()
+        self._c(self.ctx.lib.vcl_fit_raster_tuning(self.h, ctypes.byref(t), ms), "vcl_fit_raster_tuning")
+        return t.value, list(ms)
 
     def launches_per_step(self):
         return self.ctx.lib.vcl_fit_launches_per_step(self.h)

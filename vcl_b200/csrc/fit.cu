@@ -177,8 +177,21 @@ VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* f, int strategy) {
     vcl_ctx* ctx = f->ctx;
     VCL_REQUIRE(strategy == VCL_FIT_PLAIN || strategy == VCL_FIT_FUSED, "unknown strategy %d", strategy);
     VCL_REQUIRE(strategy == VCL_FIT_PLAIN || f->d.C == 4, "the fused strategy needs C = 4 channels");
-    if (strategy == VCL_FIT_FUSED && f->strategy != VCL_FIT_FUSED) {
-        vcl_status st = fit_fused_sync_counter(f, true);
+    if (strategy != f->strategy) {
+        // the plain step clears gradients when it starts, the fused step when
+        // it has consumed them: start the other strategy from zero gradients
+        const vcl_fit_desc& d = f->d;
+        size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, d.C, d.levels);
+        vcl_status st = VCL_OK;
+        auto z = [&](void* p, size_t b) {
+            if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaMemset(p, 0, b), "gradient clear");
+        };
+        z(f->g_pyr, sizeof(float) * npyr);
+        z(f->g_pos, sizeof(float) * d.nv * 3);
+        z(f->g_lobe, sizeof(float) * (size_t)d.K * (4 + d.C));
+        z(f->g_clip, sizeof(float) * (size_t)d.views * d.nv * 4);
+        if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaDeviceSynchronize(), "gradient clear");
+        if (st == VCL_OK && strategy == VCL_FIT_FUSED) st = fit_fused_sync_counter(f, true);
         if (st) return st;
     }
     f->strategy = strategy;
@@ -248,6 +261,11 @@ VCL_API int vcl_fit_launches_per_step(const vcl_fit* f) {
 VCL_API vcl_status vcl_fit_render(vcl_fit* f, float* out, void* stream) {
     if (!f) return VCL_ERR_ARG;
     return fit_forward(f, out, (cudaStream_t)stream);
+}
+
+VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* f, int* tile, float* ms_per_tile) {
+    if (!f) return VCL_ERR_ARG;
+    return fit_fused_raster_tuning(f, tile, ms_per_tile);
 }
 
 VCL_API vcl_status vcl_fit_step(vcl_fit* f, void* stream) {

@@ -30,3 +30,4 @@ int fit_plain_launches(const vcl_fit* f);
 int fit_fused_launches(const vcl_fit* f);
 void fit_fused_release(vcl_fit* f);
 vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device);
+vcl_status fit_fused_raster_tuning(vcl_fit* f, int* tile, float* ms3);

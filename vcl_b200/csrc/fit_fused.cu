@@ -42,6 +42,7 @@ struct Fused {
     cudaStream_t graph_stream = nullptr;
     int graph_mode = -1;
     cudaStream_t side = nullptr;               // lobe-gradient branch
+    float tune_ms[3] = {0.f, 0.f, 0.f};        // raster time per tile size 8/16/32
     cudaEvent_t fork = nullptr, join = nullptr;
 };
 
@@ -465,14 +466,25 @@ size_t lobes_smem(int K, int nacc, int threads) {
     return sizeof(float) * (size_t)K * nacc + (size_t)(threads / 32) * 32 * sizeof(SPix);
 }
 
+vcl_status autotune_raster(vcl_fit* f);
+
 vcl_status fused_init(vcl_fit* f) {
     if (f->fused) return VCL_OK;
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
     Fused* F = new Fused();
     F->tile = ctx->tile;
-    F->cap = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(d.views, d.nt, d.W, d.H, F->tile);
-    size_t ws = raster_ws_size(d.W, d.H, d.views, d.nt, F->tile, F->cap);
+    long long cap = 0;
+    size_t ws = 0;
+    for (int t : {8, 16, 32}) {
+        long long c = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
+        if (c > cap) cap = c;
+    }
+    for (int t : {8, 16, 32}) {
+        size_t b = raster_ws_size(d.W, d.H, d.views, d.nt, t, cap);
+        if (b > ws) ws = b;
+    }
+    F->cap = cap;
     cudaError_t e = cudaMalloc(&F->raster_ws, ws);
     if (e == cudaSuccess) e = cudaMalloc(&F->d_step, 64);
     if (e == cudaSuccess) e = cudaMalloc(&F->d_corr, 64);
@@ -490,7 +502,46 @@ vcl_status fused_init(vcl_fit* f) {
     if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "fused streams");
     size_t sf = shade_smem(d.K);
     if (sf > 48 * 1024) cudaFuncSetAttribute(k_shade_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-    return vcl_cuda_check(ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice), "fused init");
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice),
+                                   "fused init");
+    if (st) return st;
+    return autotune_raster(f);
+}
+
+// Raster autotuner: times the tile binning schedules (tile edge 8, 16, 32
+// with the automatic bin capacity) on this job's own geometry and keeps the
+// fastest for the job's captured step.  Runs once, outside any capture.
+vcl_status autotune_raster(vcl_fit* f) {
+    vcl_ctx* ctx = f->ctx;
+    Fused* F = (Fused*)f->fused;
+    const vcl_fit_desc& d = f->d;
+    cudaStream_t s = F->side;
+    vcl_status st = vcl_project_fwd(ctx, f->mvp, d.views, f->pos, d.nv, 4, f->clip, s);
+    if (st) return st;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return vcl_fail(ctx, VCL_ERR_CUDA, "autotune events");
+    float best = 1e30f;
+    int best_tile = F->tile;
+    for (int t : {8, 16, 32}) {
+        for (int rep = 0; rep < 4 && st == VCL_OK; ++rep) {
+            if (rep == 1) cudaEventRecord(e0, s);
+            st = raster_fwd_ws(ctx, F->raster_ws, t, F->cap, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views, f->rast,
+                               f->db, s);
+        }
+        cudaEventRecord(e1, s);
+        if (st) break;
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        F->tune_ms[t == 8 ? 0 : t == 16 ? 1 : 2] = ms / 3.f;
+        if (ms < best) { best = ms; best_tile = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    F->tile = best_tile;
+    return vcl_cuda_check(ctx, cudaStreamSynchronize(s), "autotune");
 }
 
 vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
@@ -658,5 +709,14 @@ vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device) {
     if (to_device)
         return vcl_cuda_check(f->ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice),
                               "step counter");
+    return VCL_OK;
+}
+
+vcl_status fit_fused_raster_tuning(vcl_fit* f, int* tile, float* ms3) {
+    vcl_status st = fused_init(f);
+    if (st) return st;
+    Fused* F = (Fused*)f->fused;
+    if (tile) *tile = F->tile;
+    if (ms3) for (int i = 0; i < 3; ++i) ms3[i] = F->tune_ms[i];
     return VCL_OK;
 }

@@ -10,7 +10,10 @@
 //     term = (e^(l - lambda1 - lambda2) - e^(-l - lambda1 - lambda2)) / max(l, 1e-6) * amp.
 // Here 1/l comes from one reciprocal square root of |.|^2 (and l = |.|^2 / l),
 // so a lobe costs two rsqrt and four exp instead of two sqrt, two
-// divisions and four exp.
+// divisions and four exp.  The exponentials use the hardware ex2 path
+// (__expf): its relative error grows with |argument|, and the terms with a
+// large |argument| are the ones e^(...) makes negligible, so the lobe sums
+// keep FP32 accuracy.
 #pragma once
 #include "common.cuh"
 
@@ -30,10 +33,10 @@ DEV void sg_terms(float3 dn, float3 sn, float3 g, float gs, float ss, float sa, 
     float3 d = dn + g;
     float l, il;
     sg_len(dot3(d, d), l, il);
-    dg = (expf(l - SG_DIFF_SHARP - gs) - expf(-l - SG_DIFF_SHARP - gs)) * il * SG_DIFF_AMP;
+    dg = (__expf(l - SG_DIFF_SHARP - gs) - __expf(-l - SG_DIFF_SHARP - gs)) * il * SG_DIFF_AMP;
     float3 s = sn + g;
     sg_len(dot3(s, s), l, il);
-    sg = (expf(l - ss - gs) - expf(-l - ss - gs)) * il * sa;
+    sg = (__expf(l - ss - gs) - __expf(-l - ss - gs)) * il * sa;
 }
 
 // Backward terms of one lobe (material.cu:398-418).
@@ -48,7 +51,7 @@ DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, flo
     float dl, il;
     sg_len(dot3(dsum, dsum), dl, il);
     float dotn = (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
-    float em = expf(dl - SG_DIFF_SHARP - gs), ep = expf(-dl - SG_DIFF_SHARP - gs);
+    float em = __expf(dl - SG_DIFF_SHARP - gs), ep = __expf(-dl - SG_DIFF_SHARP - gs);
     r.dg = (em - ep) * il * SG_DIFF_AMP;
     r.ddg = dsum * (((1.f - il) * em + (1.f + il) * ep) * il * il);
     r.ddgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
@@ -58,12 +61,42 @@ DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, flo
     float sdot = dot3(sgn, pax);
     dotn = (gs + ss * sdot) * il;
     float dotp = (gs * sdot + ss) * il;
-    em = expf(sl - ss - gs); ep = expf(-sl - ss - gs);
+    em = __expf(sl - ss - gs); ep = __expf(-sl - ss - gs);
     r.sil_e = (em - ep) * il;
     r.sgv = r.sil_e * sa;
     r.dsg = ssum * (((1.f - il) * em + (1.f + il) * ep) * il * il);
     r.dsgs = ((dotn * (1.f - il) - 1.f) * em + (dotn * (1.f + il) + 1.f) * ep) * il;
     r.dsgss = ((dotp * (1.f - il) - 1.f) * em + (dotp * (1.f + il) + 1.f) * ep) * il;
+    return r;
+}
+
+
+// The terms the lobe gradients need (no specular-lobe derivatives).
+struct SGL {
+    float dg, sgv, ddgs, dsgs;
+    float3 ddg, dsg;
+};
+
+DEV SGL sg_lobe_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa) {
+    SGL r;
+    float3 dsum = dn + sgn;
+    float dl, il;
+    sg_len(dot3(dsum, dsum), dl, il);
+    float dotn = (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
+    float em = __expf(dl - SG_DIFF_SHARP - gs), ep = __expf(-dl - SG_DIFF_SHARP - gs);
+    r.dg = (em - ep) * il * SG_DIFF_AMP;
+    float ilm = 1.f - il, ilp = 1.f + il;
+    r.ddg = dsum * ((ilm * em + ilp * ep) * il * il);
+    r.ddgs = ((dotn * ilm - 1.f) * em + (dotn * ilp + 1.f) * ep) * il;
+    float3 ssum = sn + sgn;
+    float sl;
+    sg_len(dot3(ssum, ssum), sl, il);
+    dotn = (gs + ss * dot3(sgn, pax)) * il;
+    em = __expf(sl - ss - gs); ep = __expf(-sl - ss - gs);
+    r.sgv = (em - ep) * il * sa;
+    ilm = 1.f - il; ilp = 1.f + il;
+    r.dsg = ssum * ((ilm * em + ilp * ep) * il * il);
+    r.dsgs = ((dotn * ilm - 1.f) * em + (dotn * ilp + 1.f) * ep) * il;
     return r;
 }
 
@@ -354,6 +387,45 @@ DEV void sg_bwd_lanes(LaneLobes<NL, CC>& LL, int C, int exact, const SPix* st, S
                       int G, int li) {
     const int Cn = CC ? CC : C;
     const int rounds = (m + G - 1) / G;
+    if (!PIX) {
+        // lobe gradients only: per pixel gd_k = g_k * diffuse_k once, then per
+        // lobe two FMAs per channel; contributions are dropped when the lobe's
+        // terms are not finite (the reference's guarded add, common.h:181)
+        for (int rr = 0; rr < rounds; ++rr) {
+            const int j = rr * G + g;
+            if (j >= m) continue;
+            const SPix& P = st[j];
+            const float3 n = f3(P.n[0], P.n[1], P.n[2]), pax = f3(P.pax[0], P.pax[1], P.pax[2]);
+            const float ss = P.ss, sa = P.sa;
+            const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+            float gk[CC ? CC : SG_CMAX], gdk[CC ? CC : SG_CMAX];
+#pragma unroll
+            for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
+                gk[k] = k < Cn ? P.go[k] : 0.f;
+                gdk[k] = k < Cn ? P.go[k] * P.dfs[k] : 0.f;
+            }
+#pragma unroll
+            for (int s = 0; s < NL; ++s) {
+                if (!LL.valid[s]) continue;
+                SGL t = sg_lobe_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa);
+                float sum = 0.f, sumd = 0.f;
+#pragma unroll
+                for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
+                    sum = fmaf(gk[k], LL.a[s][k], sum);
+                    sumd = fmaf(gdk[k], LL.a[s][k], sumd);
+                }
+                if (isfinite(t.dg) && isfinite(t.sgv)) {
+#pragma unroll
+                    for (int k = 0; k < (CC ? CC : SG_CMAX); ++k)
+                        LL.acc_am[s][k] = fmaf(t.sgv, gk[k], fmaf(t.dg, gdk[k], LL.acc_am[s][k]));
+                }
+                float3 cax = ((t.ddg * sumd) * SG_DIFF_AMP + (t.dsg * sum) * sa) * LL.gs[s];
+                if (fin3(cax)) { LL.acc_ax[s][0] += cax.x; LL.acc_ax[s][1] += cax.y; LL.acc_ax[s][2] += cax.z; }
+                LL.acc_sh[s] += finite_or0(sumd * t.ddgs * SG_DIFF_AMP + sum * t.dsgs * sa);
+            }
+        }
+        return;
+    }
     for (int rr = 0; rr < rounds; ++rr) {
         const int j = rr * G + g;
         const bool ok = j < m;
