@@ -135,18 +135,27 @@ def test_render_is_deterministic_and_switching_strategy_keeps_step_count(ctx):
     tgt = _target(S)
     fit.set_target(tgt)
     stream = torch.cuda.Stream()
-    fit.step(stream.cuda_stream)
-    fit.set_strategy(capi.FIT_FUSED)
-    fit.step(stream.cuda_stream)
-    fit.set_strategy(capi.FIT_PLAIN)
-    fit.step(stream.cuda_stream)
+    lm = []
+    for strategy in (capi.FIT_PLAIN, capi.FIT_FUSED, capi.FIT_PLAIN):
+        fit.set_strategy(strategy)
+        fit.step(stream.cuda_stream)
+        lm.append(fit.read_loss(stream.cuda_stream))
     p_mixed = fit.read_params(stream.cuda_stream)
     fit.close()
     ref = capi.Fit(ctx, S)
     ref.set_target(tgt)
+    lp = []
     for _ in range(3):
         ref.step(stream.cuda_stream)
+        lp.append(ref.read_loss(stream.cuda_stream))
     p_plain = ref.read_params(stream.cuda_stream)
     ref.close()
-    assert np.abs(p_mixed[1] - p_plain[1]).max() <= 2 * S.lr * 3
-    assert np.quantile(np.abs(p_mixed[1] - p_plain[1]), 0.99) <= 1e-4
+    # a stale gradient or a wrong step index would show up here at the size
+    # of a whole Adam step; what remains is summation-order noise
+    assert np.allclose(lm, lp, rtol=1e-4), (lm, lp)
+    for a, b in zip(p_mixed, p_plain):
+        if isinstance(a, tuple):
+            for x, y in zip(a, b):
+                assert np.abs(x - y).max() <= 2 * S.lr * 3
+        else:
+            assert np.abs(a - b).max() <= 2 * S.lr * 3
