@@ -140,8 +140,8 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
 // environment sum (kept for the backward's diffuse gradient).  C = 4.
 __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
                                                    float4* __restrict__ diffenv) {
-    extern __shared__ float sm[];
-    const SGLobes L = sg_stage_lobes(sm, a.K, 4, a.axis, a.sharp, a.amp);
+    extern __shared__ float4 sm4[];
+    sg_stage_lobes4(sm4, a.K, a.axis, a.sharp, a.amp);
     __syncthreads();
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.npix) return;
@@ -150,12 +150,10 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
         color[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    float de[SG_CMAX], se[SG_CMAX];
-    sg_env<4>(L, a.K, 4, q.n, q.pax, q.ss, q.sa, de, se);
-    diffenv[p] = make_float4(de[0], de[1], de[2], de[3]);
-    float4 c = make_float4(q.dfs.x * de[0] + se[0], q.dfs.y * de[1] + se[1], q.dfs.z * de[2] + se[2],
-                           q.dfs.w * de[3] + se[3]);
-    color[p] = c;
+    float4 de, se;
+    sg_env4(sm4, a.K, q.n, q.pax, q.ss, q.sa, de, se);
+    diffenv[p] = de;
+    color[p] = make_float4(q.dfs.x * de.x + se.x, q.dfs.y * de.y + se.y, q.dfs.z * de.z + se.z, q.dfs.w * de.w + se.w);
 }
 
 // loss.cu:22-30: gradient and loss in one pass.
@@ -298,23 +296,26 @@ __global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const fl
     red_add4(gcv + (size_t)i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
 }
 
-// Lobe gradients (material.cu:428-433): lobe-parallel over staged pixels whose
-// shading inputs are recomputed from the raster output.  C = 4.
+// Lobe gradients (material.cu:428-433), lobe-parallel: a warp stages up to
+// 32 covered pixels (their shading inputs recomputed from the raster output,
+// reduced to the per-pixel factors every lobe reuses), then each lane walks
+// them for its lobe(s); sums stay in registers until the end.  C = 4.
 template <int NL>
 __global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
-                                                  int nacc, float* __restrict__ g_axis, float* __restrict__ g_sharp,
+                                                  float* __restrict__ g_axis, float* __restrict__ g_sharp,
                                                   float* __restrict__ g_amp) {
     extern __shared__ float sm[];
     const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int K = a.K;
-    float* s_acc = sm;
-    SPix* s_pix = reinterpret_cast<SPix*>(sm + (size_t)K * nacc);
-    for (int i = threadIdx.x; i < K * nacc; i += blockDim.x) s_acc[i] = 0.f;
+    float* s_acc = sm;                                               // [K][8]
+    SPix4* s_pix = reinterpret_cast<SPix4*>(sm + ((size_t)K * 8 + 3) / 4 * 4);
+    for (int i = threadIdx.x; i < K * 8; i += blockDim.x) s_acc[i] = 0.f;
     __syncthreads();
     const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
-    LaneLobes<NL, 4> LL;
-    lane_lobes_load<NL, 4>(LL, li, Kp, K, 4, a.axis, a.sharp, a.amp);
-    SPix* st = s_pix + wid * 32;
+    Lobe4 LL[NL];
+#pragma unroll
+    for (int sl = 0; sl < NL; ++sl) lobe4_load(LL[sl], li + sl * Kp, K, a.axis, a.sharp, a.amp);
+    SPix4* st = s_pix + wid * 32;
     const long long nchunks = (a.npix + 31) / 32;
     for (long long chunk = (long long)blockIdx.x * nwarps + wid; chunk < nchunks; chunk += (long long)gridDim.x * nwarps) {
         const long long p = chunk * 32 + lane;
@@ -322,22 +323,27 @@ __global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const f
         const bool live = p < a.npix && shade_inputs<1>(a, td, p, q);
         const unsigned ball = __ballot_sync(0xffffffffu, live);
         const int m = __popc(ball);
-        if (live) {
-            SPix& z = st[__popc(ball & ((1u << lane) - 1u))];
-            z.n[0] = q.n.x; z.n[1] = q.n.y; z.n[2] = q.n.z;
-            z.pax[0] = q.pax.x; z.pax[1] = q.pax.y; z.pax[2] = q.pax.z;
-            z.ss = q.ss; z.sa = q.sa;
-            z.dfs[0] = q.dfs.x; z.dfs[1] = q.dfs.y; z.dfs[2] = q.dfs.z; z.dfs[3] = q.dfs.w;
-            const float4 gc = g_color[p];
-            z.go[0] = gc.x; z.go[1] = gc.y; z.go[2] = gc.z; z.go[3] = gc.w;
+        if (live) st[__popc(ball & ((1u << lane) - 1u))] = spix4(q.n, q.pax, q.ss, q.sa, q.dfs, g_color[p]);
+        __syncwarp();
+        for (int j = g; j < m; j += G) {
+            const SPix4 P = st[j];
+#pragma unroll
+            for (int sl = 0; sl < NL; ++sl)
+                if (LL[sl].valid) lobe4_accumulate(LL[sl], P);
         }
         __syncwarp();
-        if (m > 0) sg_bwd_lanes<NL, 4, false>(LL, 4, 0, st, nullptr, m, Kp, g, G, li);
-        __syncwarp();
     }
-    lane_lobes_flush<NL, 4>(LL, 4, Kp, li, s_acc, nacc, false);
+#pragma unroll
+    for (int sl = 0; sl < NL; ++sl) lobe4_flush(LL[sl], li + sl * Kp, Kp, s_acc);
     __syncthreads();
-    sg_flush_block(s_acc, K, 4, nacc, g_axis, g_sharp, g_amp, nullptr);
+    for (int j = threadIdx.x; j < K * 8; j += blockDim.x) {
+        const float v = s_acc[j];
+        if (v == 0.f) continue;
+        const int i = j >> 3, q = j & 7;
+        if (q < 3) atomicAdd(&g_axis[3 * i + q], v);
+        else if (q == 3) atomicAdd(&g_sharp[i], v);
+        else atomicAdd(&g_amp[4 * i + (q - 4)], v);
+    }
 }
 
 DEV float4 nan_add4(float4 a, float4 b) {
@@ -461,9 +467,9 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
 
 #define TRY(x) do { vcl_status _s = (x); if (_s) return _s; } while (0)
 
-size_t shade_smem(int K) { return sizeof(float) * (size_t)K * 8; }
-size_t lobes_smem(int K, int nacc, int threads) {
-    return sizeof(float) * (size_t)K * nacc + (size_t)(threads / 32) * 32 * sizeof(SPix);
+size_t shade_smem(int K) { return sizeof(float4) * (size_t)K * 2; }
+size_t lobes_smem(int K, int threads) {
+    return sizeof(float) * (((size_t)K * 8 + 3) / 4 * 4) + (size_t)(threads / 32) * 32 * sizeof(SPix4);
 }
 
 vcl_status autotune_raster(vcl_fit* f);
@@ -585,15 +591,15 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
         long long want = (chunks + 3) / 4;
         long long capg = (long long)ctx->sm_count * 6;
         int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
-        size_t lsm = lobes_smem(d.K, nacc, lthreads);
+        size_t lsm = lobes_smem(d.K, lthreads);
         if (NL <= 1)
-            k_sg_lobes<1><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+            k_sg_lobes<1><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
                                                                f->g_sharp, f->g_amp);
         else if (NL <= 2)
-            k_sg_lobes<2><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+            k_sg_lobes<2><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
                                                                f->g_sharp, f->g_amp);
         else
-            k_sg_lobes<4><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, nacc, f->g_axis,
+            k_sg_lobes<4><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
                                                                f->g_sharp, f->g_amp);
         TRY(vcl_launch_check(ctx, "fused lobe gradients"));
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));

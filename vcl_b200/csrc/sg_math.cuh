@@ -529,3 +529,171 @@ inline int sg_lobe_group(int K) {
     while (kp < K && kp < 32) kp <<= 1;
     return kp;
 }
+
+// ---------------------------------------------------------------------------
+// C = 4 fast paths (the fit configurations' RGBA lighting).
+//
+// exp(x) as 2^(x log2 e) on the hardware ex2 unit, with log2 e folded into
+// per-lobe / per-pixel constants so that each exponential costs one add and
+// one ex2.
+constexpr float SG_L2E = 1.4426950408889634f;
+DEV float ex2_fast(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Lobes packed for the pixel-parallel forward: (s*axis, s), (a0..a3).
+DEV void sg_stage_lobes4(float4* sm, int K, const float* axis, const float* sharp, const float* amp) {
+    for (int i = threadIdx.x; i < K; i += blockDim.x) {
+        float s = sharp[i];
+        sm[2 * i] = make_float4(axis[3 * i] * s, axis[3 * i + 1] * s, axis[3 * i + 2] * s, s);
+        sm[2 * i + 1] = make_float4(amp[4 * i], amp[4 * i + 1], amp[4 * i + 2], amp[4 * i + 3]);
+    }
+}
+
+// Forward environment sums of one pixel for C = 4 (material.cu:305-317);
+// same NaN-guard contract as sg_env (plain sums, guarded loop on overflow).
+DEV void sg_env4(const float4* L4, int K, float3 n, float3 pax, float ss, float sa, float4& de, float4& se) {
+    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+    const float cdl = SG_DIFF_SHARP * SG_L2E, ssl = ss * SG_L2E;
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f), e = d;
+    for (int i = 0; i < K; ++i) {
+        const float4 A = L4[2 * i], B = L4[2 * i + 1];
+        const float3 g = f3(A.x, A.y, A.z);
+        const float gsl = A.w * SG_L2E;
+        float3 v = dn + g;
+        float l, il;
+        sg_len(dot3(v, v), l, il);
+        float x = l * SG_L2E, c = cdl + gsl;
+        const float dg = (ex2_fast(x - c) - ex2_fast(-x - c)) * il * SG_DIFF_AMP;
+        v = sn + g;
+        sg_len(dot3(v, v), l, il);
+        x = l * SG_L2E; c = ssl + gsl;
+        const float sg = (ex2_fast(x - c) - ex2_fast(-x - c)) * il * sa;
+        d.x = fmaf(dg, B.x, d.x); d.y = fmaf(dg, B.y, d.y); d.z = fmaf(dg, B.z, d.z); d.w = fmaf(dg, B.w, d.w);
+        e.x = fmaf(sg, B.x, e.x); e.y = fmaf(sg, B.y, e.y); e.z = fmaf(sg, B.z, e.z); e.w = fmaf(sg, B.w, e.w);
+    }
+    if (isfinite(d.x) && isfinite(d.y) && isfinite(d.z) && isfinite(d.w) && isfinite(e.x) && isfinite(e.y) &&
+        isfinite(e.z) && isfinite(e.w)) {
+        de = d; se = e;
+        return;
+    }
+    float dd[4] = {0.f, 0.f, 0.f, 0.f}, ee[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int i = 0; i < K; ++i) {
+        const float4 A = L4[2 * i], B = L4[2 * i + 1];
+        float dg, sg;
+        sg_terms(dn, sn, f3(A.x, A.y, A.z), A.w, ss, sa, dg, sg);
+        const float b[4] = {B.x, B.y, B.z, B.w};
+        for (int k = 0; k < 4; ++k) { add_nan_check(dd[k], dg * b[k]); add_nan_check(ee[k], sg * b[k]); }
+    }
+    de = make_float4(dd[0], dd[1], dd[2], dd[3]);
+    se = make_float4(ee[0], ee[1], ee[2], ee[3]);
+}
+
+// Pixel state of the lean lobe-gradient pass: the per-pixel factors every
+// lobe reuses, computed once by the staging lane.
+struct SPix4 {
+    float4 a;    // 2.133 n, ss
+    float4 b;    // ss p, sa
+    float4 g;    // dL/dout
+    float4 gd;   // dL/dout * diffuse
+    float4 c;    // ss log2 e, -, -, -
+};
+
+DEV SPix4 spix4(float3 n, float3 pax, float ss, float sa, float4 dfs, float4 go) {
+    SPix4 z;
+    z.a = make_float4(n.x * SG_DIFF_SHARP, n.y * SG_DIFF_SHARP, n.z * SG_DIFF_SHARP, ss);
+    z.b = make_float4(pax.x * ss, pax.y * ss, pax.z * ss, sa);
+    z.g = go;
+    z.gd = make_float4(go.x * dfs.x, go.y * dfs.y, go.z * dfs.z, go.w * dfs.w);
+    z.c = make_float4(ss * SG_L2E, 0.f, 0.f, 0.f);
+    return z;
+}
+
+// One lane's lobe (C = 4) with its gradient sums.
+struct Lobe4 {
+    bool valid;
+    float3 sgn;
+    float gs, gsl, cdl, agA;   // sharpness, s*log2e, (2.133 + s)*log2e, 2.34*s
+    float4 a;
+    float3 ax;
+    float sh;
+    float4 am;
+};
+
+DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* sharp, const float* amp) {
+    L.valid = i < K;
+    const int ii = L.valid ? i : 0;
+    const float s = K ? sharp[ii] : 0.f;
+    L.gs = s;
+    L.gsl = s * SG_L2E;
+    L.cdl = (SG_DIFF_SHARP + s) * SG_L2E;
+    L.agA = SG_DIFF_AMP * s;
+    L.sgn = K ? f3(axis[3 * ii] * s, axis[3 * ii + 1] * s, axis[3 * ii + 2] * s) : f3(0.f, 0.f, 0.f);
+    L.a = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    L.ax = f3(0.f, 0.f, 0.f);
+    L.sh = 0.f;
+    L.am = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Gradient contributions of one pixel to one lobe (material.cu:398-433),
+// rearranged: d(axis) = dsum * (A s sumd sd) + ssum * (s sum sa sds) with the
+// scalar factors sd, sds in place of the vectors ddg, dsg.
+DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
+    const float3 dn = f3(P.a.x, P.a.y, P.a.z), sn = f3(P.b.x, P.b.y, P.b.z);
+    const float sa = P.b.w;
+    // diffuse lobe
+    const float3 dsum = dn + L.sgn;
+    float dl, il;
+    sg_len(dot3(dsum, dsum), dl, il);
+    const float dotn = (L.gs + dot3(L.sgn, dn)) * il;
+    float x = dl * SG_L2E;
+    float em = ex2_fast(x - L.cdl), ep = ex2_fast(-x - L.cdl);
+    float ilm = 1.f - il, ilp = 1.f + il;
+    const float dg = (em - ep) * il * SG_DIFF_AMP;
+    const float sd = (ilm * em + ilp * ep) * il * il;
+    const float ddgs = ((dotn * ilm - 1.f) * em + (dotn * ilp + 1.f) * ep) * il;
+    // specular lobe
+    const float3 ssum = sn + L.sgn;
+    float sl;
+    sg_len(dot3(ssum, ssum), sl, il);
+    const float dots = (L.gs + dot3(L.sgn, sn)) * il;
+    x = sl * SG_L2E;
+    const float c = P.c.x + L.gsl;
+    em = ex2_fast(x - c); ep = ex2_fast(-x - c);
+    ilm = 1.f - il; ilp = 1.f + il;
+    const float sgv = (em - ep) * il * sa;
+    const float sds = (ilm * em + ilp * ep) * il * il;
+    const float dsgs = ((dots * ilm - 1.f) * em + (dots * ilp + 1.f) * ep) * il;
+    // channel sums
+    const float sum = P.g.x * L.a.x + P.g.y * L.a.y + P.g.z * L.a.z + P.g.w * L.a.w;
+    const float sumd = P.gd.x * L.a.x + P.gd.y * L.a.y + P.gd.z * L.a.z + P.gd.w * L.a.w;
+    if (isfinite(dg) && isfinite(sgv)) {
+        L.am.x = fmaf(sgv, P.g.x, fmaf(dg, P.gd.x, L.am.x));
+        L.am.y = fmaf(sgv, P.g.y, fmaf(dg, P.gd.y, L.am.y));
+        L.am.z = fmaf(sgv, P.g.z, fmaf(dg, P.gd.z, L.am.z));
+        L.am.w = fmaf(sgv, P.g.w, fmaf(dg, P.gd.w, L.am.w));
+    }
+    const float c1 = sumd * sd * L.agA, c2 = sum * sds * sa * L.gs;
+    if (isfinite(c1) && isfinite(c2)) {
+        L.ax.x = fmaf(c2, ssum.x, fmaf(c1, dsum.x, L.ax.x));
+        L.ax.y = fmaf(c2, ssum.y, fmaf(c1, dsum.y, L.ax.y));
+        L.ax.z = fmaf(c2, ssum.z, fmaf(c1, dsum.z, L.ax.z));
+    }
+    L.sh += finite_or0(sumd * ddgs * SG_DIFF_AMP + sum * dsgs * sa);
+}
+
+// Folds the lobe groups of the warp together and adds the lane's sums into
+// the block accumulator s_acc [K][8] (axis xyz, sharpness, amplitude[4]).
+DEV void lobe4_flush(Lobe4& L, int i, int Kp, float* s_acc) {
+    float v[8] = {L.ax.x, L.ax.y, L.ax.z, L.sh, L.am.x, L.am.y, L.am.z, L.am.w};
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        for (int o = 16; o >= Kp; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    const int lane = threadIdx.x & 31;
+    if (lane < Kp && L.valid) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) atomicAdd(&s_acc[(size_t)i * 8 + q], v[q]);
+    }
+}

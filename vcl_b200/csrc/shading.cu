@@ -92,7 +92,9 @@ __global__ void k_sg_fwd(int C, int K, const float* __restrict__ axis, const flo
                          const float* __restrict__ ssh, const float* __restrict__ sam, float* __restrict__ out,
                          float* __restrict__ odiff, float* __restrict__ ospec) {
     extern __shared__ float sm[];
-    const SGLobes L = sg_stage_lobes(sm, K, C, axis, sharp, amp);
+    SGLobes L;
+    if (CC == 4) sg_stage_lobes4(reinterpret_cast<float4*>(sm), K, axis, sharp, amp);
+    else L = sg_stage_lobes(sm, K, C, axis, sharp, amp);
     __syncthreads();
     const int Cn = CC ? CC : C;
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -106,7 +108,14 @@ __global__ void k_sg_fwd(int C, int K, const float* __restrict__ axis, const flo
         return;
     }
     float de[SG_CMAX], se[SG_CMAX];
-    sg_env<CC>(L, K, C, ld3(normal, p), ld3(sax, p), ssh[p], sam[p], de, se);
+    if (CC == 4) {
+        float4 d4, s4;
+        sg_env4(reinterpret_cast<const float4*>(sm), K, ld3(normal, p), ld3(sax, p), ssh[p], sam[p], d4, s4);
+        de[0] = d4.x; de[1] = d4.y; de[2] = d4.z; de[3] = d4.w;
+        se[0] = s4.x; se[1] = s4.y; se[2] = s4.z; se[3] = s4.w;
+    } else {
+        sg_env<CC>(L, K, C, ld3(normal, p), ld3(sax, p), ssh[p], sam[p], de, se);
+    }
 #pragma unroll
     for (int k = 0; k < SG_CMAX; ++k) {
         if (k >= Cn) break;
@@ -287,7 +296,7 @@ size_t sg_bwd_lp_smem(int K, int C, int nacc, int threads) {
            (size_t)(threads / 32) * 32 * (sizeof(SPix) + sizeof(SPixOut));
 }
 
-size_t sg_fwd_smem(int K, int C) { return sizeof(float) * (size_t)K * (4 + C); }
+size_t sg_fwd_smem(int K, int C) { return sizeof(float) * (size_t)K * (C == 4 ? 8 : 4 + C); }
 size_t sg_bwd_smem(int K, int C, int nacc, int threads) {
     return sizeof(float) * ((size_t)K * (4 + C) + (size_t)(threads / 32) * K * nacc);
 }
