@@ -89,9 +89,12 @@ def test_chained_pipeline_matches_oracle(ctx, mode):
 
 
 @pytest.mark.parametrize("tile,cap", [(8, 0), (16, 0), (32, 0), (16, 64), (8, 1)])
-def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap):
+@pytest.mark.parametrize("subdiv", [1, 4])
+def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap, subdiv):
+    # subdiv 1: large triangles (tile binner, bins overflow when capped);
+    # subdiv 4: mostly small triangles (direct path) mixed with a few large
     import gpu_chain as G
-    S = scenes.make_scene("raster", mesh=("ico", 4), W=200, H=150, views=2, tex=16, K=1, dist=(2.0, 3.5),
+    S = scenes.make_scene("raster", mesh=("ico", subdiv), W=200, H=150, views=2, tex=16, K=1, dist=(2.0, 3.5),
                           disp=0.05, seed=9)
     clip = chain.project(O.orc(), S, S.pos)
     N = S.W * S.H * S.views
@@ -104,9 +107,9 @@ def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap):
         ov = ctx.raster_overflow_count()
         assert np.array_equal(G.host(gr), rast)
         assert np.array_equal(G.host(gd), db)
-        if cap:
+        if cap and subdiv == 1:
             assert ov > 0
-        else:
+        elif not cap:
             assert ov == 0
     finally:
         ctx.set_raster_config(16, 0)

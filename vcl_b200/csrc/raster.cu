@@ -2,21 +2,27 @@
 // 91-202, fixed-function state :252-268) and its backward pass
 // (rasterize.cu:84-141).
 //
-// Forward = triangle setup -> tile binner -> fine rasterizer:
+// Forward = triangle setup -> (small triangles: direct) / (large: tile
+// binner + fine rasterizer) -> resolve:
 //   1. setup   one thread per (view, triangle): homogeneous-2D edge
 //              functions, orientation, trivial reject, conservative pixel
-//              box; counts the tiles the box overlaps (atomic per tile);
+//              box.  A triangle whose box has at most SMALL_AREA pixels is
+//              rasterized right there by its thread: every covered pixel
+//              gets a 64-bit atomicMin of the key (depth, triangle id).
+//              Larger triangles count the tiles their box overlaps;
 //   2. scan    exclusive prefix sum of the per-tile counts -> bin offsets;
-//   3. emit    one thread per (view, triangle) writes its id into each
-//              overlapped tile's bin (order inside a bin is irrelevant);
+//   3. emit    large triangles write their id into each overlapped tile's
+//              bin (order inside a bin is irrelevant);
 //   4. fine    one CTA per tile, one thread per pixel: stages the bin's
 //              triangle records through shared memory in chunks, keeps the
-//              nearest (z/w, id) per pixel -- strictly nearer wins, equal
-//              depth keeps the lower id, which is what GL_LESS gives for
-//              triangles drawn in index order -- then writes
+//              nearest (z/w, id), then one atomicMin of its key;
+//   5. resolve one thread per pixel turns the winning key into
 //              (u, v, z/w, id+1) and the barycentric derivatives (DB).
-// A tile whose bin does not fit the bin-list capacity is rasterized by
-// testing every triangle of its view (same results, slower).
+// The key orders by depth, then by triangle id: strictly nearer wins and
+// equal depth keeps the lower id, which is what GL_LESS gives for triangles
+// drawn in index order.  A tile whose bin does not fit the bin-list
+// capacity is rasterized by testing every large triangle of its view (same
+// results, slower).
 //
 // The coverage/depth arithmetic uses explicitly rounded operations
 // (__fmul_rn etc., never fused) so that it is bit-identical to the CPU
@@ -42,6 +48,22 @@ struct __align__(16) RTri {
 };
 
 constexpr int CHUNK = 128;
+constexpr int SMALL_AREA = 256;   // box pixels up to which a triangle is rasterized by its setup thread
+constexpr unsigned long long KEY_NONE = ~0ull;
+
+// Order-preserving 64-bit key: depth bits (monotone map of the float, -0
+// folded onto +0 so that equal depths compare equal) then triangle id.
+DEV unsigned long long depth_key(float zw, int t) {
+    unsigned u = __float_as_uint(zw == 0.f ? 0.f : zw);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((unsigned long long)u << 32) | (unsigned)t;
+}
+DEV float key_depth(unsigned long long k) {
+    unsigned u = (unsigned)(k >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    return __uint_as_float(u);
+}
+DEV bool is_small(int4 b) { return (long long)(b.y - b.x + 1) * (b.w - b.z + 1) <= SMALL_AREA; }
 
 // Pixel-centre NDC coordinate (2p+1-W)/W: exact numerator, one rounding.
 DEV float ndc(int p, int W) { return dvd((float)(2 * p + 1 - W), (float)W); }
@@ -54,6 +76,22 @@ DEV bool edge_in(float A, float a, float b, float sigma) {
     if (A != 0.f) return false;
     float gx = mul(sigma, a), gy = mul(sigma, b);
     return gx > 0.f || (gx == 0.f && gy < 0.f);
+}
+
+// Coverage and depth of the pixel centre (sx, sy) against one triangle
+// record, including the clip range of z/w.  False when the pixel is not drawn.
+DEV bool pixel_test(const float4& a, const float4& b, const float4& k, const float4& z, const float4& w, float sx, float sy,
+                    float& zw) {
+    float A0 = edge(a.x, b.x, k.x, sx, sy);
+    float A1 = edge(a.y, b.y, k.y, sx, sy);
+    float A2 = edge(a.z, b.z, k.z, sx, sy);
+    if (!edge_in(A0, a.x, b.x, a.w) || !edge_in(A1, a.y, b.y, a.w) || !edge_in(A2, a.z, b.z, a.w)) return false;
+    float D = add(add(A0, A1), A2);
+    if (!(mul(a.w, D) > 0.f)) return false;
+    float zn = add(add(mul(A0, z.x), mul(A1, z.y)), mul(A2, z.z));
+    float wn = add(add(mul(A0, w.x), mul(A1, w.y)), mul(A2, w.z));
+    zw = dvd(zn, wn);
+    return zw >= -1.f && zw <= 1.f && zw < 1.f;
 }
 
 DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool& valid) {
@@ -95,7 +133,7 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
 
 __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W, int H,
                         int views, int tile, int tiles_x, int ntiles, RTri* __restrict__ setup, int* __restrict__ count,
-                        int* __restrict__ flags) {
+                        int* __restrict__ flags, unsigned long long* __restrict__ keys) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
@@ -111,6 +149,18 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
     }
     setup[gid] = r;
     if (r.box.x > r.box.y || r.box.z > r.box.w) return;
+    if (is_small(r.box)) {
+        unsigned long long* kv = keys + (size_t)view * W * H;
+        for (int py = r.box.z; py <= r.box.w; ++py) {
+            const float sy = ndc(py, H);
+            for (int px = r.box.x; px <= r.box.y; ++px) {
+                float zw;
+                if (pixel_test(r.a, r.b, r.k, r.z, r.w, ndc(px, W), sy, zw))
+                    atomicMin(&kv[(size_t)py * W + px], depth_key(zw, t));
+            }
+        }
+        return;
+    }
     int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
     int* cnt = count + (size_t)view * ntiles;
     for (int ty = ty0; ty <= ty1; ++ty)
@@ -151,7 +201,7 @@ __global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int ti
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
     int4 box = setup[gid].box;
-    if (box.x > box.y || box.z > box.w) return;
+    if (box.x > box.y || box.z > box.w || is_small(box)) return;
     int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
@@ -191,30 +241,31 @@ template <int T>
 __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, const int* __restrict__ count,
                                                 const int* __restrict__ offset, const int* __restrict__ list,
                                                 long long cap, int nt, int W, int H, int tiles_x, int ntiles,
-                                                const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri,
-                                                float4* __restrict__ rast, float4* __restrict__ db, int* __restrict__ flags) {
+                                                unsigned long long* __restrict__ keys, int* __restrict__ flags) {
     __shared__ RTri s_tri[CHUNK];
     __shared__ int s_id[CHUNK];
     const int view = blockIdx.y, tile_id = blockIdx.x;
+    const size_t ti = (size_t)view * ntiles + tile_id;
+    const int c = count[ti];
+    const int off = offset[ti];
+    const bool overflow = (long long)off + c > cap;
+    if (c == 0) return;
     const int tx = tile_id % tiles_x, ty = tile_id / tiles_x;
     const int px = tx * T + threadIdx.x, py = ty * T + threadIdx.y;
     const int tid = threadIdx.y * T + threadIdx.x;
     const bool inside = px < W && py < H;
     const float sx = ndc(px, W), sy = ndc(py, H);
-    const size_t ti = (size_t)view * ntiles + tile_id;
-    const int c = count[ti];
-    const int off = offset[ti];
-    const bool overflow = (long long)off + c > cap;
     const int n_iter = overflow ? nt : c;
     const RTri* vs = setup + (size_t)view * nt;
-    float best_z = 1.f;
-    int best_t = -1;
+    unsigned long long best = KEY_NONE;
     constexpr int CH = T * T < CHUNK ? T * T : CHUNK;   // records staged per pass (<= threads)
     for (int i0 = 0; i0 < n_iter; i0 += CH) {
         if (tid < CH && i0 + tid < n_iter) {
             int t = overflow ? i0 + tid : list[off + i0 + tid];
             s_id[tid] = t;
             s_tri[tid] = vs[t];
+            // in the all-triangles fallback the small ones are done already
+            if (overflow && is_small(s_tri[tid].box)) s_tri[tid].box = make_int4(1, 0, 1, 0);
         }
         __syncthreads();
         const int m = min(CH, n_iter - i0);
@@ -222,42 +273,46 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
             for (int j = 0; j < m; ++j) {
                 const int4 box = s_tri[j].box;
                 if (px < box.x || px > box.y || py < box.z || py > box.w) continue;
-                const float4 a = s_tri[j].a, b = s_tri[j].b, k = s_tri[j].k;
-                float A0 = edge(a.x, b.x, k.x, sx, sy);
-                float A1 = edge(a.y, b.y, k.y, sx, sy);
-                float A2 = edge(a.z, b.z, k.z, sx, sy);
-                if (!edge_in(A0, a.x, b.x, a.w) || !edge_in(A1, a.y, b.y, a.w) || !edge_in(A2, a.z, b.z, a.w)) continue;
-                float D = add(add(A0, A1), A2);
-                if (!(mul(a.w, D) > 0.f)) continue;
-                const float4 z = s_tri[j].z, w = s_tri[j].w;
-                float zn = add(add(mul(A0, z.x), mul(A1, z.y)), mul(A2, z.z));
-                float wn = add(add(mul(A0, w.x), mul(A1, w.y)), mul(A2, w.z));
-                float zw = dvd(zn, wn);
-                if (!(zw >= -1.f && zw <= 1.f)) continue;
-                int t = s_id[j];
-                if (zw < best_z || (zw == best_z && best_t >= 0 && t < best_t)) { best_z = zw; best_t = t; }
+                float zw;
+                if (!pixel_test(s_tri[j].a, s_tri[j].b, s_tri[j].k, s_tri[j].z, s_tri[j].w, sx, sy, zw)) continue;
+                const unsigned long long key = depth_key(zw, s_id[j]);
+                best = key < best ? key : best;
             }
         }
         __syncthreads();
     }
     if (overflow && tid == 0) atomicAdd(&flags[0], 1);
-    if (!inside) return;
-    const size_t pix = ((size_t)view * H + py) * W + px;
-    if (best_t < 0) {
+    if (inside && best != KEY_NONE) atomicMin(&keys[((size_t)view * H + py) * W + px], best);
+}
+
+// Winning key -> (u, v, z/w, id+1) and DB per pixel.
+__global__ void k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, long long npix,
+                          const unsigned long long* __restrict__ keys, const float4* __restrict__ clip, int nv,
+                          const uint32_t* __restrict__ tri, float4* __restrict__ rast, float4* __restrict__ db) {
+    const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= npix) return;
+    const unsigned long long key = keys[pix];
+    if (key == KEY_NONE) {
         rast[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (db) db[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    const RTri r = vs[best_t];
+    const long long hw = (long long)W * H;
+    const int view = (int)(pix / hw);
+    const int rem = (int)(pix - view * hw);
+    const int py = rem / W, px = rem - py * W;
+    const int t = (int)(unsigned)(key & 0xffffffffu);
+    const RTri r = setup[(size_t)view * nt + t];
+    const float sx = ndc(px, W), sy = ndc(py, H);
     float A0 = edge(r.a.x, r.b.x, r.k.x, sx, sy);
     float A1 = edge(r.a.y, r.b.y, r.k.y, sx, sy);
     float A2 = edge(r.a.z, r.b.z, r.k.z, sx, sy);
     float D = add(add(A0, A1), A2);
     float u = dvd(A0, D), v = dvd(A1, D);
-    rast[pix] = make_float4(u, v, best_z, (float)(best_t + 1));
+    rast[pix] = make_float4(u, v, key_depth(key), (float)(t + 1));
     if (db) {
         const float4* cv = clip + (size_t)view * nv;
-        float4 c0 = cv[tri[3 * (size_t)best_t]], c1 = cv[tri[3 * (size_t)best_t + 1]], c2 = cv[tri[3 * (size_t)best_t + 2]];
+        float4 c0 = cv[tri[3 * (size_t)t]], c1 = cv[tri[3 * (size_t)t + 1]], c2 = cv[tri[3 * (size_t)t + 2]];
         db[pix] = db_eval(c0, c1, c2, dvd(2.f, (float)W), dvd(2.f, (float)H), u, v);
     }
 }
@@ -308,6 +363,7 @@ __global__ void k_raster_bwd(const float* __restrict__ clip, int nv, const uint3
 }
 
 struct RasterWS {
+    unsigned long long* keys;
     RTri* setup;
     int* count;
     int* offset;
@@ -324,14 +380,16 @@ long long auto_capacity_(long long views, long long nt, int W, int H, int tile) 
     return c > (1ll << 31) - 1 ? (1ll << 31) - 1 : c;
 }
 
-size_t ws_bytes(long long views, long long nt, long long ntiles, long long cap) {
-    return align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1)) + 3 * align256(sizeof(int) * (size_t)ntiles) +
+size_t ws_bytes(long long npix, long long views, long long nt, long long ntiles, long long cap) {
+    return align256(sizeof(unsigned long long) * (size_t)npix) +
+           align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1)) + 3 * align256(sizeof(int) * (size_t)ntiles) +
            align256(sizeof(int) * (size_t)cap);
 }
 
-RasterWS carve(void* base, long long views, long long nt, long long ntiles, long long cap) {
+RasterWS carve(void* base, long long npix, long long views, long long nt, long long ntiles, long long cap) {
     char* p = (char*)base;
     RasterWS w;
+    w.keys = (unsigned long long*)p; p += align256(sizeof(unsigned long long) * (size_t)npix);
     w.setup = (RTri*)p; p += align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1));
     w.count = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
     w.offset = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
@@ -349,18 +407,21 @@ long long raster_auto_capacity(long long views, long long nt, int W, int H, int 
 
 size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap) {
     long long ntiles = (long long)((W + tile - 1) / tile) * ((H + tile - 1) / tile) * views;
-    return ws_bytes(views, nt, ntiles, cap);
+    return ws_bytes((long long)W * H * views, views, nt, ntiles, cap);
 }
 
-int raster_fwd_launches() { return 4; }
+int raster_fwd_launches() { return 5; }
 
 vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const float* clip, int nv, const uint32_t* tri,
                          int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s) {
     const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
     const long long ntiles_view = (long long)tiles_x * tiles_y;
     const long long ntiles = ntiles_view * views;
-    RasterWS w = carve(ws, views, nt, ntiles, cap);
-    vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
+    const long long npix = (long long)W * H * views;
+    RasterWS w = carve(ws, npix, views, nt, ntiles, cap);
+    vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(w.keys, 0xff, sizeof(unsigned long long) * npix, s), "raster memset");
+    if (st) return st;
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
     st = vcl_cuda_check(ctx, cudaMemsetAsync(w.cursor, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
@@ -369,7 +430,7 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const flo
     long long work = (long long)views * nt;
     if (work > 0) {
         k_setup<<<vcl_blocks(work, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
-                                                       (int)ntiles_view, w.setup, w.count, ctx->dev_flags);
+                                                       (int)ntiles_view, w.setup, w.count, ctx->dev_flags, w.keys);
     }
     k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
     if (work > 0) {
@@ -377,16 +438,17 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const flo
                                                       w.cursor, w.list, cap);
     }
     dim3 grid((unsigned)ntiles_view, (unsigned)views);
-    const float4* c4 = (const float4*)clip;
     if (T == 8)
         k_fine<8><<<grid, dim3(8, 8), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                             (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+                                             (int)ntiles_view, w.keys, ctx->dev_flags);
     else if (T == 16)
         k_fine<16><<<grid, dim3(16, 16), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+                                               (int)ntiles_view, w.keys, ctx->dev_flags);
     else
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, c4, nv, tri, (float4*)rast, (float4*)db, ctx->dev_flags);
+                                               (int)ntiles_view, w.keys, ctx->dev_flags);
+    k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, (const float4*)clip, nv, tri,
+                                                     (float4*)rast, (float4*)db);
     return vcl_launch_check(ctx, "rasterize_fwd");
 }
 
@@ -400,7 +462,7 @@ VCL_API vcl_status vcl_reserve_raster(vcl_ctx* ctx, int W, int H, int views, int
     size_t need = 0;
     for (int t : ts) {
         long long ntiles = (long long)((W + t - 1) / t) * ((H + t - 1) / t) * views;
-        size_t b = ws_bytes(views, nt, ntiles, cap);
+        size_t b = ws_bytes((long long)W * H * views, views, nt, ntiles, cap);
         if (b > need) need = b;
     }
     return vcl_ws_reserve(ctx, need);
@@ -422,7 +484,7 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     const long long ntiles = ntiles_view * views;
     VCL_REQUIRE(ntiles < (1ll << 31), "too many tiles");
     long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity_(views, nt, W, H, T);
-    vcl_status st = vcl_ws_reserve(ctx, ws_bytes(views, nt, ntiles, cap));
+    vcl_status st = vcl_ws_reserve(ctx, ws_bytes((long long)W * H * views, views, nt, ntiles, cap));
     if (st) return st;
     return raster_fwd_ws(ctx, ctx->ws, T, cap, clip, nv, tri, nt, W, H, views, rast, db, s);
 }
