@@ -105,6 +105,24 @@ VCL_API vcl_status vcl_project_bwd(vcl_ctx* ctx, const float* mats, int views, c
  * bit-identical to the CPU restatement of the same rules. */
 VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
                                      int W, int H, int views, float* rast, float* db, void* stream);
+/* vcl_rasterize_fwd on a fixed scratch area that is part of the loaded
+ * module (a file-scope device array of VCL_RASTER_SCRATCH_BYTES) instead of
+ * the context workspace: the call allocates nothing, for callers that must
+ * not allocate device memory or synchronize the device on their per-frame
+ * path.  No counterpart in the reference (its rasterizer has no workspace).
+ * Same arguments and results as vcl_rasterize_fwd.  Requests whose depth
+ * keys (8 B per pixel and view), triangle records (80 B per view and
+ * triangle) and tile counters exceed the limit return VCL_ERR_ARG.  No part
+ * of the scratch needs to start at zero.  One scratch per device: calls
+ * whose work overlaps on the device race, so serialize them.  The first call
+ * per device (or vcl_raster_scratch_init) resolves the scratch address with
+ * the context's device current; make it during set-up, before any stream
+ * capture. */
+#define VCL_RASTER_SCRATCH_BYTES (32u << 20)
+VCL_API size_t vcl_raster_scratch_bytes(void);
+VCL_API vcl_status vcl_raster_scratch_init(vcl_ctx* ctx);
+VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
+                                            int W, int H, int views, float* rast, float* db, void* stream);
 /* Rasterize::backward (rasterize.cu:143-148, kernel :84-141): grad_clip
  * (x, y, w of each vertex) += dL/d(clip) from grad_bary [pixels][2].  The
  * DB gradient is not consumed (as in the reference). */

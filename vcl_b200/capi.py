@@ -37,6 +37,9 @@ SIGNATURES = {
     "vcl_project_fwd": (c_int, [P, P, c_int, P, c_int, c_int, P, P]),
     "vcl_project_bwd": (c_int, [P, P, c_int, P, c_int, c_int, P, P]),
     "vcl_rasterize_fwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
+    "vcl_raster_scratch_bytes": (c_size, []),
+    "vcl_raster_scratch_init": (c_int, [P]),
+    "vcl_rasterize_fwd_static": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
     "vcl_rasterize_bwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
     "vcl_interpolate_fwd": (c_int, [P, P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P]),
     "vcl_interpolate_bwd": (c_int, [P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P, P]),
