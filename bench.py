@@ -1,10 +1,13 @@
 """Benchmark: fit iterations per second (forward + backward + Adam) of the
-inverse-rendering fit on the scale configuration -- UV sphere 256x128
-(65,024 triangles) displaced N(0,0.02), 8 views of 1024x1024, 2048^2 RGBA
-texture with 12 mip levels, 32 SG lobes, Adam on positions, texture and
-lobes -- with seeded synthetic inputs (no dataset).
+inverse-rendering fit at 1024^2 with a batch of 16 views -- UV sphere
+256x128 (65,024 triangles) displaced N(0,0.02), 16 views of 1024x1024 at
+seeded cameras, 2048^2 RGBA texture with 12 mip levels, 32 SG lobes, Adam
+on positions, texture and lobes -- with seeded synthetic inputs (no
+dataset).  The fused graph-captured step ("batched") is timed beside the
+plain one-launch-per-operator pipeline.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vcl|reference]
+                  [--views V] [--config config1|config2|config5|mix|serve]
 
 One JSON line on rank 0.  Multi-GPU runs are independent replicas (one fit
 job per GPU, no data-path collective; weak scaling); times are max over
@@ -33,8 +36,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vcl", choices=["vcl", "reference"])
-    ap.add_argument("--views", type=int, default=8)
-    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5"])
+    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5", "mix", "serve"])
+    ap.add_argument("--scenes", type=int, default=64, help="mix: scenes per batched launch")
+    ap.add_argument("--jobs", type=int, default=32, help="serve: fit jobs submitted")
+    ap.add_argument("--lams", default="10,30,100,300,1000", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -384,6 +390,38 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_mixed(args, rank, world):
+    """--config mix / serve: the batched engine and the serving loop on the
+    uneven scene mix (one GPU; replicas when launched with several ranks)."""
+    import torch
+    from vcl_b200 import capi, mixbench
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    ctx = capi.Context(dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if args.config == "mix":
+        r = mixbench.run_mix(ctx, args.scenes, args.steps, args.warmup)
+        metric = "scene fit-iterations/s (fwd+bwd+Adam), uneven scene mix, batched vs plain"
+    else:
+        r = mixbench.run_serve(ctx, args.jobs, [float(x) for x in args.lams.split(",")])
+        metric = "fit-job p50/p99 latency and iters/s under Poisson arrivals, served vs plain one at a time"
+    clk = clocks.stop()
+    ctx.close()
+    if rank != 0:
+        return
+    line = {"metric": metric, "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "dtype": "f32",
+            "data": "synthetic (seeded; no dataset)", "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "clocks": clk}
+    line.update(r)
+    if args.config == "serve":
+        best = max(r["sweep"], key=lambda x: x["iters_per_s"])
+        line.update(value=best["iters_per_s"], unit="iters/s",
+                    config={"workload": f"{r['jobs']} fit jobs from the uneven scene mix, U[50,500] iterations, "
+                                        f"Poisson arrivals, {r['budget_gb']} GB admission budget"})
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,6 +430,8 @@ def main():
         if rank == 0:
             print(json.dumps(run_reference(args, rank, world)), flush=True)
         return
+    if args.config in ("mix", "serve"):
+        return run_mixed(args, rank, world)
     import torch
     if world > 1:
         import datetime

@@ -312,11 +312,76 @@ VCL_API vcl_status vcl_fit_read_params(vcl_fit* fit, float* pos, float* tex_leve
  * and the measured milliseconds per raster call for each (ms_per_tile[3],
  * may be NULL). */
 VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* fit, int* tile, float* ms_per_tile);
-/* Device bytes held by a job with this descriptor (for admission). */
+/* The fused strategy's raster binning schedule for this job: tile edge,
+ * box area (pixels) up to which triangles are rasterized directly instead
+ * of binned, bin-list capacity, whether it came from the process-wide tuning
+ * cache, and the overflowed tiles of the last step (any pointer may be
+ * NULL; overflow_tiles synchronizes the device).  The autotuner times tile
+ * {8, 16, 32} x direct area {0, 64, 256, 1024} on the job's first fused step
+ * and sizes the capacity to twice the measured bin demand (at least the
+ * automatic capacity); jobs of the same
+ * (W, H, views, power-of-two triangle count) reuse the cached choice. */
+VCL_API vcl_status vcl_fit_raster_schedule(vcl_fit* fit, int* tile, int* small_area, long long* bin_capacity,
+                                           int* from_cache, long long* overflow_tiles);
+VCL_API void vcl_raster_tuning_cache_clear(void);
+/* Device bytes a job with this descriptor holds at most (arena plus the
+ * fused strategy's raster workspace), for admission control. */
 VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc);
 /* Number of kernel launches one vcl_fit_step issues with the current
  * strategy (memsets and copies not counted). */
 VCL_API int vcl_fit_launches_per_step(const vcl_fit* fit);
+
+/* ------------------------------------------------------------- batches */
+/* Batched engine: resident fit jobs of any sizes advanced together, one
+ * iteration each per vcl_batch_step, as ONE CUDA graph launch.  Every member
+ * runs the fused strategy (vcl_batch_add switches it); its captured step is
+ * a child graph with no edges to the others, so members run concurrently.
+ * The graph is rebuilt when membership or the mode changes.  No reference
+ * counterpart (the reference runs one scene per process).  Remove a job
+ * before destroying it; one host thread per batch. */
+typedef struct vcl_batch vcl_batch;
+VCL_API vcl_status vcl_batch_create(vcl_ctx* ctx, vcl_batch** out);
+VCL_API void vcl_batch_destroy(vcl_batch* batch);
+VCL_API vcl_status vcl_batch_add(vcl_batch* batch, vcl_fit* fit);
+VCL_API vcl_status vcl_batch_remove(vcl_batch* batch, vcl_fit* fit);
+VCL_API int vcl_batch_size(const vcl_batch* batch);
+VCL_API vcl_status vcl_batch_step(vcl_batch* batch, void* stream);
+VCL_API int vcl_batch_launches_per_step(const vcl_batch* batch);
+
+/* -------------------------------------------------------------- serving */
+/* Serving loop: fit jobs are submitted with their host data and an
+ * iteration count, admitted in arrival order while their footprint fits
+ * `budget_bytes` and fewer than `max_live` jobs are resident, advanced
+ * together one iteration per tick by a batched launch, and retired when
+ * done.  Each tick leaves one batched launch queued behind the running one.
+ * Job latency = completion - submission on the host's steady clock.  All
+ * host arrays are copied at submission.  No reference counterpart. */
+typedef struct vcl_server vcl_server;
+#define VCL_JOB_QUEUED 0
+#define VCL_JOB_LIVE 1
+#define VCL_JOB_DONE 2
+#define VCL_JOB_FAILED 3
+VCL_API vcl_status vcl_server_create(vcl_ctx* ctx, size_t budget_bytes, int max_live, vcl_server** out);
+VCL_API void vcl_server_destroy(vcl_server* server);
+VCL_API const char* vcl_server_last_error(const vcl_server* server);
+/* target: host images [views][H][W][4].  keep_result: keep the final
+ * parameters for vcl_server_job_result. */
+VCL_API vcl_status vcl_server_submit(vcl_server* server, const vcl_fit_desc* desc, const float* target,
+                                     int iterations, int keep_result, long long* job_id);
+/* Retire finished jobs, admit queued ones, launch one batched iteration of
+ * every live job, wait for the previous tick.  Outputs may be NULL. */
+VCL_API vcl_status vcl_server_tick(vcl_server* server, void* stream, int* live, int* completed);
+VCL_API vcl_status vcl_server_drain(vcl_server* server, void* stream);
+/* The server's clock (ms since creation; the clock of the job times). */
+VCL_API double vcl_server_now_ms(const vcl_server* server);
+/* Jobs queued, live or finishing. */
+VCL_API int vcl_server_pending(const vcl_server* server);
+VCL_API vcl_status vcl_server_job_status(const vcl_server* server, long long job_id, int* state, int* iters_done,
+                                         double* submit_ms, double* admit_ms, double* done_ms);
+VCL_API vcl_status vcl_server_job_result(const vcl_server* server, long long job_id, float* pos, float* tex_level0,
+                                         float* lobe_axis, float* lobe_sharp, float* lobe_amp, float* loss);
+VCL_API vcl_status vcl_server_stats(const vcl_server* server, double* p50_ms, double* p99_ms, long long* iterations,
+                                    int* completed, long long* ticks, size_t* resident_bytes);
 
 #ifdef __cplusplus
 }

@@ -72,6 +72,26 @@ SIGNATURES = {
     "vcl_fit_footprint": (c_size, [P]),
     "vcl_fit_raster_tuning": (c_int, [P, P, P]),
     "vcl_fit_launches_per_step": (c_int, [P]),
+    "vcl_fit_raster_schedule": (c_int, [P, P, P, P, P, P]),
+    "vcl_raster_tuning_cache_clear": (None, []),
+    "vcl_batch_create": (c_int, [P, ctypes.POINTER(c_void_p)]),
+    "vcl_batch_destroy": (None, [P]),
+    "vcl_batch_add": (c_int, [P, P]),
+    "vcl_batch_remove": (c_int, [P, P]),
+    "vcl_batch_size": (c_int, [P]),
+    "vcl_batch_step": (c_int, [P, P]),
+    "vcl_batch_launches_per_step": (c_int, [P]),
+    "vcl_server_create": (c_int, [P, c_size, c_int, ctypes.POINTER(c_void_p)]),
+    "vcl_server_destroy": (None, [P]),
+    "vcl_server_last_error": (c_char_p, [P]),
+    "vcl_server_submit": (c_int, [P, P, P, c_int, c_int, P]),
+    "vcl_server_tick": (c_int, [P, P, P, P]),
+    "vcl_server_drain": (c_int, [P, P]),
+    "vcl_server_pending": (c_int, [P]),
+    "vcl_server_now_ms": (c_double, [P]),
+    "vcl_server_job_status": (c_int, [P, c_ll, P, P, P, P, P]),
+    "vcl_server_job_result": (c_int, [P, c_ll, P, P, P, P, P, P]),
+    "vcl_server_stats": (c_int, [P, P, P, P, P, P, P]),
 }
 
 FIT_PLAIN = 0
@@ -183,29 +203,43 @@ class Context:
         return lambda *a: self.call(name, *a)
 
 
+def fit_desc(S, tex=None, pos=None, lobes=None, learn=(1, 1, 1)):
+    """vcl_fit_desc for scene S (starting values default to the scene's
+    initial ones).  Returns (desc, arrays): the arrays back the descriptor's
+    host pointers and must outlive its use."""
+    import numpy as np
+    tex = S.tex_init if tex is None else tex
+    pos = S.pos if pos is None else pos
+    axis, sharp, amp = lobes if lobes is not None else (S.lobe_axis_init, S.lobe_sharp_init, S.lobe_amp_init)
+    keep = [np.ascontiguousarray(a, dtype=dt) for a, dt in (
+        (pos, np.float32), (S.tri, np.uint32), (S.uv, np.float32), (S.normal, np.float32), (tex, np.float32),
+        (axis, np.float32), (sharp, np.float32), (amp, np.float32), (S.mvp, np.float32), (S.pvinv, np.float32),
+        (S.rot, np.float32))]
+    d = FitDesc()
+    d.W, d.H, d.views, d.C, d.K = S.W, S.H, S.views, S.C, S.K
+    d.nv, d.nt, d.tex_w, d.tex_h, d.levels = S.nv, S.nt, S.tex_w, S.tex_h, S.levels
+    (d.pos, d.tri, d.uv, d.normal, d.tex, d.lobe_axis, d.lobe_sharp, d.lobe_amp, d.mvp, d.pvinv,
+     d.rot) = [a.ctypes.data for a in keep]
+    d.roughness, d.ior = S.roughness, S.ior
+    d.lr, d.beta1, d.beta2, d.eps = S.lr, 0.9, 0.999, 1e-8
+    d.learn_pos, d.learn_tex, d.learn_lobes = learn
+    return d, keep
+
+
+def footprint(S):
+    """Device bytes a fit job for scene S holds at most."""
+    d, keep = fit_desc(S)
+    return lib().vcl_fit_footprint(ctypes.byref(d))
+
+
 class Fit:
     """A resident fit job (vcl_fit_*).  `scene` is a vcl_b200.scenes.Scene;
     its host arrays are uploaded at creation."""
 
     def __init__(self, ctx, scene, tex=None, pos=None, lobes=None, learn=(1, 1, 1), strategy=FIT_PLAIN):
-        import numpy as np
         self.ctx = ctx
-        self.scene = S = scene
-        tex = S.tex_init if tex is None else tex
-        pos = S.pos if pos is None else pos
-        axis, sharp, amp = lobes if lobes is not None else (S.lobe_axis_init, S.lobe_sharp_init, S.lobe_amp_init)
-        keep = [np.ascontiguousarray(a, dtype=dt) for a, dt in (
-            (pos, np.float32), (S.tri, np.uint32), (S.uv, np.float32), (S.normal, np.float32), (tex, np.float32),
-            (axis, np.float32), (sharp, np.float32), (amp, np.float32), (S.mvp, np.float32), (S.pvinv, np.float32),
-            (S.rot, np.float32))]
-        d = FitDesc()
-        d.W, d.H, d.views, d.C, d.K = S.W, S.H, S.views, S.C, S.K
-        d.nv, d.nt, d.tex_w, d.tex_h, d.levels = S.nv, S.nt, S.tex_w, S.tex_h, S.levels
-        (d.pos, d.tri, d.uv, d.normal, d.tex, d.lobe_axis, d.lobe_sharp, d.lobe_amp, d.mvp, d.pvinv,
-         d.rot) = [a.ctypes.data for a in keep]
-        d.roughness, d.ior = S.roughness, S.ior
-        d.lr, d.beta1, d.beta2, d.eps = S.lr, 0.9, 0.999, 1e-8
-        d.learn_pos, d.learn_tex, d.learn_lobes = learn
+        self.scene = scene
+        d, keep = fit_desc(scene, tex, pos, lobes, learn)
         self.desc = d
         h = c_void_p()
         ctx._check(ctx.lib.vcl_fit_create(ctx.h, ctypes.byref(d), ctypes.byref(h)), "vcl_fit_create")
@@ -271,3 +305,140 @@ class Fit:
         self._c(self.ctx.lib.vcl_fit_read_params(self.h, pos.ctypes.data, tex.ctypes.data, ax.ctypes.data,
                                                  sh.ctypes.data, am.ctypes.data, stream), "vcl_fit_read_params")
         return pos, tex, (ax, sh, am)
+
+    def raster_schedule(self):
+        """(tile, direct-raster box area, bin capacity, from cache, overflowed tiles of the last step)."""
+        t, sa, cached = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        cap, ov = c_ll(), c_ll()
+        self._c(self.ctx.lib.vcl_fit_raster_schedule(self.h, ctypes.byref(t), ctypes.byref(sa), ctypes.byref(cap),
+                                                     ctypes.byref(cached), ctypes.byref(ov)),
+                "vcl_fit_raster_schedule")
+        return t.value, sa.value, cap.value, bool(cached.value), ov.value
+
+
+class Batch:
+    """vcl_batch: fit jobs advanced together by one graph launch per step."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = c_void_p()
+        ctx._check(ctx.lib.vcl_batch_create(ctx.h, ctypes.byref(h)), "vcl_batch_create")
+        self.h = h
+        self.jobs = []
+
+    def add(self, fit):
+        self.ctx._check(self.ctx.lib.vcl_batch_add(self.h, fit.h), "vcl_batch_add")
+        self.jobs.append(fit)
+
+    def remove(self, fit):
+        self.ctx._check(self.ctx.lib.vcl_batch_remove(self.h, fit.h), "vcl_batch_remove")
+        self.jobs.remove(fit)
+
+    def step(self, stream=None):
+        self.ctx._check(self.ctx.lib.vcl_batch_step(self.h, stream), "vcl_batch_step")
+
+    def launches_per_step(self):
+        return self.ctx.lib.vcl_batch_launches_per_step(self.h)
+
+    def __len__(self):
+        return self.ctx.lib.vcl_batch_size(self.h)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.vcl_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+JOB_QUEUED, JOB_LIVE, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """vcl_server: admission by device footprint, continuous batching of the
+    live jobs' iterations, p50/p99 job latency."""
+
+    def __init__(self, ctx, budget_bytes, max_live=64):
+        self.ctx = ctx
+        h = c_void_p()
+        st = ctx.lib.vcl_server_create(ctx.h, int(budget_bytes), int(max_live), ctypes.byref(h))
+        if st:
+            raise VclError(f"vcl_server_create failed with status {st}")
+        self.h = h
+        self.scenes = {}
+
+    def _c(self, st, name):
+        if st:
+            msg = self.ctx.lib.vcl_server_last_error(self.h)
+            raise VclError(f"{name} failed (status {st}): {msg.decode() if msg else ''}")
+
+    def submit(self, scene, target, iterations, keep_result=False):
+        """target: host float32 array [views][H][W][4]."""
+        import numpy as np
+        d, keep = fit_desc(scene)
+        t = np.ascontiguousarray(target, dtype=np.float32)
+        jid = c_ll()
+        self._c(self.ctx.lib.vcl_server_submit(self.h, ctypes.byref(d), t.ctypes.data, int(iterations),
+                                               int(keep_result), ctypes.byref(jid)), "vcl_server_submit")
+        self.scenes[jid.value] = scene
+        return jid.value
+
+    def tick(self, stream=None):
+        live, done = ctypes.c_int(), ctypes.c_int()
+        self._c(self.ctx.lib.vcl_server_tick(self.h, stream, ctypes.byref(live), ctypes.byref(done)),
+                "vcl_server_tick")
+        return live.value, done.value
+
+    def drain(self, stream=None):
+        self._c(self.ctx.lib.vcl_server_drain(self.h, stream), "vcl_server_drain")
+
+    def pending(self):
+        return self.ctx.lib.vcl_server_pending(self.h)
+
+    def now_ms(self):
+        return self.ctx.lib.vcl_server_now_ms(self.h)
+
+    def status(self, jid):
+        st, it = ctypes.c_int(), ctypes.c_int()
+        sub, adm, done = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._c(self.ctx.lib.vcl_server_job_status(self.h, jid, ctypes.byref(st), ctypes.byref(it), ctypes.byref(sub),
+                                                   ctypes.byref(adm), ctypes.byref(done)), "vcl_server_job_status")
+        return dict(state=st.value, iters=it.value, submit_ms=sub.value, admit_ms=adm.value, done_ms=done.value)
+
+    def result(self, jid):
+        import numpy as np
+        S = self.scenes[jid]
+        pos = np.zeros((S.nv, 3), np.float32)
+        tex = np.zeros((S.tex_h, S.tex_w, S.C), np.float32)
+        ax = np.zeros((S.K, 3), np.float32); sh = np.zeros(S.K, np.float32); am = np.zeros((S.K, S.C), np.float32)
+        loss = ctypes.c_float()
+        self._c(self.ctx.lib.vcl_server_job_result(self.h, jid, pos.ctypes.data, tex.ctypes.data, ax.ctypes.data,
+                                                   sh.ctypes.data, am.ctypes.data, ctypes.byref(loss)),
+                "vcl_server_job_result")
+        return pos, tex, (ax, sh, am), loss.value
+
+    def stats(self):
+        p50, p99 = ctypes.c_double(), ctypes.c_double()
+        iters, ticks = c_ll(), c_ll()
+        comp = ctypes.c_int()
+        res = c_size()
+        self._c(self.ctx.lib.vcl_server_stats(self.h, ctypes.byref(p50), ctypes.byref(p99), ctypes.byref(iters),
+                                              ctypes.byref(comp), ctypes.byref(ticks), ctypes.byref(res)),
+                "vcl_server_stats")
+        return dict(p50_ms=p50.value, p99_ms=p99.value, iterations=iters.value, completed=comp.value,
+                    ticks=ticks.value, resident_bytes=res.value)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.vcl_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

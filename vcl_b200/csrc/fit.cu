@@ -103,7 +103,7 @@ VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc) {
     if (!desc) return 0;
     Layout L;
     plan(*desc, nullptr, L);
-    return L.total;
+    return L.total + fit_fused_footprint(*desc);
 }
 
 VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fit** out) {
@@ -267,6 +267,14 @@ VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* f, int* tile, float* ms_per_ti
     if (!f) return VCL_ERR_ARG;
     return fit_fused_raster_tuning(f, tile, ms_per_tile);
 }
+
+VCL_API vcl_status vcl_fit_raster_schedule(vcl_fit* f, int* tile, int* small_area, long long* bin_capacity,
+                                           int* from_cache, long long* overflow_tiles) {
+    if (!f) return VCL_ERR_ARG;
+    return fit_fused_raster_schedule(f, tile, small_area, bin_capacity, from_cache, overflow_tiles);
+}
+
+VCL_API void vcl_raster_tuning_cache_clear(void) { fit_fused_tuning_cache_clear(); }
 
 VCL_API vcl_status vcl_fit_step(vcl_fit* f, void* stream) {
     if (!f) return VCL_ERR_ARG;

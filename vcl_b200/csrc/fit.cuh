@@ -31,3 +31,12 @@ int fit_fused_launches(const vcl_fit* f);
 void fit_fused_release(vcl_fit* f);
 vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device);
 vcl_status fit_fused_raster_tuning(vcl_fit* f, int* tile, float* ms3);
+vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, long long* cap, int* cached,
+                                     long long* overflow);
+void fit_fused_tuning_cache_clear();
+// Device bytes the fused strategy adds to a job (raster workspace upper
+// bound and step state).
+size_t fit_fused_footprint(const vcl_fit_desc& d);
+// The job's fused step as a CUDA graph (captured on `s` the first time; owned
+// by the job, valid until the job is destroyed or the mode changes).
+vcl_status fit_fused_graph(vcl_fit* f, cudaStream_t s, cudaGraph_t* out);

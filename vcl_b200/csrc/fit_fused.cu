@@ -24,6 +24,10 @@
 // On a non-default stream the whole step is captured once into a CUDA
 // graph and replayed (the step index lives in device memory, so the graph
 // never changes).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "fit.cuh"
 #include "sg_math.cuh"
 #include "tex_math.cuh"
@@ -34,15 +38,17 @@ namespace {
 
 struct Fused {
     void* raster_ws = nullptr;
-    int tile = 16;
-    long long cap = 0;
+    size_t raster_ws_bytes = 0;
+    RasterSched sched{16, 0, 0};
+    bool sched_cached = false;                 // schedule taken from the tuning cache
+    int* flags = nullptr;                      // [0] overflowed raster tiles of the last step
     int* d_step = nullptr;
     double* d_corr = nullptr;    // 1 - beta1^t', 1 - beta2^t'
+    cudaGraph_t graph_def = nullptr;           // the captured step (child of batch graphs)
     cudaGraphExec_t graph = nullptr;
-    cudaStream_t graph_stream = nullptr;
     int graph_mode = -1;
     cudaStream_t side = nullptr;               // lobe-gradient branch
-    float tune_ms[3] = {0.f, 0.f, 0.f};        // raster time per tile size 8/16/32
+    float tune_ms[3] = {0.f, 0.f, 0.f};        // best raster time per tile size 8/16/32
     cudaEvent_t fork = nullptr, join = nullptr;
 };
 
@@ -479,25 +485,15 @@ vcl_status fused_init(vcl_fit* f) {
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
     Fused* F = new Fused();
-    F->tile = ctx->tile;
-    long long cap = 0;
-    size_t ws = 0;
-    for (int t : {8, 16, 32}) {
-        long long c = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
-        if (c > cap) cap = c;
-    }
-    for (int t : {8, 16, 32}) {
-        size_t b = raster_ws_size(d.W, d.H, d.views, d.nt, t, cap);
-        if (b > ws) ws = b;
-    }
-    F->cap = cap;
-    cudaError_t e = cudaMalloc(&F->raster_ws, ws);
-    if (e == cudaSuccess) e = cudaMalloc(&F->d_step, 64);
+    cudaError_t e = cudaMalloc(&F->d_step, 64);
     if (e == cudaSuccess) e = cudaMalloc(&F->d_corr, 64);
+    if (e == cudaSuccess) e = cudaMalloc(&F->flags, 64);
+    if (e == cudaSuccess) e = cudaMemset(F->flags, 0, 64);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        if (F->raster_ws) cudaFree(F->raster_ws);
         if (F->d_step) cudaFree(F->d_step);
+        if (F->d_corr) cudaFree(F->d_corr);
+        if (F->flags) cudaFree(F->flags);
         delete F;
         return vcl_fail(ctx, VCL_ERR_NOMEM, "fused fit state: %s", cudaGetErrorString(e));
     }
@@ -514,40 +510,141 @@ vcl_status fused_init(vcl_fit* f) {
     return autotune_raster(f);
 }
 
-// Raster autotuner: times the tile binning schedules (tile edge 8, 16, 32
-// with the automatic bin capacity) on this job's own geometry and keeps the
-// fastest for the job's captured step.  Runs once, outside any capture.
+vcl_status raster_ws_ensure(vcl_fit* f, size_t bytes) {
+    Fused* F = (Fused*)f->fused;
+    if (bytes <= F->raster_ws_bytes) return VCL_OK;
+    if (F->raster_ws) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return vcl_cuda_check(f->ctx, e, "raster workspace sync");
+        cudaFree(F->raster_ws);
+        F->raster_ws = nullptr;
+        F->raster_ws_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&F->raster_ws, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return vcl_fail(f->ctx, VCL_ERR_NOMEM, "raster workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    F->raster_ws_bytes = bytes;
+    return VCL_OK;
+}
+
+// Process-wide cache of tuned raster schedules, keyed by the image size, the
+// number of views and the triangle count's power-of-two bucket.
+struct TuneKey {
+    int W, H, views, nt_log2;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(W, H, views, nt_log2) < std::tie(o.W, o.H, o.views, o.nt_log2);
+    }
+};
+struct TuneVal {
+    int tile, small_area;
+    double cap_per_tri;   // bin entries per (view, triangle)
+    float ms[3];
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+TuneKey tune_key(const vcl_fit_desc& d) {
+    int lg = 0;
+    while ((1ll << (lg + 1)) <= (long long)d.nt) ++lg;
+    return TuneKey{d.W, d.H, d.views, lg};
+}
+
+// The automatic capacity (6 entries per view and triangle plus headroom) is
+// the floor: the bins of a deforming mesh grow during the fit, and an
+// overflowing tile takes the slow every-triangle path.
+long long cap_floor(const vcl_fit_desc& d, int tile) { return raster_auto_capacity(d.views, d.nt, d.W, d.H, tile); }
+
+// Raster autotuner.  Times the binning schedules -- tile edge {8, 16, 32} x
+// direct-rasterization box area {0, 64, 256, 1024} pixels -- on this job's
+// own geometry, keeps the fastest, then sizes the bin-list capacity to twice
+// the entries that schedule asked for, never below the automatic capacity
+// (the mesh moves during the fit; an overflowing tile still gets exact
+// results through the all-triangle fallback, only slower).  Jobs of the same size bucket reuse the cached choice.  Runs
+// once per job, outside any capture.
 vcl_status autotune_raster(vcl_fit* f) {
     vcl_ctx* ctx = f->ctx;
     Fused* F = (Fused*)f->fused;
     const vcl_fit_desc& d = f->d;
+    const TuneKey key = tune_key(d);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            long long cap = (long long)(it->second.cap_per_tri * d.views * d.nt);
+            if (cap < cap_floor(d, it->second.tile)) cap = cap_floor(d, it->second.tile);
+            F->sched = RasterSched{it->second.tile, cap, it->second.small_area};
+            for (int i = 0; i < 3; ++i) F->tune_ms[i] = it->second.ms[i];
+            F->sched_cached = true;
+            return raster_ws_ensure(f, raster_ws_size(d.W, d.H, d.views, d.nt, F->sched.tile, cap));
+        }
+    }
+    const int tiles[3] = {8, 16, 32};
+    const int smalls[4] = {0, 64, 256, 1024};
+    long long cap = 0;
+    size_t ws = 0;
+    for (int t : tiles) {
+        long long c = raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
+        if (c > cap) cap = c;
+    }
+    for (int t : tiles) {
+        size_t b = raster_ws_size(d.W, d.H, d.views, d.nt, t, cap);
+        if (b > ws) ws = b;
+    }
+    vcl_status st = raster_ws_ensure(f, ws);
+    if (st) return st;
     cudaStream_t s = F->side;
-    vcl_status st = vcl_project_fwd(ctx, f->mvp, d.views, f->pos, d.nv, 4, f->clip, s);
+    st = vcl_project_fwd(ctx, f->mvp, d.views, f->pos, d.nv, 4, f->clip, s);
     if (st) return st;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
         return vcl_fail(ctx, VCL_ERR_CUDA, "autotune events");
     float best = 1e30f;
-    int best_tile = F->tile;
-    for (int t : {8, 16, 32}) {
-        for (int rep = 0; rep < 4 && st == VCL_OK; ++rep) {
-            if (rep == 1) cudaEventRecord(e0, s);
-            st = raster_fwd_ws(ctx, F->raster_ws, t, F->cap, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views, f->rast,
-                               f->db, s);
+    RasterSched pick{16, cap, raster_default_small_area()};
+    for (int i = 0; i < 3; ++i) F->tune_ms[i] = 1e30f;
+    for (int ti = 0; ti < 3 && st == VCL_OK; ++ti) {
+        for (int sa : smalls) {
+            RasterSched rs{tiles[ti], cap, sa};
+            for (int rep = 0; rep < 4 && st == VCL_OK; ++rep) {
+                if (rep == 1) cudaEventRecord(e0, s);
+                st = raster_fwd_ws(ctx, F->raster_ws, rs, F->flags, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views,
+                                   f->rast, f->db, s);
+            }
+            cudaEventRecord(e1, s);
+            if (st) break;
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= 3.f;
+            if (ms < F->tune_ms[ti]) F->tune_ms[ti] = ms;
+            if (ms < best) { best = ms; pick = rs; }
         }
-        cudaEventRecord(e1, s);
-        if (st) break;
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        F->tune_ms[t == 8 ? 0 : t == 16 ? 1 : 2] = ms / 3.f;
-        if (ms < best) { best = ms; best_tile = t; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st) return st;
-    F->tile = best_tile;
-    return vcl_cuda_check(ctx, cudaStreamSynchronize(s), "autotune");
+    // bin demand of the chosen schedule on the starting geometry
+    st = raster_fwd_ws(ctx, F->raster_ws, pick, F->flags, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views, f->rast,
+                       f->db, s);
+    long long demand = 0;
+    if (!st) st = raster_bin_demand(ctx, F->raster_ws, pick, d.W, d.H, d.views, d.nt, s, &demand);
+    if (st) return st;
+    long long sized = 2 * demand;
+    if (sized < cap_floor(d, pick.tile)) sized = cap_floor(d, pick.tile);
+    pick.cap = sized;
+    st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "autotune");
+    if (!st) st = raster_ws_ensure(f, raster_ws_size(d.W, d.H, d.views, d.nt, pick.tile, sized));
+    if (st) return st;
+    F->sched = pick;
+    F->sched_cached = false;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        TuneVal v{pick.tile, pick.small_area, (double)sized / ((double)d.views * (d.nt > 0 ? d.nt : 1)),
+                  {F->tune_ms[0], F->tune_ms[1], F->tune_ms[2]}};
+        g_tune[key] = v;
+    }
+    return VCL_OK;
 }
 
 vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
@@ -563,7 +660,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_clip, 0, sizeof(float) * V * d.nv * 4, s), "clear"));
     if (npyr > n0) TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_pyr + n0, 0, sizeof(float) * (npyr - n0), s), "clear"));
     TRY(vcl_project_fwd(ctx, f->mvp, V, f->pos, d.nv, 4, f->clip, s));
-    TRY(raster_fwd_ws(ctx, F->raster_ws, F->tile, F->cap, f->clip, d.nv, f->tri, d.nt, W, H, V, f->rast, f->db, s));
+    TRY(raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H, V, f->rast, f->db, s));
     ShadeIn a;
     a.rast = (const float4*)f->rast; a.db = (const float4*)f->db; a.uvattr = f->uvattr; a.tri = f->tri;
     a.nt = d.nt; a.nv = d.nv; a.pyr = f->pyr; a.rot = f->rot; a.nrm = f->nrmattr; a.pvinv = f->pvinv;
@@ -579,7 +676,6 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     TRY(aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
                      d.learn_pos ? f->g_clip : nullptr, s));
     const bool lobes = d.learn_lobes && d.K;
-    const int nacc = 4 + 4 + 1;
     // the lobe gradients run beside the per-pixel backward on a forked stream
     if (lobes) {
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->fork, s), "fork"));
@@ -644,6 +740,34 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
 
 }  // namespace
 
+// Captures the job's step into F->graph_def (once per mode) on `s`, which
+// must be a stream that can be captured (not the legacy default stream).
+vcl_status fit_fused_graph(vcl_fit* f, cudaStream_t s, cudaGraph_t* out) {
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(f->d.C == 4, "the fused strategy needs C = 4 channels (got %d)", f->d.C);
+    VCL_REQUIRE(s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread,
+                "graph capture needs a created stream");
+    vcl_status st = fused_init(f);
+    if (st) return st;
+    Fused* F = (Fused*)f->fused;
+    if (!F->graph_def || F->graph_mode != ctx->mode) {
+        if (F->graph) { cudaGraphExecDestroy(F->graph); F->graph = nullptr; }
+        if (F->graph_def) { cudaGraphDestroy(F->graph_def); F->graph_def = nullptr; }
+        st = vcl_cuda_check(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        if (st) return st;
+        vcl_status est = enqueue(f, s);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (est) { if (g) cudaGraphDestroy(g); return est; }
+        st = vcl_cuda_check(ctx, e, "graph capture end");
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        F->graph_def = g;
+        F->graph_mode = ctx->mode;
+    }
+    *out = F->graph_def;
+    return VCL_OK;
+}
+
 vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
     vcl_ctx* ctx = f->ctx;
     VCL_REQUIRE(f->d.C == 4, "the fused strategy needs C = 4 channels (got %d)", f->d.C);
@@ -655,22 +779,13 @@ vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
         if (!st) ++f->step_count;
         return st;
     }
-    if (!F->graph || F->graph_stream != s || F->graph_mode != ctx->mode) {
-        if (F->graph) { cudaGraphExecDestroy(F->graph); F->graph = nullptr; }
-        st = vcl_cuda_check(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
-        if (st) return st;
-        vcl_status est = enqueue(f, s);
+    if (!F->graph || F->graph_mode != ctx->mode) {
         cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamEndCapture(s, &g);
-        if (est) { if (g) cudaGraphDestroy(g); return est; }
-        st = vcl_cuda_check(ctx, e, "graph capture end");
-        if (st) { if (g) cudaGraphDestroy(g); return st; }
-        e = cudaGraphInstantiate(&F->graph, g, 0);
-        cudaGraphDestroy(g);
-        st = vcl_cuda_check(ctx, e, "graph instantiate");
+        st = fit_fused_graph(f, s, &g);
+        if (st) return st;
+        if (F->graph) { cudaGraphExecDestroy(F->graph); F->graph = nullptr; }
+        st = vcl_cuda_check(ctx, cudaGraphInstantiate(&F->graph, g, 0), "graph instantiate");
         if (st) { F->graph = nullptr; return st; }
-        F->graph_stream = s;
-        F->graph_mode = ctx->mode;
     }
     st = vcl_cuda_check(ctx, cudaGraphLaunch(F->graph, s), "graph launch");
     if (!st) ++f->step_count;
@@ -697,7 +812,9 @@ void fit_fused_release(vcl_fit* f) {
     Fused* F = (Fused*)f->fused;
     if (!F) return;
     if (F->graph) cudaGraphExecDestroy(F->graph);
+    if (F->graph_def) cudaGraphDestroy(F->graph_def);
     if (F->raster_ws) cudaFree(F->raster_ws);
+    if (F->flags) cudaFree(F->flags);
     if (F->d_step) cudaFree(F->d_step);
     if (F->d_corr) cudaFree(F->d_corr);
     if (F->side) cudaStreamDestroy(F->side);
@@ -722,7 +839,40 @@ vcl_status fit_fused_raster_tuning(vcl_fit* f, int* tile, float* ms3) {
     vcl_status st = fused_init(f);
     if (st) return st;
     Fused* F = (Fused*)f->fused;
-    if (tile) *tile = F->tile;
+    if (tile) *tile = F->sched.tile;
     if (ms3) for (int i = 0; i < 3; ++i) ms3[i] = F->tune_ms[i];
     return VCL_OK;
+}
+
+vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, long long* cap, int* cached,
+                                     long long* overflow) {
+    vcl_status st = fused_init(f);
+    if (st) return st;
+    Fused* F = (Fused*)f->fused;
+    if (tile) *tile = F->sched.tile;
+    if (small_area) *small_area = F->sched.small_area;
+    if (cap) *cap = F->sched.cap;
+    if (cached) *cached = F->sched_cached ? 1 : 0;
+    if (overflow) {
+        int h = 0;
+        st = vcl_cuda_check(f->ctx, cudaMemcpy(&h, F->flags, sizeof(int), cudaMemcpyDeviceToHost), "overflow read");
+        if (st) return st;
+        *overflow = h;
+    }
+    return VCL_OK;
+}
+
+size_t fit_fused_footprint(const vcl_fit_desc& d) {
+    size_t ws = 0;
+    for (int t : {8, 16, 32}) {
+        long long cap = raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
+        size_t b = raster_ws_size(d.W, d.H, d.views, d.nt, t, cap);
+        if (b > ws) ws = b;
+    }
+    return ws + 3 * 256;
+}
+
+void fit_fused_tuning_cache_clear() {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.clear();
 }

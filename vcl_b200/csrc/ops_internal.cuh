@@ -16,6 +16,20 @@ void launch_mip_down(const float* src, float* dst, int w, int h, int C, cudaStre
 // captured graph never points into a workspace that another call regrows).
 long long raster_auto_capacity(long long views, long long nt, int W, int H, int tile);
 size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap);
-vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int tile, long long cap, const float* clip, int nv,
+// Binning schedule: tile edge (8, 16 or 32), bin-list capacity (entries),
+// and the box area (pixels) up to which a triangle skips the bins and is
+// rasterized directly by its setup thread (0 = every triangle is binned).
+struct RasterSched {
+    int tile;
+    long long cap;
+    int small_area;
+};
+int raster_default_small_area();
+// `flags[0]` receives the number of tiles whose bins overflowed.
+vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* flags, const float* clip, int nv,
                          const uint32_t* tri, int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s);
+// Bin-list entries the last raster_fwd_ws on `ws` with schedule `rs` asked
+// for (synchronizes `s`).
+vcl_status raster_bin_demand(vcl_ctx* ctx, void* ws, const RasterSched& rs, int W, int H, int views, int nt,
+                             cudaStream_t s, long long* demand);
 int raster_fwd_launches();

@@ -48,7 +48,8 @@ struct __align__(16) RTri {
 };
 
 constexpr int CHUNK = 128;
-constexpr int SMALL_AREA = 256;   // box pixels up to which a triangle is rasterized by its setup thread
+// default box area (pixels) up to which a triangle is rasterized by its setup thread
+constexpr int SMALL_AREA = 256;
 constexpr unsigned long long KEY_NONE = ~0ull;
 
 // Order-preserving 64-bit key: depth bits (monotone map of the float, -0
@@ -63,7 +64,7 @@ DEV float key_depth(unsigned long long k) {
     u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
     return __uint_as_float(u);
 }
-DEV bool is_small(int4 b) { return (long long)(b.y - b.x + 1) * (b.w - b.z + 1) <= SMALL_AREA; }
+DEV bool is_small(int4 b, int small_area) { return (long long)(b.y - b.x + 1) * (b.w - b.z + 1) <= small_area; }
 
 // Pixel-centre NDC coordinate (2p+1-W)/W: exact numerator, one rounding.
 DEV float ndc(int p, int W) { return dvd((float)(2 * p + 1 - W), (float)W); }
@@ -133,7 +134,7 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
 
 __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W, int H,
                         int views, int tile, int tiles_x, int ntiles, RTri* __restrict__ setup, int* __restrict__ count,
-                        int* __restrict__ flags, unsigned long long* __restrict__ keys) {
+                        int* __restrict__ flags, unsigned long long* __restrict__ keys, int small_area) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
@@ -149,7 +150,7 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
     }
     setup[gid] = r;
     if (r.box.x > r.box.y || r.box.z > r.box.w) return;
-    if (is_small(r.box)) {
+    if (is_small(r.box, small_area)) {
         unsigned long long* kv = keys + (size_t)view * W * H;
         for (int py = r.box.z; py <= r.box.w; ++py) {
             const float sy = ndc(py, H);
@@ -196,12 +197,13 @@ __global__ void k_scan(const int* __restrict__ in, int* __restrict__ out, int n)
 }
 
 __global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int tile, int tiles_x, int ntiles,
-                       const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list, long long cap) {
+                       const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list, long long cap,
+                       int small_area) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
     int4 box = setup[gid].box;
-    if (box.x > box.y || box.z > box.w || is_small(box)) return;
+    if (box.x > box.y || box.z > box.w || is_small(box, small_area)) return;
     int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
@@ -241,7 +243,8 @@ template <int T>
 __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, const int* __restrict__ count,
                                                 const int* __restrict__ offset, const int* __restrict__ list,
                                                 long long cap, int nt, int W, int H, int tiles_x, int ntiles,
-                                                unsigned long long* __restrict__ keys, int* __restrict__ flags) {
+                                                unsigned long long* __restrict__ keys, int* __restrict__ flags,
+                                                int small_area) {
     __shared__ RTri s_tri[CHUNK];
     __shared__ int s_id[CHUNK];
     const int view = blockIdx.y, tile_id = blockIdx.x;
@@ -265,7 +268,7 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
             s_id[tid] = t;
             s_tri[tid] = vs[t];
             // in the all-triangles fallback the small ones are done already
-            if (overflow && is_small(s_tri[tid].box)) s_tri[tid].box = make_int4(1, 0, 1, 0);
+            if (overflow && is_small(s_tri[tid].box, small_area)) s_tri[tid].box = make_int4(1, 0, 1, 0);
         }
         __syncthreads();
         const int m = min(CH, n_iter - i0);
@@ -412,8 +415,13 @@ size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap) 
 
 int raster_fwd_launches() { return 5; }
 
-vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const float* clip, int nv, const uint32_t* tri,
-                         int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s) {
+int raster_default_small_area() { return SMALL_AREA; }
+
+vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* flags, const float* clip, int nv,
+                         const uint32_t* tri, int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s) {
+    const int T = rs.tile;
+    const long long cap = rs.cap;
+    const int sa = rs.small_area;
     const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
     const long long ntiles_view = (long long)tiles_x * tiles_y;
     const long long ntiles = ntiles_view * views;
@@ -425,31 +433,46 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, int T, long long cap, const flo
     if (st) return st;
     st = vcl_cuda_check(ctx, cudaMemsetAsync(w.cursor, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
-    st = vcl_cuda_check(ctx, cudaMemsetAsync(ctx->dev_flags, 0, sizeof(int), s), "raster memset");
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(flags, 0, sizeof(int), s), "raster memset");
     if (st) return st;
     long long work = (long long)views * nt;
     if (work > 0) {
         k_setup<<<vcl_blocks(work, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
-                                                       (int)ntiles_view, w.setup, w.count, ctx->dev_flags, w.keys);
+                                                       (int)ntiles_view, w.setup, w.count, flags, w.keys, sa);
     }
     k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
     if (work > 0) {
         k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, T, tiles_x, (int)ntiles_view, w.offset,
-                                                      w.cursor, w.list, cap);
+                                                      w.cursor, w.list, cap, sa);
     }
     dim3 grid((unsigned)ntiles_view, (unsigned)views);
     if (T == 8)
         k_fine<8><<<grid, dim3(8, 8), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                             (int)ntiles_view, w.keys, ctx->dev_flags);
+                                             (int)ntiles_view, w.keys, flags, sa);
     else if (T == 16)
         k_fine<16><<<grid, dim3(16, 16), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, w.keys, ctx->dev_flags);
+                                               (int)ntiles_view, w.keys, flags, sa);
     else
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, w.keys, ctx->dev_flags);
+                                               (int)ntiles_view, w.keys, flags, sa);
     k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, (const float4*)clip, nv, tri,
                                                      (float4*)rast, (float4*)db);
     return vcl_launch_check(ctx, "rasterize_fwd");
+}
+
+vcl_status raster_bin_demand(vcl_ctx* ctx, void* ws, const RasterSched& rs, int W, int H, int views, int nt,
+                             cudaStream_t s, long long* demand) {
+    const int T = rs.tile;
+    const long long ntiles = (long long)((W + T - 1) / T) * ((H + T - 1) / T) * views;
+    RasterWS w = carve(ws, (long long)W * H * views, views, nt, ntiles, rs.cap);
+    int last[2] = {0, 0};
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(&last[0], w.offset + ntiles - 1, sizeof(int),
+                                                        cudaMemcpyDeviceToHost, s), "bin demand");
+    if (!st) st = vcl_cuda_check(ctx, cudaMemcpyAsync(&last[1], w.count + ntiles - 1, sizeof(int),
+                                                      cudaMemcpyDeviceToHost, s), "bin demand");
+    if (!st) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "bin demand");
+    if (!st) *demand = (long long)last[0] + last[1];
+    return st;
 }
 
 extern "C" {
@@ -486,7 +509,8 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity_(views, nt, W, H, T);
     vcl_status st = vcl_ws_reserve(ctx, ws_bytes((long long)W * H * views, views, nt, ntiles, cap));
     if (st) return st;
-    return raster_fwd_ws(ctx, ctx->ws, T, cap, clip, nv, tri, nt, W, H, views, rast, db, s);
+    return raster_fwd_ws(ctx, ctx->ws, RasterSched{T, cap, SMALL_AREA}, ctx->dev_flags, clip, nv, tri, nt, W, H, views,
+                         rast, db, s);
 }
 
 VCL_API vcl_status vcl_rasterize_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W, int H,

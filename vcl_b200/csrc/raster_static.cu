@@ -106,7 +106,8 @@ VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int
     void* scratch = nullptr;
     vcl_status st = scratch_address(ctx, &scratch);
     if (st) return st;
-    return raster_fwd_ws(ctx, scratch, T, cap, clip, nv, tri, nt, W, H, views, rast, db, (cudaStream_t)stream);
+    return raster_fwd_ws(ctx, scratch, RasterSched{T, cap, raster_default_small_area()}, ctx->dev_flags, clip, nv, tri,
+                         nt, W, H, views, rast, db, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -14,6 +14,7 @@ Conventions shared with the kernels:
 """
 from __future__ import annotations
 
+import functools
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -25,6 +26,12 @@ ZFAR = 10.0
 # ----------------------------------------------------------------- meshes
 def icosphere(subdiv: int):
     """Unit icosphere: 10*4^s + 2 vertices, 20*4^s triangles."""
+    v, f = _icosphere(subdiv)
+    return v.copy(), f.copy()
+
+
+@functools.lru_cache(maxsize=None)
+def _icosphere(subdiv: int):
     t = (1.0 + 5.0 ** 0.5) / 2.0
     verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
              (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -238,6 +245,32 @@ def config2(seed=0, views=8):
     8 views at 1024^2, 2048^2 texture (12 levels), 32 lobes."""
     return make_scene(f"uvs256x128-1024x{views}-tex2048-K32", mesh=("uv", 256, 128), W=1024, H=1024,
                       views=views, tex=2048, K=32, dist=(2.5, 4.0), disp=0.02, seed=seed, iters=200)
+
+
+CONFIG3_RES = (128, 256, 512, 1024)
+CONFIG3_TEX = (256, 512, 1024, 2048)
+
+
+def config3_scene(seed, index):
+    """One scene of the uneven batched mix: icosphere whose triangle count is
+    drawn log-uniform in [1k, 200k] (subdivision 3..6 nearest in log scale),
+    N(0, 0.01) displacement, resolution from {128..1024}^2, 1-16 views,
+    texture from {256..2048}^2 with a full mip chain, 8-32 lobes."""
+    rng = np.random.default_rng([seed, index])
+    T = float(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+    subdiv = int(np.clip(np.floor(np.log(T / 20.0) / np.log(4.0) + 0.5), 3, 6))
+    res = int(rng.choice(CONFIG3_RES))
+    views = int(rng.integers(1, 17))
+    tex = int(rng.choice(CONFIG3_TEX))
+    K = int(rng.integers(8, 33))
+    sub_seed = int(rng.integers(0, 2 ** 31 - 1))
+    return make_scene(f"mix{index}-ico{subdiv}-{res}x{views}-tex{tex}-K{K}", mesh=("ico", subdiv), W=res, H=res,
+                      views=views, tex=tex, K=K, dist=(2.5, 4.0), disp=0.01, seed=sub_seed, iters=100)
+
+
+def config3(seed=0, n=64):
+    """The batched uneven-scene workload: n scenes from config3_scene."""
+    return [config3_scene(seed, i) for i in range(n)]
 
 
 def config5(seed=0):
