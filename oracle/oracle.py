@@ -1,9 +1,11 @@
 """ctypes bindings for the CPU checker.  TEST INFRASTRUCTURE ONLY.
 
-Two libraries with the same function signatures:
+Three libraries with the same function signatures:
 
 * ``liborc.so`` -- the C restatement in ``vcl_oracle.c`` (always available;
   built from source on first use if missing);
+* ``liborc64.so`` -- the same restatement with float replaced by double
+  (``vcl_oracle64.c``), for the finite-difference gradient checks;
 * ``_ref/libvclref.so`` -- the reference's own kernel sources compiled as host
   C++ by ``make -C oracle ref`` (available where the reference sources were
   present at build time).
@@ -61,16 +63,20 @@ def _build_orc():
 
 
 class _Lib:
-    def __init__(self, path, prefix):
+    def __init__(self, path, prefix, real=np.float32):
         self.lib = ctypes.CDLL(path)
         self.prefix = prefix
         self.path = path
+        self.dtype = real
+        kind = dict(_KIND)
+        if real == np.float64:
+            kind["f"] = _d          # float scalars are double in the double build
         for name, kinds in SIGS.items():
             fn = getattr(self.lib, prefix + name, None)
             if fn is None:
                 continue
-            fn.argtypes = [_KIND[k] for k in kinds]
-            fn.restype = _RESTYPE.get(name, None)
+            fn.argtypes = [kind[k] for k in kinds]
+            fn.restype = _d if (real == np.float64 and name in _RESTYPE) else _RESTYPE.get(name, None)
 
     def has(self, name):
         return hasattr(self.lib, self.prefix + name)
@@ -105,6 +111,21 @@ def orc():
             _build_orc()
         _orc = _Lib(ORC_PATH, "orc_")
     return _orc
+
+
+_orc64 = None
+
+
+def orc64():
+    """The C restatement compiled in double precision (arrays and scalars
+    that the header declares float are double), for finite differences."""
+    global _orc64
+    if _orc64 is None:
+        path = os.path.join(HERE, "liborc64.so")
+        if not os.path.exists(path):
+            _build_orc()
+        _orc64 = _Lib(path, "orc_", real=np.float64)
+    return _orc64
 
 
 def ref():

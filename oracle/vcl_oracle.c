@@ -623,7 +623,7 @@ static void aa_edge_fwd(int C, const float* in, float* out, size_t pidx, size_t 
     }
 }
 
-typedef struct { f2 v[3]; float iw[3]; uint32_t id[3]; } aa_tri;
+typedef struct { f2 v[3]; f2 ndc[3]; float iw[3]; uint32_t id[3]; } aa_tri;
 
 /* antialias.cu:37-55 and :240-257: the triangle of pixel `pidx` in
  * pixel units relative to f. Returns 0 when the pixel is background. */
@@ -635,6 +635,7 @@ static int aa_fetch(const float* proj, const uint32_t* tri, const float* rast, s
         t->id[k] = vi;
         f2 v = F2(proj[vi * 4], proj[vi * 4 + 1]);
         t->iw[k] = 1.f / proj[vi * 4 + 3];
+        t->ndc[k] = F2(v.x * t->iw[k], v.y * t->iw[k]);
         t->v[k] = F2((v.x * t->iw[k] + 1.f) * s.x - f.x, (v.y * t->iw[k] + 1.f) * s.y - f.y);
     }
     return 1;
@@ -685,9 +686,13 @@ void orc_antialias_fwd(int W, int H, int views, int C, const float* clip, int nv
     }
 }
 
-/* antialias.cu:196-240 */
-static void aa_edge_bwd(int C, const float* in, const float* g_out, float* g_in, float* g_clip,
-                        size_t pidx, size_t oidx, f2 pa, f2 pb, uint32_t ia_, uint32_t ib_,
+/* antialias.cu:196-240.  The w gradient: a vertex's pixel position is
+ * (x/w + 1) s - f, so d/dw = -(x/w) s / w and dL/dw = -(dL/dx' . x/w) with
+ * dL/dx' the x,y gradient already scaled by s/w.  The reference multiplies
+ * by the pixel position relative to f instead of x/w (:241-242); exact uses
+ * x/w (`na`, `nb`). */
+static void aa_edge_bwd(int exact, int C, const float* in, const float* g_out, float* g_in, float* g_clip,
+                        size_t pidx, size_t oidx, f2 pa, f2 pb, f2 na, f2 nb, uint32_t ia_, uint32_t ib_,
                         float iwa, float iwb, f2 o, f2 s) {
     float a = cross2(pa, pb);
     float oa = cross2(F2(pa.x - o.x, pa.y - o.y), F2(pb.x - o.x, pb.y - o.y));
@@ -722,8 +727,9 @@ static void aa_edge_bwd(int C, const float* in, const float* g_out, float* g_in,
             da.x *= -pb.x; da.y *= -pb.x; da.x *= r;
             db.x *= pa.x; db.y *= pa.x; db.x *= r;
         }
-        g_clip[ia_ * 4] += da.x; g_clip[ia_ * 4 + 1] += da.y; g_clip[ia_ * 4 + 3] += -(da.x * pa.x + da.y * pa.y);
-        g_clip[ib_ * 4] += db.x; g_clip[ib_ * 4 + 1] += db.y; g_clip[ib_ * 4 + 3] += -(db.x * pb.x + db.y * pb.y);
+        f2 wa = exact ? na : pa, wb = exact ? nb : pb;
+        g_clip[ia_ * 4] += da.x; g_clip[ia_ * 4 + 1] += da.y; g_clip[ia_ * 4 + 3] += -(da.x * wa.x + da.y * wa.y);
+        g_clip[ib_ * 4] += db.x; g_clip[ib_ * 4 + 1] += db.y; g_clip[ib_ * 4 + 3] += -(db.x * wb.x + db.y * wb.y);
     }
 }
 
@@ -731,7 +737,7 @@ static void aa_edge_bwd(int C, const float* in, const float* g_out, float* g_in,
  * (the current pixel's id used for both sides), under which a background
  * current pixel makes the reference fetch triangle -1 out of bounds; that
  * fetch contributes nothing here.  exact uses the neighbour's id, as the
- * forward pass does (:74). */
+ * forward pass does (:74), and the corrected w gradient (aa_edge_bwd). */
 void orc_antialias_bwd(int mode, int W, int H, int views, int C, const float* clip, int nv,
                        const uint32_t* tri, const float* rast, const float* in,
                        const float* g_out, float* g_in, float* g_clip) {
@@ -756,9 +762,11 @@ void orc_antialias_bwd(int mode, int W, int H, int views, int C, const float* cl
                     f2 o = F2(pp > op ? -1.f : 1.f, 0.f);
                     aa_tri t;
                     if (aa_fetch(proj, tri, rast, pp, s, f, &t)) {
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[0], t.v[1], t.id[0], t.id[1], t.iw[0], t.iw[1], o, s);
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[1], t.v[2], t.id[1], t.id[2], t.iw[1], t.iw[2], o, s);
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[2], t.v[0], t.id[2], t.id[0], t.iw[2], t.iw[0], o, s);
+                        for (int k = 0; k < 3; ++k) {
+                            int k2 = (k + 1) % 3;
+                            aa_edge_bwd(mode != 0, C, in, g_out, g_in, gc, pp, op, t.v[k], t.v[k2], t.ndc[k], t.ndc[k2],
+                                        t.id[k], t.id[k2], t.iw[k], t.iw[k2], o, s);
+                        }
                     }
                 }
                 if (tv.y != tr.y) {
@@ -770,9 +778,11 @@ void orc_antialias_bwd(int mode, int W, int H, int views, int C, const float* cl
                     f2 o = F2(0.f, pp > op ? -1.f : 1.f);
                     aa_tri t;
                     if (aa_fetch(proj, tri, rast, pp, s, f, &t)) {
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[0], t.v[1], t.id[0], t.id[1], t.iw[0], t.iw[1], o, s);
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[1], t.v[2], t.id[1], t.id[2], t.iw[1], t.iw[2], o, s);
-                        aa_edge_bwd(C, in, g_out, g_in, gc, pp, op, t.v[2], t.v[0], t.id[2], t.id[0], t.iw[2], t.iw[0], o, s);
+                        for (int k = 0; k < 3; ++k) {
+                            int k2 = (k + 1) % 3;
+                            aa_edge_bwd(mode != 0, C, in, g_out, g_in, gc, pp, op, t.v[k], t.v[k2], t.ndc[k], t.ndc[k2],
+                                        t.id[k], t.id[k2], t.iw[k], t.iw[k2], o, s);
+                        }
                     }
                 }
             }
@@ -922,7 +932,8 @@ void orc_sg_fwd(int W, int H, int views, int C, const float* rast, int K,
 }
 
 /* material.cu:369-438.  Per-lobe gradients (axis, sharpness, amplitude) are
- * sums over all pixels.  compat keeps the reference's specular-lobe
+ * sums over all pixels.  exact also replaces the reference's sharpness
+ * derivative of the lobe lengths (see below).  compat keeps the reference's specular-lobe
  * gradient indexing: sharpness at [lobe] (:436) and amplitude at
  * [pixel*C + channel] (:430; the caller sizes that buffer N*C).  exact
  * writes both per pixel and uses d(specg)/d(spec amplitude) for the
@@ -949,7 +960,11 @@ void orc_sg_bwd(int mode, int W, int H, int views, int C, const float* rast, int
             f3 dsum = add3(diffn, sgn);
             float dl = len3(dsum);
             float il = (float)(1.0 / fmax((double)dl, 1e-6));
-            float dotn = (gs + DIFF_SHARP * dot3(sgn, n)) * il;
+            /* d|v|/ds for v = c*u + s*a is (a.v)/|v|; the reference has
+             * (s + c*(s*a).u)/|v| (material.cu:405,413-414).  exact uses the
+             * derivative, and (u.v)/|v| for the specular sharpness. */
+            f3 ax = ld3(axis, i);
+            float dotn = mode != 0 ? dot3(ax, dsum) * il : (gs + DIFF_SHARP * dot3(sgn, n)) * il;
             float em = expf(dl - DIFF_SHARP - gs), ep = expf(-dl - DIFF_SHARP - gs);
             float dg = (em - ep) * il * DIFF_AMP;
             f3 ddg = mul3s(mul3s(dsum, ((1.f - il) * em + (1.f + il) * ep) * il), il);
@@ -958,8 +973,8 @@ void orc_sg_bwd(int mode, int W, int H, int views, int C, const float* rast, int
             f3 ssum = add3(specn, sgn);
             float sl = len3(ssum);
             il = (float)(1.0 / fmax((double)sl, 1e-6));
-            dotn = (gs + ss * dot3(sgn, p)) * il;
-            float dotp = (gs * dot3(sgn, p) + ss) * il;
+            dotn = mode != 0 ? dot3(ax, ssum) * il : (gs + ss * dot3(sgn, p)) * il;
+            float dotp = mode != 0 ? dot3(p, ssum) * il : (gs * dot3(sgn, p) + ss) * il;
             em = expf(sl - ss - gs); ep = expf(-sl - ss - gs);
             float sgv = (em - ep) * il * sa;
             f3 dsg = mul3s(mul3s(ssum, ((1.f - il) * em + (1.f + il) * ep) * il), il);

@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const fl
 // 32 covered pixels (their shading inputs recomputed from the raster output,
 // reduced to the per-pixel factors every lobe reuses), then each lane walks
 // them for its lobe(s); sums stay in registers until the end.  C = 4.
-template <int NL>
+template <int NL, bool EXACT>
 __global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
                                                   float* __restrict__ g_axis, float* __restrict__ g_sharp,
                                                   float* __restrict__ g_amp) {
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const f
             const SPix4 P = st[j];
 #pragma unroll
             for (int sl = 0; sl < NL; ++sl)
-                if (LL[sl].valid) lobe4_accumulate(LL[sl], P);
+                if (LL[sl].valid) lobe4_accumulate<EXACT>(LL[sl], P);
         }
         __syncwarp();
     }
@@ -688,15 +688,16 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
         long long capg = (long long)ctx->sm_count * 6;
         int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
         size_t lsm = lobes_smem(d.K, lthreads);
-        if (NL <= 1)
-            k_sg_lobes<1><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
-                                                               f->g_sharp, f->g_amp);
-        else if (NL <= 2)
-            k_sg_lobes<2><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
-                                                               f->g_sharp, f->g_amp);
-        else
-            k_sg_lobes<4><<<lgrid, lthreads, lsm, F->side>>>(a, td, (const float4*)f->g_color, Kp, f->g_axis,
-                                                               f->g_sharp, f->g_amp);
+        const float4* gc = (const float4*)f->g_color;
+        if (compat) {
+            if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+            else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+            else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        } else {
+            if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+            else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+            else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        }
         TRY(vcl_launch_check(ctx, "fused lobe gradients"));
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));
     }

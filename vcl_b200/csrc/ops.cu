@@ -316,7 +316,7 @@ __global__ void k_clamp(float* __restrict__ p, long long n, float lo, float hi) 
 }
 
 // ------------------------------------------------------------ antialias
-struct AATri { float2 v[3]; float iw[3]; uint32_t id[3]; };
+struct AATri { float2 v[3]; float2 ndc[3]; float iw[3]; uint32_t id[3]; };
 
 // antialias.cu:37-55 / :240-257.  Screen positions use exactly rounded
 // arithmetic so that the edge decisions match the CPU restatement.
@@ -329,7 +329,8 @@ DEV bool aa_fetch(const float4* __restrict__ proj, int nv, const uint32_t* __res
         float4 c = proj[i[k]];
         t.id[k] = i[k];
         t.iw[k] = __fdiv_rn(1.f, c.w);
-        t.v[k] = make_float2(sub(mul(add(mul(c.x, t.iw[k]), 1.f), s.x), f.x), sub(mul(add(mul(c.y, t.iw[k]), 1.f), s.y), f.y));
+        t.ndc[k] = make_float2(mul(c.x, t.iw[k]), mul(c.y, t.iw[k]));
+        t.v[k] = make_float2(sub(mul(add(t.ndc[k].x, 1.f), s.x), f.x), sub(mul(add(t.ndc[k].y, 1.f), s.y), f.y));
     }
     return true;
 }
@@ -503,8 +504,12 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
                     da.x *= -pb.x; da.y *= -pb.x; da.x *= r;
                     dbv.x *= pa.x; dbv.y *= pa.x; dbv.x *= r;
                 }
-                red_add4(gv + (size_t)P.t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * pa.x + da.y * pa.y));
-                red_add4(gv + (size_t)P.t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * pb.x + dbv.y * pb.y));
+                // w: the reference multiplies by the pixel position relative to
+                // the pixel edge (antialias.cu:241-242); the derivative of
+                // (x/w + 1) s - f w.r.t. w needs x/w (EXACT)
+                const float2 wa = exact ? P.t.ndc[ka] : pa, wb = exact ? P.t.ndc[kb] : pb;
+                red_add4(gv + (size_t)P.t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * wa.x + da.y * wa.y));
+                red_add4(gv + (size_t)P.t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * wb.x + dbv.y * wb.y));
             }
         }
     }

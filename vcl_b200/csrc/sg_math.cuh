@@ -39,18 +39,24 @@ DEV void sg_terms(float3 dn, float3 sn, float3 g, float gs, float ss, float sa, 
     sg = (__expf(l - ss - gs) - __expf(-l - ss - gs)) * il * sa;
 }
 
-// Backward terms of one lobe (material.cu:398-418).
+// Backward terms of one lobe (material.cu:398-418).  The sharpness
+// derivatives need d|v|/ds for v = c*u + s*a (c*u the pixel's diffuse or
+// specular vector, a the lobe axis): (a.v)/|v|.  The reference computes
+// (s + c*(s*a).u)/|v| (material.cu:405,413-414), which equals it only for
+// |a| = 1 and s = 1; COMPAT keeps that, EXACT uses (a.v)/|v| and, for the
+// specular sharpness, (u.v)/|v|.  `ax` is the raw lobe axis (EXACT only).
 struct SGB {
     float dg, sgv, ddgs, dsgs, dsgss, sil_e;   // sil_e = (e- - e+) / max(l,1e-6) of the specular term
     float3 ddg, dsg;
 };
 
-DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa) {
+DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa,
+                     bool exact, float3 ax) {
     SGB r;
     float3 dsum = dn + sgn;
     float dl, il;
     sg_len(dot3(dsum, dsum), dl, il);
-    float dotn = (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
+    float dotn = exact ? dot3(ax, dsum) * il : (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
     float em = __expf(dl - SG_DIFF_SHARP - gs), ep = __expf(-dl - SG_DIFF_SHARP - gs);
     r.dg = (em - ep) * il * SG_DIFF_AMP;
     r.ddg = dsum * (((1.f - il) * em + (1.f + il) * ep) * il * il);
@@ -59,8 +65,8 @@ DEV SGB sg_bwd_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, flo
     float sl;
     sg_len(dot3(ssum, ssum), sl, il);
     float sdot = dot3(sgn, pax);
-    dotn = (gs + ss * sdot) * il;
-    float dotp = (gs * sdot + ss) * il;
+    dotn = exact ? dot3(ax, ssum) * il : (gs + ss * sdot) * il;
+    float dotp = exact ? dot3(pax, ssum) * il : (gs * sdot + ss) * il;
     em = __expf(sl - ss - gs); ep = __expf(-sl - ss - gs);
     r.sil_e = (em - ep) * il;
     r.sgv = r.sil_e * sa;
@@ -77,12 +83,13 @@ struct SGL {
     float3 ddg, dsg;
 };
 
-DEV SGL sg_lobe_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa) {
+DEV SGL sg_lobe_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, float gs, float ss, float sa,
+                      bool exact, float3 ax) {
     SGL r;
     float3 dsum = dn + sgn;
     float dl, il;
     sg_len(dot3(dsum, dsum), dl, il);
-    float dotn = (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
+    float dotn = exact ? dot3(ax, dsum) * il : (gs + SG_DIFF_SHARP * dot3(sgn, n)) * il;
     float em = __expf(dl - SG_DIFF_SHARP - gs), ep = __expf(-dl - SG_DIFF_SHARP - gs);
     r.dg = (em - ep) * il * SG_DIFF_AMP;
     float ilm = 1.f - il, ilp = 1.f + il;
@@ -91,7 +98,7 @@ DEV SGL sg_lobe_terms(float3 n, float3 dn, float3 pax, float3 sn, float3 sgn, fl
     float3 ssum = sn + sgn;
     float sl;
     sg_len(dot3(ssum, ssum), sl, il);
-    dotn = (gs + ss * dot3(sgn, pax)) * il;
+    dotn = exact ? dot3(ax, ssum) * il : (gs + ss * dot3(sgn, pax)) * il;
     em = __expf(sl - ss - gs); ep = __expf(-sl - ss - gs);
     r.sgv = (em - ep) * il * sa;
     ilm = 1.f - il; ilp = 1.f + il;
@@ -109,11 +116,13 @@ DEV float warp_sum(float v) {
 DEV bool fin3(float3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
 DEV float finite_or0(float v) { return isfinite(v) ? v : 0.f; }
 
-// Lobes staged in shared memory: axis pre-multiplied by sharpness.
+// Lobes staged in shared memory: axis pre-multiplied by sharpness; the raw
+// axis stays in global memory (read only by the EXACT sharpness derivative).
 struct SGLobes {
     const float* ax;   // [K][3] axis * sharpness
     const float* sh;   // [K]
     const float* am;   // [K][C]
+    const float* raw;  // [K][3] axis (global)
 };
 
 DEV SGLobes sg_stage_lobes(float* sm, int K, int C, const float* axis, const float* sharp, const float* amp) {
@@ -126,7 +135,7 @@ DEV SGLobes sg_stage_lobes(float* sm, int K, int C, const float* axis, const flo
         s_ax[3 * i] = axis[3 * i] * s; s_ax[3 * i + 1] = axis[3 * i + 1] * s; s_ax[3 * i + 2] = axis[3 * i + 2] * s;
     }
     for (int i = threadIdx.x; i < K * C; i += blockDim.x) s_am[i] = amp[i];
-    return SGLobes{s_ax, s_sh, s_am};
+    return SGLobes{s_ax, s_sh, s_am, axis};
 }
 
 // Diffuse and specular environment sums of one pixel with the reference's
@@ -214,7 +223,8 @@ DEV void sg_bwd_pixel_slow(const SGLobes& L, int K, int C, int exact, SGPix& q, 
     for (int i = 0; i < K; ++i) {
         float gs = L.sh[i];
         float3 sgn = f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]);
-        SGB t = sg_bwd_terms(q.n, dn, q.pax, sn, sgn, gs, q.ss, q.sa);
+        const float3 ax = exact ? f3(L.raw[3 * i], L.raw[3 * i + 1], L.raw[3 * i + 2]) : f3(0.f, 0.f, 0.f);
+        SGB t = sg_bwd_terms(q.n, dn, q.pax, sn, sgn, gs, q.ss, q.sa, exact, ax);
         float sum = 0.f, sum_sa = 0.f;
         for (int k = 0; k < Cn; ++k) {
             float a = L.am[i * C + k], g = q.go[k];
@@ -255,6 +265,7 @@ DEV void sg_bwd_block(const SGLobes& L, int K, int C, int exact, SGPix (&q)[P], 
     for (int i = 0; i < K; ++i) {
         const float gs = L.sh[i];
         const float3 sgn = f3(L.ax[3 * i], L.ax[3 * i + 1], L.ax[3 * i + 2]);
+        const float3 ax = exact ? f3(L.raw[3 * i], L.raw[3 * i + 1], L.raw[3 * i + 2]) : f3(0.f, 0.f, 0.f);
         float c_ax0 = 0.f, c_ax1 = 0.f, c_ax2 = 0.f, c_sh = 0.f, c_ssh = 0.f;
         float c_am[SG_CMAX];
 #pragma unroll
@@ -262,7 +273,7 @@ DEV void sg_bwd_block(const SGLobes& L, int K, int C, int exact, SGPix (&q)[P], 
 #pragma unroll
         for (int j = 0; j < P; ++j) {
             if (!live[j]) continue;
-            SGB t = sg_bwd_terms(q[j].n, dn[j], q[j].pax, sn[j], sgn, gs, q[j].ss, q[j].sa);
+            SGB t = sg_bwd_terms(q[j].n, dn[j], q[j].pax, sn[j], sgn, gs, q[j].ss, q[j].sa, exact, ax);
             float sum = 0.f, sumd = 0.f, sum_sa = 0.f;
 #pragma unroll
             for (int k = 0; k < SG_CMAX; ++k) {
@@ -348,6 +359,7 @@ struct LaneLobes {
     bool valid[NL];
     float gs[NL];
     float3 sgn[NL];
+    float3 ax[NL];     // raw axis (EXACT sharpness derivative)
     float a[NL][CC ? CC : SG_CMAX];
     float acc_ax[NL][3], acc_sh[NL], acc_ssh[NL];
     float acc_am[NL][CC ? CC : SG_CMAX];
@@ -365,6 +377,7 @@ DEV void lane_lobes_load(LaneLobes<NL, CC>& LL, int li, int Kp, int K, int C, co
         float gs = K ? sharp[ii] : 0.f;
         LL.gs[s] = gs;
         LL.sgn[s] = K ? f3(axis[3 * ii] * gs, axis[3 * ii + 1] * gs, axis[3 * ii + 2] * gs) : f3(0.f, 0.f, 0.f);
+        LL.ax[s] = K ? f3(axis[3 * ii], axis[3 * ii + 1], axis[3 * ii + 2]) : f3(0.f, 0.f, 0.f);
 #pragma unroll
         for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) LL.a[s][k] = (k < Cn && K) ? amp[ii * C + k] : 0.f;
         LL.acc_ax[s][0] = LL.acc_ax[s][1] = LL.acc_ax[s][2] = 0.f;
@@ -407,7 +420,7 @@ DEV void sg_bwd_lanes(LaneLobes<NL, CC>& LL, int C, int exact, const SPix* st, S
 #pragma unroll
             for (int s = 0; s < NL; ++s) {
                 if (!LL.valid[s]) continue;
-                SGL t = sg_lobe_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa);
+                SGL t = sg_lobe_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa, exact, LL.ax[s]);
                 float sum = 0.f, sumd = 0.f;
 #pragma unroll
                 for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
@@ -440,7 +453,7 @@ DEV void sg_bwd_lanes(LaneLobes<NL, CC>& LL, int C, int exact, const SPix* st, S
 #pragma unroll
             for (int s = 0; s < NL; ++s) {
                 if (!LL.valid[s]) continue;
-                SGB t = sg_bwd_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa);
+                SGB t = sg_bwd_terms(n, dn, pax, sn, LL.sgn[s], LL.gs[s], ss, sa, exact, LL.ax[s]);
                 float sum = 0.f, sumd = 0.f, sum_sa = 0.f;
 #pragma unroll
                 for (int k = 0; k < (CC ? CC : SG_CMAX); ++k) {
@@ -615,6 +628,7 @@ DEV SPix4 spix4(float3 n, float3 pax, float ss, float sa, float4 dfs, float4 go)
 struct Lobe4 {
     bool valid;
     float3 sgn;
+    float3 a0;                 // raw axis (EXACT sharpness derivative)
     float gs, gsl, cdl, agA;   // sharpness, s*log2e, (2.133 + s)*log2e, 2.34*s
     float4 a;
     float3 ax;
@@ -631,6 +645,7 @@ DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* shar
     L.cdl = (SG_DIFF_SHARP + s) * SG_L2E;
     L.agA = SG_DIFF_AMP * s;
     L.sgn = K ? f3(axis[3 * ii] * s, axis[3 * ii + 1] * s, axis[3 * ii + 2] * s) : f3(0.f, 0.f, 0.f);
+    L.a0 = K ? f3(axis[3 * ii], axis[3 * ii + 1], axis[3 * ii + 2]) : f3(0.f, 0.f, 0.f);
     L.a = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
     L.ax = f3(0.f, 0.f, 0.f);
     L.sh = 0.f;
@@ -640,6 +655,7 @@ DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* shar
 // Gradient contributions of one pixel to one lobe (material.cu:398-433),
 // rearranged: d(axis) = dsum * (A s sumd sd) + ssum * (s sum sa sds) with the
 // scalar factors sd, sds in place of the vectors ddg, dsg.
+template <bool EXACT>
 DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
     const float3 dn = f3(P.a.x, P.a.y, P.a.z), sn = f3(P.b.x, P.b.y, P.b.z);
     const float sa = P.b.w;
@@ -647,7 +663,7 @@ DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
     const float3 dsum = dn + L.sgn;
     float dl, il;
     sg_len(dot3(dsum, dsum), dl, il);
-    const float dotn = (L.gs + dot3(L.sgn, dn)) * il;
+    const float dotn = EXACT ? dot3(L.a0, dsum) * il : (L.gs + dot3(L.sgn, dn)) * il;
     float x = dl * SG_L2E;
     float em = ex2_fast(x - L.cdl), ep = ex2_fast(-x - L.cdl);
     float ilm = 1.f - il, ilp = 1.f + il;
@@ -658,7 +674,7 @@ DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
     const float3 ssum = sn + L.sgn;
     float sl;
     sg_len(dot3(ssum, ssum), sl, il);
-    const float dots = (L.gs + dot3(L.sgn, sn)) * il;
+    const float dots = EXACT ? dot3(L.a0, ssum) * il : (L.gs + dot3(L.sgn, sn)) * il;
     x = sl * SG_L2E;
     const float c = P.c.x + L.gsl;
     em = ex2_fast(x - c); ep = ex2_fast(-x - c);
