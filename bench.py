@@ -142,7 +142,7 @@ def stage_bytes(S, ncov):
 # ------------------------------------------------------------------ vcl arm
 def run_vcl(args, rank, world):
     import torch
-    from vcl_b200 import capi
+    from vcl_b200 import capi, replicas
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -184,16 +184,11 @@ def run_vcl(args, rank, world):
         return e0.elapsed_time(e1)
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        replicas.barrier()
         torch.cuda.synchronize()
 
-    def maxr(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    maxr = replicas.max_over_ranks
 
     out = {}
     strategies = [] if args.strategy == "fused" else [("plain", capi.FIT_PLAIN)]
@@ -433,13 +428,12 @@ def main():
     if args.config in ("mix", "serve"):
         return run_mixed(args, rank, world)
     import torch
+    from vcl_b200 import replicas
     if world > 1:
-        import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        replicas.init("nccl", timeout_s=120)
     r = run_vcl(args, rank, world)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish()
     if rank != 0:
         return
     S = r["scene"]
