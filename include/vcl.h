@@ -280,6 +280,9 @@ typedef struct {
     float roughness, ior;
     double lr, beta1, beta2, eps;
     int learn_pos, learn_tex, learn_lobes;
+    /* per-group Adam step sizes (the reference sets each parameter group's
+     * Adam separately, preset_primitives.cpp:103-115); 0 = use `lr` */
+    double lr_pos, lr_tex, lr_lobes;
 } vcl_fit_desc;
 
 /* Execution strategy of vcl_fit_step. */
@@ -294,8 +297,15 @@ VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* fit, int strategy);
 VCL_API vcl_status vcl_fit_set_target(vcl_fit* fit, const float* src, int src_is_device, void* stream);
 /* New cameras for the next iterations (host arrays as in the descriptor). */
 VCL_API vcl_status vcl_fit_set_cameras(vcl_fit* fit, const float* mvp, const float* pvinv, void* stream);
-/* One fit iteration (forward, backward, optimizer).  Asynchronous. */
+/* One fit iteration (forward, backward, optimizer).  Asynchronous.  If a
+ * target was staged, the step first waits for its upload and makes it the
+ * target. */
 VCL_API vcl_status vcl_fit_step(vcl_fit* fit, void* stream);
+/* Uploads the NEXT step's target images from host memory (pinned, for an
+ * asynchronous copy) into a staging buffer on `copy_stream`, so that the
+ * upload overlaps the current step; the next vcl_fit_step consumes it.  One
+ * staged target at a time (VCL_ERR_ARG if the last one was not consumed). */
+VCL_API vcl_status vcl_fit_stage_target(vcl_fit* fit, const float* host_src, void* copy_stream);
 /* Forward only with the current parameters: antialiased image
  * [views][H][W][C] into the device buffer `out`. */
 VCL_API vcl_status vcl_fit_render(vcl_fit* fit, float* out, void* stream);
@@ -324,6 +334,15 @@ VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* fit, int* tile, float* ms_per_
 VCL_API vcl_status vcl_fit_raster_schedule(vcl_fit* fit, int* tile, int* small_area, long long* bin_capacity,
                                            int* from_cache, long long* overflow_tiles);
 VCL_API void vcl_raster_tuning_cache_clear(void);
+/* Average device time (ms per launch) of each fused-step stage on the job's
+ * current state, after at least one fused step: ms[i] for stage i of
+ * vcl_fit_kernel_name(i) ("raster", "shade_fwd", "aa_fwd", "mse", "aa_bwd",
+ * "bwd_pix", "sg_lobes"); one untimed launch, then `reps` timed ones on
+ * `stream`.  Parameters and Adam moments are untouched; the gradient
+ * buffers are cleared (the next step recomputes them).  Synchronizes. */
+VCL_API int vcl_fit_kernel_count(void);
+VCL_API const char* vcl_fit_kernel_name(int i);
+VCL_API vcl_status vcl_fit_time_kernels(vcl_fit* fit, void* stream, int reps, float* ms, int n);
 /* Device bytes a job with this descriptor holds at most (arena plus the
  * fused strategy's raster workspace), for admission control. */
 VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc);

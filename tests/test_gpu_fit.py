@@ -159,3 +159,38 @@ def test_render_is_deterministic_and_switching_strategy_keeps_step_count(ctx):
                 assert np.abs(x - y).max() <= 2 * S.lr * 3
         else:
             assert np.abs(a - b).max() <= 2 * S.lr * 3
+
+
+def test_staged_target_upload_equals_set_target(ctx):
+    """vcl_fit_stage_target (upload on a copy stream, consumed by the next
+    step) gives the same iterations as vcl_fit_set_target before each step."""
+    from vcl_b200 import capi
+    S = _scene()
+    rng = np.random.default_rng(7)
+    targets = [rng.random((S.W * S.H * S.views, S.C)).astype(np.float32) for _ in range(3)]
+    stream, copy = torch.cuda.Stream(), torch.cuda.Stream()
+    res = []
+    for staged in (False, True):
+        fit = capi.Fit(ctx, S, strategy=capi.FIT_FUSED)
+        pinned = [torch.from_numpy(t.reshape(-1)).pin_memory() for t in targets]
+        losses = []
+        if staged:
+            fit.stage_target(pinned[0], copy.cuda_stream)
+        for i in range(3):
+            if not staged:
+                fit.set_target(targets[i], stream.cuda_stream)
+            fit.step(stream.cuda_stream)
+            if staged and i + 1 < 3:
+                fit.stage_target(pinned[i + 1], copy.cuda_stream)
+            losses.append(fit.read_loss(stream.cuda_stream))
+        res.append((losses, fit.read_params(stream.cuda_stream)))
+        if staged:
+            with pytest.raises(capi.VclError):
+                fit.stage_target(pinned[0], copy.cuda_stream)
+                fit.stage_target(pinned[0], copy.cuda_stream)   # the first one was not consumed
+        copy.synchronize()
+        fit.close()
+    (l0, p0), (l1, p1) = res
+    assert np.allclose(l0, l1, rtol=1e-5)
+    for a, b in zip(p0[:2], p1[:2]):
+        assert_adam_close(b, a, S.lr, 3)

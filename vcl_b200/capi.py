@@ -74,6 +74,10 @@ SIGNATURES = {
     "vcl_fit_launches_per_step": (c_int, [P]),
     "vcl_fit_raster_schedule": (c_int, [P, P, P, P, P, P]),
     "vcl_raster_tuning_cache_clear": (None, []),
+    "vcl_fit_stage_target": (c_int, [P, P, P]),
+    "vcl_fit_kernel_count": (c_int, []),
+    "vcl_fit_kernel_name": (c_char_p, [c_int]),
+    "vcl_fit_time_kernels": (c_int, [P, P, c_int, P, c_int]),
     "vcl_batch_create": (c_int, [P, ctypes.POINTER(c_void_p)]),
     "vcl_batch_destroy": (None, [P]),
     "vcl_batch_add": (c_int, [P, P]),
@@ -106,7 +110,8 @@ class FitDesc(ctypes.Structure):
                 ("lobe_axis", c_void_p), ("lobe_sharp", c_void_p), ("lobe_amp", c_void_p), ("mvp", c_void_p),
                 ("pvinv", c_void_p), ("rot", c_void_p), ("roughness", c_float), ("ior", c_float),
                 ("lr", c_double), ("beta1", c_double), ("beta2", c_double), ("eps", c_double),
-                ("learn_pos", c_int), ("learn_tex", c_int), ("learn_lobes", c_int)]
+                ("learn_pos", c_int), ("learn_tex", c_int), ("learn_lobes", c_int),
+                ("lr_pos", c_double), ("lr_tex", c_double), ("lr_lobes", c_double)]
 
 
 class VclError(RuntimeError):
@@ -223,6 +228,8 @@ def fit_desc(S, tex=None, pos=None, lobes=None, learn=(1, 1, 1)):
     d.roughness, d.ior = S.roughness, S.ior
     d.lr, d.beta1, d.beta2, d.eps = S.lr, 0.9, 0.999, 1e-8
     d.learn_pos, d.learn_tex, d.learn_lobes = learn
+    d.lr_pos = getattr(S, "lr_pos", 0.0) or 0.0
+    d.lr_tex = d.lr_lobes = 0.0
     return d, keep
 
 
@@ -269,9 +276,15 @@ class Fit:
         addr = src.ctypes.data if hasattr(src, "ctypes") else _addr(src)
         self._c(self.ctx.lib.vcl_fit_set_target(self.h, addr, int(is_device), stream), "vcl_fit_set_target")
 
+    def stage_target(self, host, copy_stream=None):
+        """Upload the next step's target (host memory; pinned for overlap) on `copy_stream`."""
+        addr = host.ctypes.data if hasattr(host, "ctypes") else _addr(host)
+        self._c(self.ctx.lib.vcl_fit_stage_target(self.h, addr, copy_stream), "vcl_fit_stage_target")
+
     def set_cameras(self, mvp, pvinv, stream=None):
-        self._c(self.ctx.lib.vcl_fit_set_cameras(self.h, mvp.ctypes.data, pvinv.ctypes.data, stream),
-                "vcl_fit_set_cameras")
+        a = mvp.ctypes.data if hasattr(mvp, "ctypes") else _addr(mvp)
+        b = pvinv.ctypes.data if hasattr(pvinv, "ctypes") else _addr(pvinv)
+        self._c(self.ctx.lib.vcl_fit_set_cameras(self.h, a, b, stream), "vcl_fit_set_cameras")
 
     def step(self, stream=None):
         self._c(self.ctx.lib.vcl_fit_step(self.h, stream), "vcl_fit_step")
@@ -305,6 +318,14 @@ class Fit:
         self._c(self.ctx.lib.vcl_fit_read_params(self.h, pos.ctypes.data, tex.ctypes.data, ax.ctypes.data,
                                                  sh.ctypes.data, am.ctypes.data, stream), "vcl_fit_read_params")
         return pos, tex, (ax, sh, am)
+
+    def time_kernels(self, stream=None, reps=5):
+        """{stage name: ms per launch} of the fused step's stages (clears the gradients)."""
+        L = self.ctx.lib
+        n = L.vcl_fit_kernel_count()
+        ms = (ctypes.c_float * n)()
+        self._c(L.vcl_fit_time_kernels(self.h, stream, reps, ms, n), "vcl_fit_time_kernels")
+        return {L.vcl_fit_kernel_name(i).decode(): ms[i] for i in range(n)}
 
     def raster_schedule(self):
         """(tile, direct-raster box area, bin capacity, from cache, overflowed tiles of the last step)."""

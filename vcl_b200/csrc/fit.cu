@@ -115,6 +115,9 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
     vcl_fit* f = new vcl_fit();
     f->ctx = ctx;
     f->d = *desc;
+    if (f->d.lr_pos <= 0) f->d.lr_pos = f->d.lr;
+    if (f->d.lr_tex <= 0) f->d.lr_tex = f->d.lr;
+    if (f->d.lr_lobes <= 0) f->d.lr_lobes = f->d.lr;
     Layout L;
     plan(f->d, nullptr, L);
     cudaError_t e = cudaMalloc(&f->arena, L.total);
@@ -167,6 +170,9 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
 
 VCL_API void vcl_fit_destroy(vcl_fit* f) {
     if (!f) return;
+    if (f->staging) cudaFree(f->staging);
+    if (f->st_full) cudaEventDestroy(f->st_full);
+    if (f->st_free) cudaEventDestroy(f->st_free);
     if (f->arena) cudaFree(f->arena);
     fit_fused_release(f);
     delete f;
@@ -276,9 +282,58 @@ VCL_API vcl_status vcl_fit_raster_schedule(vcl_fit* f, int* tile, int* small_are
 
 VCL_API void vcl_raster_tuning_cache_clear(void) { fit_fused_tuning_cache_clear(); }
 
+VCL_API int vcl_fit_kernel_count(void) { return fit_fused_kernel_count(); }
+VCL_API const char* vcl_fit_kernel_name(int i) { return fit_fused_kernel_name(i); }
+
+VCL_API vcl_status vcl_fit_time_kernels(vcl_fit* f, void* stream, int reps, float* ms, int n) {
+    if (!f) return VCL_ERR_ARG;
+    return fit_fused_time_kernels(f, (cudaStream_t)stream, reps, ms, n);
+}
+
+VCL_API vcl_status vcl_fit_stage_target(vcl_fit* f, const float* host_src, void* copy_stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(host_src, "null target");
+    VCL_REQUIRE(!f->st_pending, "a staged target has not been consumed by a step yet");
+    const size_t bytes = sizeof(float) * (size_t)f->d.W * f->d.H * f->d.views * f->d.C;
+    if (!f->staging) {
+        cudaError_t e = cudaMalloc(&f->staging, bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_full, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_free, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            return vcl_fail(ctx, VCL_ERR_NOMEM, "target staging buffer: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaStream_t cs = (cudaStream_t)copy_stream;
+    // the previous staged target must have been moved out of the buffer
+    if (f->st_used) {
+        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(cs, f->st_free, 0), "staging wait");
+        if (st) return st;
+    }
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->staging, host_src, bytes, cudaMemcpyHostToDevice, cs),
+                                   "target staging copy");
+    if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_full, cs), "staging event");
+    if (!st) f->st_pending = true;
+    return st;
+}
+
 VCL_API vcl_status vcl_fit_step(vcl_fit* f, void* stream) {
     if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
     cudaStream_t s = (cudaStream_t)stream;
+    if (f->st_pending) {
+        // a staged target becomes this step's target: wait for its upload,
+        // move it in on the device, free the staging buffer for the next one
+        const size_t bytes = sizeof(float) * (size_t)f->d.W * f->d.H * f->d.views * f->d.C;
+        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(s, f->st_full, 0), "staging wait");
+        if (!st) st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->target, f->staging, bytes, cudaMemcpyDeviceToDevice, s),
+                                     "staged target");
+        if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_free, s), "staging event");
+        if (st) return st;
+        f->st_pending = false;
+        f->st_used = true;
+    }
     return f->strategy == VCL_FIT_FUSED ? fit_step_fused(f, s) : fit_step_plain(f, s);
 }
 

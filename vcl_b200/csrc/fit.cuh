@@ -21,6 +21,11 @@ struct vcl_fit {
     float* loss;
     // fused-strategy resources
     void* fused = nullptr;
+    // staged target upload (vcl_fit_stage_target): device staging buffer,
+    // "staging filled" / "staging consumed" events, a fill not yet consumed
+    float* staging = nullptr;
+    cudaEvent_t st_full = nullptr, st_free = nullptr;
+    bool st_pending = false, st_used = false;
 };
 
 vcl_status fit_step_plain(vcl_fit* f, cudaStream_t s);
@@ -37,6 +42,9 @@ void fit_fused_tuning_cache_clear();
 // Device bytes the fused strategy adds to a job (raster workspace upper
 // bound and step state).
 size_t fit_fused_footprint(const vcl_fit_desc& d);
+int fit_fused_kernel_count();
+const char* fit_fused_kernel_name(int i);
+vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* ms, int n);
 // The job's fused step as a CUDA graph (captured on `s` the first time; owned
 // by the job, valid until the job is destroyed or the mode changes).
 vcl_status fit_fused_graph(vcl_fit* f, cudaStream_t s, cudaGraph_t* out);

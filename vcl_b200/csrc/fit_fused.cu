@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const fl
 // reduced to the per-pixel factors every lobe reuses), then each lane walks
 // them for its lobe(s); sums stay in registers until the end.  C = 4.
 template <int NL, bool EXACT>
-__global__ void __launch_bounds__(128) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
+__global__ void __launch_bounds__(128, NL == 1 ? 8 : 1) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
                                                   float* __restrict__ g_axis, float* __restrict__ g_sharp,
                                                   float* __restrict__ g_amp) {
     extern __shared__ float sm[];
@@ -366,6 +366,7 @@ DEV float clamp01(float x) { return x < 0.f ? 0.f : x > 1.f ? 1.f : x; }
 struct AdamArgs {
     double b1, b2, lr, eps;
     const double* corr;
+    double lr1;          // k_adam_small: step size of the second group
 };
 
 // TextureGrad::gradSumup (buffer.cu:615-648) folded into level 0, Adam
@@ -467,7 +468,7 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
     else if (i < n0 + n1) { p = p1; g = g1; m = mv1; v = mv1 + n1; j = i - n0; }
     else return;
     float P = p[j], M = m[j], V = v[j];
-    adam_one(P, g[j], M, V, aa.b1, aa.b2, aa.lr, aa.eps, aa.corr[0], aa.corr[1]);
+    adam_one(P, g[j], M, V, aa.b1, aa.b2, i < n0 ? aa.lr : aa.lr1, aa.eps, aa.corr[0], aa.corr[1]);
     p[j] = P; m[j] = M; v[j] = V; g[j] = 0.f;
 }
 
@@ -647,12 +648,68 @@ vcl_status autotune_raster(vcl_fit* f) {
     return VCL_OK;
 }
 
+ShadeIn shade_in(const vcl_fit* f) {
+    const vcl_fit_desc& d = f->d;
+    ShadeIn a;
+    a.rast = (const float4*)f->rast; a.db = (const float4*)f->db; a.uvattr = f->uvattr; a.tri = f->tri;
+    a.nt = d.nt; a.nv = d.nv; a.pyr = f->pyr; a.rot = f->rot; a.nrm = f->nrmattr; a.pvinv = f->pvinv;
+    a.W = d.W; a.H = d.H; a.npix = (long long)d.W * d.H * d.views; a.rough = d.roughness; a.ior = d.ior;
+    a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
+    return a;
+}
+
+// The fused stages, each one launch (shared by the captured step and the
+// per-kernel timing).
+vcl_status stage_shade(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
+    k_shade_fwd<<<vcl_blocks(a.npix, 256), 256, shade_smem(a.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse);
+    return vcl_launch_check(f->ctx, "fused shade");
+}
+
+vcl_status stage_mse(vcl_fit* f, cudaStream_t s) {
+    const long long N = (long long)f->d.W * f->d.H * f->d.views;
+    k_mse_init<<<f->ctx->sm_count * 4, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N,
+                                                    (float4*)f->g_aa, f->loss);
+    return vcl_launch_check(f->ctx, "fused mse");
+}
+
+vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
+    vcl_ctx* ctx = f->ctx;
+    const vcl_fit_desc& d = f->d;
+    const long long N = a.npix;
+    const int compat = ctx->mode == VCL_MODE_COMPAT;
+    const int Kp = sg_lobe_group(d.K);
+    const int NL = (d.K + 31) / 32;
+    const int lthreads = 128;
+    long long chunks = (N + 31) / 32;
+    long long want = (chunks + 3) / 4;
+    long long capg = (long long)ctx->sm_count * (NL == 1 ? 8 : 4);
+    int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
+    size_t lsm = lobes_smem(d.K, lthreads);
+    const float4* gc = (const float4*)f->g_color;
+    if (compat) {
+        if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+    } else {
+        if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+    }
+    return vcl_launch_check(ctx, "fused lobe gradients");
+}
+
+vcl_status stage_bwd_pix(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
+    const vcl_fit_desc& d = f->d;
+    k_bwd_pix<<<vcl_blocks(a.npix, 256), 256, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
+                                                      f->g_pyr, f->clip, f->g_clip, d.learn_tex, d.learn_pos);
+    return vcl_launch_check(f->ctx, "fused backward");
+}
+
 vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     vcl_ctx* ctx = f->ctx;
     Fused* F = (Fused*)f->fused;
     const vcl_fit_desc& d = f->d;
     const int W = d.W, H = d.H, V = d.views;
-    const long long N = (long long)W * H * V;
     const size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, 4, d.levels);
     const size_t n0 = (size_t)d.tex_w * d.tex_h * 4;
     const int compat = ctx->mode == VCL_MODE_COMPAT;
@@ -661,18 +718,11 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     if (npyr > n0) TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_pyr + n0, 0, sizeof(float) * (npyr - n0), s), "clear"));
     TRY(vcl_project_fwd(ctx, f->mvp, V, f->pos, d.nv, 4, f->clip, s));
     TRY(raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H, V, f->rast, f->db, s));
-    ShadeIn a;
-    a.rast = (const float4*)f->rast; a.db = (const float4*)f->db; a.uvattr = f->uvattr; a.tri = f->tri;
-    a.nt = d.nt; a.nv = d.nv; a.pyr = f->pyr; a.rot = f->rot; a.nrm = f->nrmattr; a.pvinv = f->pvinv;
-    a.W = W; a.H = H; a.npix = N; a.rough = d.roughness; a.ior = d.ior;
-    a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
-    TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
-    k_shade_fwd<<<vcl_blocks(N, 256), 256, shade_smem(d.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse);
-    TRY(vcl_launch_check(ctx, "fused shade"));
+    const ShadeIn a = shade_in(f);
+    const TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
+    TRY(stage_shade(f, a, td, s));
     TRY(aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
-    int grid = ctx->sm_count * 4;
-    k_mse_init<<<grid, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N, (float4*)f->g_aa, f->loss);
-    TRY(vcl_launch_check(ctx, "fused mse"));
+    TRY(stage_mse(f, s));
     TRY(aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
                      d.learn_pos ? f->g_clip : nullptr, s));
     const bool lobes = d.learn_lobes && d.K;
@@ -680,35 +730,14 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     if (lobes) {
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->fork, s), "fork"));
         TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(F->side, F->fork, 0), "fork"));
-        const int Kp = sg_lobe_group(d.K);
-        const int NL = (d.K + 31) / 32;
-        const int lthreads = 128;
-        long long chunks = (N + 31) / 32;
-        long long want = (chunks + 3) / 4;
-        long long capg = (long long)ctx->sm_count * 6;
-        int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
-        size_t lsm = lobes_smem(d.K, lthreads);
-        const float4* gc = (const float4*)f->g_color;
-        if (compat) {
-            if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-            else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-            else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        } else {
-            if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-            else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-            else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, F->side>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        }
-        TRY(vcl_launch_check(ctx, "fused lobe gradients"));
+        TRY(stage_lobes(f, a, td, F->side));
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));
     }
-    if (d.learn_tex || d.learn_pos) {
-        k_bwd_pix<<<vcl_blocks(N, 256), 256, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
-                                                     f->g_pyr, f->clip, f->g_clip, d.learn_tex, d.learn_pos);
-        TRY(vcl_launch_check(ctx, "fused backward"));
-    }
+    if (d.learn_tex || d.learn_pos) TRY(stage_bwd_pix(f, a, td, s));
     if (lobes) TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join"));
     if (d.learn_pos) TRY(vcl_project_bwd(ctx, f->mvp, V, f->g_clip, d.nv, 4, f->g_pos, s));
-    AdamArgs aa{d.beta1, d.beta2, d.lr, d.eps, F->d_corr};
+    AdamArgs aa{d.beta1, d.beta2, d.lr_tex, d.eps, F->d_corr, 0.0};
+    AdamArgs ap{d.beta1, d.beta2, d.lr_pos, d.eps, F->d_corr, d.lr_lobes};
     const float wpush = ctx->mode == VCL_MODE_EXACT ? 0.25f : 1.f;
     if (d.learn_tex) {
         const bool tile = d.tex_w % 32 == 0 && d.tex_h % 32 == 0 && d.levels >= 2;
@@ -733,7 +762,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     long long nl = lobes ? (long long)d.K * 8 : 0;
     if (np + nl > 0) {
         k_adam_small<<<vcl_blocks(np + nl, 256), 256, 0, s>>>(f->pos, f->g_pos, f->mv_pos, np, f->lobe, f->g_lobe,
-                                                              f->mv_lobe, nl, aa);
+                                                              f->mv_lobe, nl, ap);
         TRY(vcl_launch_check(ctx, "fused adam"));
     }
     return VCL_OK;
@@ -861,6 +890,70 @@ vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, lon
         *overflow = h;
     }
     return VCL_OK;
+}
+
+const char* const kFusedKernelNames[] = {"raster", "shade_fwd", "aa_fwd", "mse", "aa_bwd", "bwd_pix", "sg_lobes"};
+constexpr int kFusedKernels = 7;
+
+int fit_fused_kernel_count() { return kFusedKernels; }
+const char* fit_fused_kernel_name(int i) { return i >= 0 && i < kFusedKernels ? kFusedKernelNames[i] : nullptr; }
+
+// Average device time of each fused stage: one untimed launch, then `reps`
+// launches between two events on `s`.  Runs on the job's current state (its
+// last step's raster and gradients); the stages that accumulate gradients
+// leave them undefined, so all gradient buffers are cleared at the end and
+// the parameters and Adam moments are untouched.
+vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* ms, int n) {
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(f->fused && f->step_count > 0, "time the kernels after at least one fused step");
+    VCL_REQUIRE(reps > 0 && ms, "bad arguments");
+    Fused* F = (Fused*)f->fused;
+    const vcl_fit_desc& d = f->d;
+    const int W = d.W, H = d.H, V = d.views;
+    const ShadeIn a = shade_in(f);
+    const TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return vcl_fail(ctx, VCL_ERR_CUDA, "timing events");
+    vcl_status st = VCL_OK;
+    for (int k = 0; k < kFusedKernels && k < n && st == VCL_OK; ++k) {
+        auto run = [&]() -> vcl_status {
+            switch (k) {
+                case 0: return raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H,
+                                             V, f->rast, f->db, s);
+                case 1: return stage_shade(f, a, td, s);
+                case 2: return aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s);
+                case 3: return stage_mse(f, s);
+                case 4: return aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
+                                            f->g_color, d.learn_pos ? f->g_clip : nullptr, s);
+                case 5: return stage_bwd_pix(f, a, td, s);
+                default: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;
+            }
+        };
+        st = run();
+        if (st) break;
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps && st == VCL_OK; ++r) st = run();
+        cudaEventRecord(e1, s);
+        if (st) break;
+        cudaEventSynchronize(e1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms[k] = t / reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    const size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, 4, d.levels);
+    auto z = [&](void* p, size_t b) {
+        if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaMemsetAsync(p, 0, b, s), "gradient clear");
+    };
+    z(f->g_pyr, sizeof(float) * npyr);
+    z(f->g_clip, sizeof(float) * (size_t)V * d.nv * 4);
+    z(f->g_pos, sizeof(float) * (size_t)d.nv * 3);
+    z(f->g_lobe, sizeof(float) * (size_t)d.K * 8);
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "kernel timing");
+    return st;
 }
 
 size_t fit_fused_footprint(const vcl_fit_desc& d) {

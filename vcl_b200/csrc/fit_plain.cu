@@ -77,14 +77,14 @@ vcl_status fit_step_plain(vcl_fit* f, cudaStream_t s) {
     const int t = ++f->step_count;
     if (d.learn_tex) {
         TRY(vcl_texture_grad_pushdown(ctx, f->g_pyr, d.tex_w, d.tex_h, C, d.levels, s));
-        TRY(vcl_adam_step(ctx, f->pyr, f->g_pyr, f->mv_tex, f->mv_tex + n0, n0, d.lr, d.beta1, d.beta2, d.eps, t, s));
+        TRY(vcl_adam_step(ctx, f->pyr, f->g_pyr, f->mv_tex, f->mv_tex + n0, n0, d.lr_tex, d.beta1, d.beta2, d.eps, t, s));
         TRY(vcl_clamp(ctx, f->pyr, n0, 0.f, 1.f, s));
         TRY(vcl_texture_build_mips(ctx, f->pyr, d.tex_w, d.tex_h, C, d.levels, s));
     }
     if (d.learn_pos)
-        TRY(vcl_adam_step(ctx, f->pos, f->g_pos, f->mv_pos, f->mv_pos + (size_t)d.nv * 3, (size_t)d.nv * 3, d.lr,
+        TRY(vcl_adam_step(ctx, f->pos, f->g_pos, f->mv_pos, f->mv_pos + (size_t)d.nv * 3, (size_t)d.nv * 3, d.lr_pos,
                           d.beta1, d.beta2, d.eps, t, s));
     if (lobes)
-        TRY(vcl_adam_step(ctx, f->lobe, f->g_lobe, f->mv_lobe, f->mv_lobe + nl, nl, d.lr, d.beta1, d.beta2, d.eps, t, s));
+        TRY(vcl_adam_step(ctx, f->lobe, f->g_lobe, f->mv_lobe, f->mv_lobe + nl, nl, d.lr_lobes, d.beta1, d.beta2, d.eps, t, s));
     return VCL_OK;
 }

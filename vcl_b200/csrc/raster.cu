@@ -95,6 +95,30 @@ DEV bool pixel_test(const float4& a, const float4& b, const float4& k, const flo
     return zw >= -1.f && zw <= 1.f && zw < 1.f;
 }
 
+// Conservative triangle/tile test: false only when, for some edge, every
+// pixel centre of the tile (clipped to the triangle's box) lies outside by
+// more than a rounding margin, so no pixel of the tile can be covered.  The
+// edge functions are linear in (sx, sy), so their maximum over the tile is
+// at a corner.
+DEV bool tile_overlaps(const RTri& r, int tx, int ty, int T, int W, int H) {
+    const int x0 = max(tx * T, r.box.x), x1 = min(tx * T + T - 1, r.box.y);
+    const int y0 = max(ty * T, r.box.z), y1 = min(ty * T + T - 1, r.box.w);
+    if (x0 > x1 || y0 > y1) return false;
+    const float sx0 = ndc(x0, W), sx1 = ndc(x1, W), sy0 = ndc(y0, H), sy1 = ndc(y1, H);
+    const float sg = r.a.w;
+    const float ea[3] = {r.a.x, r.a.y, r.a.z}, eb[3] = {r.b.x, r.b.y, r.b.z}, ek[3] = {r.k.x, r.k.y, r.k.z};
+    // explicitly rounded operations: the count pass and the emit pass must
+    // reach the same decision for every tile
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float a = mul(sg, ea[i]), b = mul(sg, eb[i]), k = mul(sg, ek[i]);
+        const float mx = add(add(k, fmaxf(mul(a, sx0), mul(a, sx1))), fmaxf(mul(b, sy0), mul(b, sy1)));
+        const float margin = mul(1e-5f, add(add(fabsf(a), fabsf(b)), fabsf(k)));
+        if (mx < -margin) return false;
+    }
+    return true;
+}
+
 DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool& valid) {
     float x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y, x2 = c2.x, y2 = c2.y;
     float w0 = c0.w, w1 = c1.w, w2 = c2.w;
@@ -165,7 +189,8 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
     int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
     int* cnt = count + (size_t)view * ntiles;
     for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) atomicAdd(&cnt[ty * tiles_x + tx], 1);
+        for (int tx = tx0; tx <= tx1; ++tx)
+            if (tile_overlaps(r, tx, ty, tile, W, H)) atomicAdd(&cnt[ty * tiles_x + tx], 1);
 }
 
 // Exclusive scan of n ints by one CTA of 1024 threads (chunked).
@@ -196,17 +221,19 @@ __global__ void k_scan(const int* __restrict__ in, int* __restrict__ out, int n)
     }
 }
 
-__global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int tile, int tiles_x, int ntiles,
-                       const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list, long long cap,
-                       int small_area) {
+__global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int W, int H, int tile, int tiles_x,
+                       int ntiles, const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list,
+                       long long cap, int small_area) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
-    int4 box = setup[gid].box;
+    const RTri r = setup[gid];
+    const int4 box = r.box;
     if (box.x > box.y || box.z > box.w || is_small(box, small_area)) return;
     int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
+            if (!tile_overlaps(r, tx, ty, tile, W, H)) continue;
             size_t ti = (size_t)view * ntiles + ty * tiles_x + tx;
             int slot = atomicAdd(&cursor[ti], 1);
             long long p = (long long)offset[ti] + slot;
@@ -265,6 +292,7 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
     for (int i0 = 0; i0 < n_iter; i0 += CH) {
         if (tid < CH && i0 + tid < n_iter) {
             int t = overflow ? i0 + tid : list[off + i0 + tid];
+            if ((unsigned)t >= (unsigned)nt) t = 0;   // never taken: every counted slot is emitted
             s_id[tid] = t;
             s_tri[tid] = vs[t];
             // in the all-triangles fallback the small ones are done already
@@ -442,8 +470,8 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     }
     k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
     if (work > 0) {
-        k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, T, tiles_x, (int)ntiles_view, w.offset,
-                                                      w.cursor, w.list, cap, sa);
+        k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, W, H, T, tiles_x, (int)ntiles_view,
+                                                      w.offset, w.cursor, w.list, cap, sa);
     }
     dim3 grid((unsigned)ntiles_view, (unsigned)views);
     if (T == 8)

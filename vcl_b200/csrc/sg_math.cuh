@@ -611,27 +611,32 @@ struct SPix4 {
     float4 b;    // ss p, sa
     float4 g;    // dL/dout
     float4 gd;   // dL/dout * diffuse
-    float4 c;    // ss log2 e, -, -, -
+    float4 c;    // ss log2 e, |2.133 n|^2, |ss p|^2, -
 };
 
 DEV SPix4 spix4(float3 n, float3 pax, float ss, float sa, float4 dfs, float4 go) {
     SPix4 z;
-    z.a = make_float4(n.x * SG_DIFF_SHARP, n.y * SG_DIFF_SHARP, n.z * SG_DIFF_SHARP, ss);
-    z.b = make_float4(pax.x * ss, pax.y * ss, pax.z * ss, sa);
+    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+    z.a = make_float4(dn.x, dn.y, dn.z, ss);
+    z.b = make_float4(sn.x, sn.y, sn.z, sa);
     z.g = go;
     z.gd = make_float4(go.x * dfs.x, go.y * dfs.y, go.z * dfs.z, go.w * dfs.w);
-    z.c = make_float4(ss * SG_L2E, 0.f, 0.f, 0.f);
+    z.c = make_float4(ss * SG_L2E, dot3(dn, dn), dot3(sn, sn), 0.f);
     return z;
 }
 
-// One lane's lobe (C = 4) with its gradient sums.
+// One lane's lobe (C = 4) with its gradient sums.  The axis gradient
+// sum_p c1 (u_d + s a) + c2 (u_s + s a) is kept as ax = sum (c1 u_d + c2 u_s)
+// plus axs = sum (c1 + c2), combined with s a when the lane flushes.
 struct Lobe4 {
     bool valid;
     float3 sgn;
     float3 a0;                 // raw axis (EXACT sharpness derivative)
     float gs, gsl, cdl, agA;   // sharpness, s*log2e, (2.133 + s)*log2e, 2.34*s
+    float sg2, a02;            // |s a|^2, |a|^2
     float4 a;
     float3 ax;
+    float axs;
     float sh;
     float4 am;
 };
@@ -644,66 +649,88 @@ DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* shar
     L.gsl = s * SG_L2E;
     L.cdl = (SG_DIFF_SHARP + s) * SG_L2E;
     L.agA = SG_DIFF_AMP * s;
-    L.sgn = K ? f3(axis[3 * ii] * s, axis[3 * ii + 1] * s, axis[3 * ii + 2] * s) : f3(0.f, 0.f, 0.f);
     L.a0 = K ? f3(axis[3 * ii], axis[3 * ii + 1], axis[3 * ii + 2]) : f3(0.f, 0.f, 0.f);
+    L.sgn = L.a0 * s;
+    L.sg2 = dot3(L.sgn, L.sgn);
+    L.a02 = dot3(L.a0, L.a0);
     L.a = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
     L.ax = f3(0.f, 0.f, 0.f);
+    L.axs = 0.f;
     L.sh = 0.f;
     L.am = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Gradient contributions of one pixel to one lobe (material.cu:398-433),
-// rearranged: d(axis) = dsum * (A s sumd sd) + ssum * (s sum sa sds) with the
-// scalar factors sd, sds in place of the vectors ddg, dsg.
+// rearranged.  With v = u + s a (u = 2.133 n for the diffuse term, ss p for
+// the specular one), |v|^2 = |u|^2 + |s a|^2 + 2 u.(s a), and the dot product
+// is the one the reference's sharpness derivative uses.  With e-/e+ the two
+// exponentials, Dm = e- - e+ and T = (e- + e+) - il Dm:  value = Dm il,
+// (d value/d|v|)/|v| = T il^2,  d value/ds = il (dotn T - Dm)  (the
+// reference's ((dotn (1-il) - 1) e- + (dotn (1+il) + 1) e+) il, expanded).
+// The reference's guarded adds (common.h:181) drop a non-finite
+// contribution; when the contributions sum to a finite value they are all
+// finite and are added plainly, else each is checked.
 template <bool EXACT>
 DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
     const float3 dn = f3(P.a.x, P.a.y, P.a.z), sn = f3(P.b.x, P.b.y, P.b.z);
     const float sa = P.b.w;
     // diffuse lobe
-    const float3 dsum = dn + L.sgn;
-    float dl, il;
-    sg_len(dot3(dsum, dsum), dl, il);
-    const float dotn = EXACT ? dot3(L.a0, dsum) * il : (L.gs + dot3(L.sgn, dn)) * il;
+    const float dd = dot3(L.sgn, dn);
+    float dl, dil;
+    sg_len(fmaf(2.f, dd, P.c.y + L.sg2), dl, dil);
+    const float dotn = EXACT ? fmaf(L.gs, L.a02, dot3(L.a0, dn)) * dil : (L.gs + dd) * dil;
     float x = dl * SG_L2E;
     float em = ex2_fast(x - L.cdl), ep = ex2_fast(-x - L.cdl);
-    float ilm = 1.f - il, ilp = 1.f + il;
-    const float dg = (em - ep) * il * SG_DIFF_AMP;
-    const float sd = (ilm * em + ilp * ep) * il * il;
-    const float ddgs = ((dotn * ilm - 1.f) * em + (dotn * ilp + 1.f) * ep) * il;
+    const float dDm = em - ep, dT = fmaf(-dil, dDm, em + ep);
     // specular lobe
-    const float3 ssum = sn + L.sgn;
-    float sl;
-    sg_len(dot3(ssum, ssum), sl, il);
-    const float dots = EXACT ? dot3(L.a0, ssum) * il : (L.gs + dot3(L.sgn, sn)) * il;
+    const float sd = dot3(L.sgn, sn);
+    float sl, sil;
+    sg_len(fmaf(2.f, sd, P.c.z + L.sg2), sl, sil);
+    const float dots = EXACT ? fmaf(L.gs, L.a02, dot3(L.a0, sn)) * sil : (L.gs + sd) * sil;
     x = sl * SG_L2E;
     const float c = P.c.x + L.gsl;
     em = ex2_fast(x - c); ep = ex2_fast(-x - c);
-    ilm = 1.f - il; ilp = 1.f + il;
-    const float sgv = (em - ep) * il * sa;
-    const float sds = (ilm * em + ilp * ep) * il * il;
-    const float dsgs = ((dots * ilm - 1.f) * em + (dots * ilp + 1.f) * ep) * il;
+    const float sDm = em - ep, sT = fmaf(-sil, sDm, em + ep);
     // channel sums
     const float sum = P.g.x * L.a.x + P.g.y * L.a.y + P.g.z * L.a.z + P.g.w * L.a.w;
     const float sumd = P.gd.x * L.a.x + P.gd.y * L.a.y + P.gd.z * L.a.z + P.gd.w * L.a.w;
+    const float dg = dDm * dil * SG_DIFF_AMP;
+    const float sgv = sDm * sil * sa;
+    const float c1 = sumd * (dT * dil * dil) * L.agA;
+    const float c2 = sum * (sT * sil * sil) * (sa * L.gs);
+    const float shc = fmaf(sumd * dil * SG_DIFF_AMP, fmaf(dotn, dT, -dDm), sum * sil * sa * fmaf(dots, sT, -sDm));
+    if (isfinite(dg + sgv + c1 + c2 + shc)) {
+        L.am.x = fmaf(sgv, P.g.x, fmaf(dg, P.gd.x, L.am.x));
+        L.am.y = fmaf(sgv, P.g.y, fmaf(dg, P.gd.y, L.am.y));
+        L.am.z = fmaf(sgv, P.g.z, fmaf(dg, P.gd.z, L.am.z));
+        L.am.w = fmaf(sgv, P.g.w, fmaf(dg, P.gd.w, L.am.w));
+        L.ax.x = fmaf(c2, sn.x, fmaf(c1, dn.x, L.ax.x));
+        L.ax.y = fmaf(c2, sn.y, fmaf(c1, dn.y, L.ax.y));
+        L.ax.z = fmaf(c2, sn.z, fmaf(c1, dn.z, L.ax.z));
+        L.axs += c1 + c2;
+        L.sh += shc;
+        return;
+    }
     if (isfinite(dg) && isfinite(sgv)) {
         L.am.x = fmaf(sgv, P.g.x, fmaf(dg, P.gd.x, L.am.x));
         L.am.y = fmaf(sgv, P.g.y, fmaf(dg, P.gd.y, L.am.y));
         L.am.z = fmaf(sgv, P.g.z, fmaf(dg, P.gd.z, L.am.z));
         L.am.w = fmaf(sgv, P.g.w, fmaf(dg, P.gd.w, L.am.w));
     }
-    const float c1 = sumd * sd * L.agA, c2 = sum * sds * sa * L.gs;
     if (isfinite(c1) && isfinite(c2)) {
-        L.ax.x = fmaf(c2, ssum.x, fmaf(c1, dsum.x, L.ax.x));
-        L.ax.y = fmaf(c2, ssum.y, fmaf(c1, dsum.y, L.ax.y));
-        L.ax.z = fmaf(c2, ssum.z, fmaf(c1, dsum.z, L.ax.z));
+        L.ax.x = fmaf(c2, sn.x, fmaf(c1, dn.x, L.ax.x));
+        L.ax.y = fmaf(c2, sn.y, fmaf(c1, dn.y, L.ax.y));
+        L.ax.z = fmaf(c2, sn.z, fmaf(c1, dn.z, L.ax.z));
+        L.axs += c1 + c2;
     }
-    L.sh += finite_or0(sumd * ddgs * SG_DIFF_AMP + sum * dsgs * sa);
+    L.sh += finite_or0(shc);
 }
 
 // Folds the lobe groups of the warp together and adds the lane's sums into
 // the block accumulator s_acc [K][8] (axis xyz, sharpness, amplitude[4]).
 DEV void lobe4_flush(Lobe4& L, int i, int Kp, float* s_acc) {
-    float v[8] = {L.ax.x, L.ax.y, L.ax.z, L.sh, L.am.x, L.am.y, L.am.z, L.am.w};
+    float v[8] = {fmaf(L.axs, L.sgn.x, L.ax.x), fmaf(L.axs, L.sgn.y, L.ax.y), fmaf(L.axs, L.sgn.z, L.ax.z), L.sh,
+                  L.am.x, L.am.y, L.am.z, L.am.w};
 #pragma unroll
     for (int q = 0; q < 8; ++q)
         for (int o = 16; o >= Kp; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
