@@ -291,6 +291,10 @@ typedef struct {
 
 VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fit** out);
 VCL_API void vcl_fit_destroy(vcl_fit* fit);
+/* Destroys the job without synchronizing the device: its device memory is
+ * returned in stream order on `stream`, after all work already queued there
+ * (the job's last step must be on `stream` or complete). */
+VCL_API void vcl_fit_destroy_async(vcl_fit* fit, void* stream);
 VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* fit, int strategy);
 /* Target images [views][H][W][C]; `src` is a device pointer when
  * src_is_device, else host memory (pinned for an asynchronous copy). */
@@ -301,6 +305,10 @@ VCL_API vcl_status vcl_fit_set_cameras(vcl_fit* fit, const float* mvp, const flo
  * target was staged, the step first waits for its upload and makes it the
  * target. */
 VCL_API vcl_status vcl_fit_step(vcl_fit* fit, void* stream);
+/* Sets up the fused strategy now instead of at the first fused step: raster
+ * autotuning and capture of the step's graph on `stream` (a created stream,
+ * not the legacy default stream).  Synchronizes `stream`. */
+VCL_API vcl_status vcl_fit_prepare(vcl_fit* fit, void* stream);
 /* Uploads the NEXT step's target images from host memory (pinned, for an
  * asynchronous copy) into a staging buffer on `copy_stream`, so that the
  * upload overlaps the current step; the next vcl_fit_step consumes it.  One
@@ -327,7 +335,8 @@ VCL_API vcl_status vcl_fit_raster_tuning(vcl_fit* fit, int* tile, float* ms_per_
  * of binned, bin-list capacity, whether it came from the process-wide tuning
  * cache, and the overflowed tiles of the last step (any pointer may be
  * NULL; overflow_tiles synchronizes the device).  The autotuner times tile
- * {8, 16, 32} x direct area {0, 64, 256, 1024} on the job's first fused step
+ * {8, 16, 32} at the default direct area, then direct areas {0, 64, 1024}
+ * at the best tile, on the job's first fused step
  * and sizes the capacity to twice the measured bin demand (at least the
  * automatic capacity); jobs of the same
  * (W, H, views, power-of-two triangle count) reuse the cached choice. */
@@ -355,7 +364,8 @@ VCL_API int vcl_fit_launches_per_step(const vcl_fit* fit);
  * iteration each per vcl_batch_step, as ONE CUDA graph launch.  Every member
  * runs the fused strategy (vcl_batch_add switches it); its captured step is
  * a child graph with no edges to the others, so members run concurrently.
- * The graph is rebuilt when membership or the mode changes.  No reference
+ * The graph is rebuilt when membership or the mode changes.  Members may
+ * come from different contexts of the same device.  No reference
  * counterpart (the reference runs one scene per process).  Remove a job
  * before destroying it; one host thread per batch. */
 typedef struct vcl_batch vcl_batch;
@@ -370,11 +380,14 @@ VCL_API int vcl_batch_launches_per_step(const vcl_batch* batch);
 /* -------------------------------------------------------------- serving */
 /* Serving loop: fit jobs are submitted with their host data and an
  * iteration count, admitted in arrival order while their footprint fits
- * `budget_bytes` and fewer than `max_live` jobs are resident, advanced
- * together one iteration per tick by a batched launch, and retired when
- * done.  Each tick leaves one batched launch queued behind the running one.
- * Job latency = completion - submission on the host's steady clock.  All
- * host arrays are copied at submission.  No reference counterpart. */
+ * `budget_bytes` and fewer than `max_live` jobs are resident, set up on a
+ * worker thread (upload, raster autotuning, graph capture) while the device
+ * keeps running, advanced together one iteration per tick by a batched
+ * launch, and retired when done.  Each tick leaves one batched launch queued
+ * behind the running one.  Job latency = completion - submission on the
+ * host's steady clock.  All host arrays are copied at submission.  The
+ * context's mode must not change while the server exists.  No reference
+ * counterpart. */
 typedef struct vcl_server vcl_server;
 #define VCL_JOB_QUEUED 0
 #define VCL_JOB_LIVE 1

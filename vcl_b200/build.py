@@ -51,7 +51,7 @@ def build(verbose=False, extra=None):
         subprocess.run(cmd, check=True)
         changed = True
     if changed or not os.path.exists(LIB):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -75,6 +75,8 @@ SIGNATURES = {
     "vcl_fit_raster_schedule": (c_int, [P, P, P, P, P, P]),
     "vcl_raster_tuning_cache_clear": (None, []),
     "vcl_fit_stage_target": (c_int, [P, P, P]),
+    "vcl_fit_prepare": (c_int, [P, P]),
+    "vcl_fit_destroy_async": (None, [P, P]),
     "vcl_fit_kernel_count": (c_int, []),
     "vcl_fit_kernel_name": (c_char_p, [c_int]),
     "vcl_fit_time_kernels": (c_int, [P, P, c_int, P, c_int]),

@@ -77,7 +77,7 @@ VCL_API void vcl_batch_destroy(vcl_batch* b) {
 VCL_API vcl_status vcl_batch_add(vcl_batch* b, vcl_fit* f) {
     if (!b) return VCL_ERR_ARG;
     vcl_ctx* ctx = b->ctx;
-    VCL_REQUIRE(f && f->ctx == ctx, "job is null or belongs to another context");
+    VCL_REQUIRE(f && f->ctx->device == ctx->device, "job is null or on another device");
     VCL_REQUIRE(std::find(b->jobs.begin(), b->jobs.end(), f) == b->jobs.end(), "job already in the batch");
     vcl_status st = vcl_fit_set_strategy(f, VCL_FIT_FUSED);
     if (st) return st;
@@ -103,7 +103,9 @@ VCL_API vcl_status vcl_batch_step(vcl_batch* b, void* stream) {
     vcl_ctx* ctx = b->ctx;
     cudaStream_t s = (cudaStream_t)stream;
     if (b->jobs.empty()) return VCL_OK;
-    if (b->dirty || b->mode != ctx->mode) {
+    bool stale = b->dirty || b->mode != ctx->mode;
+    for (const vcl_fit* f : b->jobs) stale = stale || f->ctx->mode != ctx->mode;
+    if (stale) {
         vcl_status st = rebuild(b);
         if (st) return st;
     }

@@ -19,6 +19,7 @@ struct vcl_ctx {
     void* ws = nullptr;
     size_t ws_bytes = 0;
     int* dev_flags = nullptr;     // [0] = overflowed tiles of the last raster call
+    cudaStream_t aux = nullptr;   // non-blocking stream for job set-up (uploads, allocations)
 };
 
 vcl_status vcl_fail(vcl_ctx* ctx, vcl_status code, const char* fmt, ...);

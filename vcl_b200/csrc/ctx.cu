@@ -64,6 +64,11 @@ VCL_API vcl_status vcl_create(int device, vcl_ctx** out) {
         delete c;
         return VCL_ERR_NOMEM;
     }
+    if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaFree(c->dev_flags);
+        delete c;
+        return VCL_ERR_CUDA;
+    }
     *out = c;
     return VCL_OK;
 }
@@ -73,6 +78,7 @@ VCL_API void vcl_destroy(vcl_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->ws) cudaFree(ctx->ws);
     if (ctx->dev_flags) cudaFree(ctx->dev_flags);
+    if (ctx->aux) cudaStreamDestroy(ctx->aux);
     delete ctx;
 }
 

@@ -120,7 +120,10 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
     if (f->d.lr_lobes <= 0) f->d.lr_lobes = f->d.lr;
     Layout L;
     plan(f->d, nullptr, L);
-    cudaError_t e = cudaMalloc(&f->arena, L.total);
+    // set-up runs on the context's non-blocking stream, so creating a job does
+    // not wait for other jobs' work on the device
+    cudaStream_t up_s = ctx->aux;
+    cudaError_t e = cudaMallocAsync(&f->arena, L.total, up_s);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
         delete f;
@@ -133,9 +136,10 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
     const size_t N = (size_t)d.W * d.H * d.views;
     const size_t n0 = (size_t)d.tex_w * d.tex_h * d.C;
     auto up = [&](void* dst, const void* src, size_t bytes) {
-        if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "fit upload");
+        if (st == VCL_OK)
+            st = vcl_cuda_check(ctx, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, up_s), "fit upload");
     };
-    st = vcl_cuda_check(ctx, cudaMemset(f->arena, 0, L.total), "fit clear");
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(f->arena, 0, L.total, up_s), "fit clear");
     up(f->pos, d.pos, sizeof(float) * d.nv * 3);
     up(f->tri, d.tri, sizeof(uint32_t) * d.nt * 3);
     up(f->uvattr, d.uv, sizeof(float) * d.nv * 2);
@@ -149,13 +153,10 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
     up(f->mvp, d.mvp, sizeof(float) * d.views * 16);
     up(f->pvinv, d.pvinv, sizeof(float) * d.views * 9);
     up(f->rot, d.rot, sizeof(float) * 16);
-    if (st == VCL_OK) {
-        std::vector<float> r(N, d.roughness);
-        up(f->rough, r.data(), sizeof(float) * N);
-    }
-    if (st == VCL_OK) st = vcl_texture_build_mips(ctx, f->pyr, d.tex_w, d.tex_h, d.C, d.levels, nullptr);
-    if (st == VCL_OK) st = vcl_reserve_raster(ctx, d.W, d.H, d.views, d.nt);
-    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaDeviceSynchronize(), "fit create");
+    std::vector<float> r(N, d.roughness);
+    up(f->rough, r.data(), sizeof(float) * N);
+    if (st == VCL_OK) st = vcl_texture_build_mips(ctx, f->pyr, d.tex_w, d.tex_h, d.C, d.levels, up_s);
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaStreamSynchronize(up_s), "fit create");
     if (st) {
         vcl_fit_destroy(f);
         return st;
@@ -174,7 +175,18 @@ VCL_API void vcl_fit_destroy(vcl_fit* f) {
     if (f->st_full) cudaEventDestroy(f->st_full);
     if (f->st_free) cudaEventDestroy(f->st_free);
     if (f->arena) cudaFree(f->arena);
-    fit_fused_release(f);
+    fit_fused_release(f, nullptr, false);
+    delete f;
+}
+
+VCL_API void vcl_fit_destroy_async(vcl_fit* f, void* stream) {
+    if (!f) return;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (f->staging) cudaFreeAsync(f->staging, s);
+    if (f->st_full) cudaEventDestroy(f->st_full);
+    if (f->st_free) cudaEventDestroy(f->st_free);
+    if (f->arena) cudaFreeAsync(f->arena, s);
+    fit_fused_release(f, s, true);
     delete f;
 }
 
@@ -183,9 +195,10 @@ VCL_API vcl_status vcl_fit_set_strategy(vcl_fit* f, int strategy) {
     vcl_ctx* ctx = f->ctx;
     VCL_REQUIRE(strategy == VCL_FIT_PLAIN || strategy == VCL_FIT_FUSED, "unknown strategy %d", strategy);
     VCL_REQUIRE(strategy == VCL_FIT_PLAIN || f->d.C == 4, "the fused strategy needs C = 4 channels");
-    if (strategy != f->strategy) {
+    if (strategy != f->strategy && f->step_count > 0) {
         // the plain step clears gradients when it starts, the fused step when
         // it has consumed them: start the other strategy from zero gradients
+        // (a job that has not stepped still has the zeroed arena)
         const vcl_fit_desc& d = f->d;
         size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, d.C, d.levels);
         vcl_status st = VCL_OK;
@@ -288,6 +301,14 @@ VCL_API const char* vcl_fit_kernel_name(int i) { return fit_fused_kernel_name(i)
 VCL_API vcl_status vcl_fit_time_kernels(vcl_fit* f, void* stream, int reps, float* ms, int n) {
     if (!f) return VCL_ERR_ARG;
     return fit_fused_time_kernels(f, (cudaStream_t)stream, reps, ms, n);
+}
+
+VCL_API vcl_status vcl_fit_prepare(vcl_fit* f, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(f->strategy == VCL_FIT_FUSED, "prepare applies to the fused strategy");
+    cudaGraph_t g = nullptr;
+    return fit_fused_graph(f, (cudaStream_t)stream, &g);
 }
 
 VCL_API vcl_status vcl_fit_stage_target(vcl_fit* f, const float* host_src, void* copy_stream) {

@@ -33,7 +33,8 @@ vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s);
 vcl_status fit_forward(vcl_fit* f, float* out, cudaStream_t s);
 int fit_plain_launches(const vcl_fit* f);
 int fit_fused_launches(const vcl_fit* f);
-void fit_fused_release(vcl_fit* f);
+// Frees the fused state; `async`: stream-ordered frees on `s` (no device sync).
+void fit_fused_release(vcl_fit* f, cudaStream_t s, bool async);
 vcl_status fit_fused_sync_counter(vcl_fit* f, bool to_device);
 vcl_status fit_fused_raster_tuning(vcl_fit* f, int* tile, float* ms3);
 vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, long long* cap, int* cached,

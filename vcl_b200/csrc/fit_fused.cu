@@ -486,15 +486,18 @@ vcl_status fused_init(vcl_fit* f) {
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
     Fused* F = new Fused();
-    cudaError_t e = cudaMalloc(&F->d_step, 64);
-    if (e == cudaSuccess) e = cudaMalloc(&F->d_corr, 64);
-    if (e == cudaSuccess) e = cudaMalloc(&F->flags, 64);
-    if (e == cudaSuccess) e = cudaMemset(F->flags, 0, 64);
+    cudaStream_t as = ctx->aux;
+    cudaError_t e = cudaMallocAsync(&F->d_step, 64, as);
+    if (e == cudaSuccess) e = cudaMallocAsync(&F->d_corr, 64, as);
+    if (e == cudaSuccess) e = cudaMallocAsync(&F->flags, 64, as);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F->flags, 0, 64, as);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice, as);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        if (F->d_step) cudaFree(F->d_step);
-        if (F->d_corr) cudaFree(F->d_corr);
-        if (F->flags) cudaFree(F->flags);
+        if (F->d_step) cudaFreeAsync(F->d_step, as);
+        if (F->d_corr) cudaFreeAsync(F->d_corr, as);
+        if (F->flags) cudaFreeAsync(F->flags, as);
         delete F;
         return vcl_fail(ctx, VCL_ERR_NOMEM, "fused fit state: %s", cudaGetErrorString(e));
     }
@@ -505,25 +508,28 @@ vcl_status fused_init(vcl_fit* f) {
     if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "fused streams");
     size_t sf = shade_smem(d.K);
     if (sf > 48 * 1024) cudaFuncSetAttribute(k_shade_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
-    vcl_status st = vcl_cuda_check(ctx, cudaMemcpy(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice),
-                                   "fused init");
-    if (st) return st;
     return autotune_raster(f);
 }
 
+// Grows the job's raster workspace.  Called only while the job has no step
+// in flight (from the autotuner, before its step is captured), so the old
+// buffer can go back to the pool once the job's own stream is idle.
 vcl_status raster_ws_ensure(vcl_fit* f, size_t bytes) {
     Fused* F = (Fused*)f->fused;
     if (bytes <= F->raster_ws_bytes) return VCL_OK;
+    cudaStream_t as = f->ctx->aux;
+    cudaError_t e = cudaSuccess;
     if (F->raster_ws) {
-        cudaError_t e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) return vcl_cuda_check(f->ctx, e, "raster workspace sync");
-        cudaFree(F->raster_ws);
+        e = cudaStreamSynchronize(F->side);
+        if (e == cudaSuccess) e = cudaFreeAsync(F->raster_ws, as);
         F->raster_ws = nullptr;
         F->raster_ws_bytes = 0;
     }
-    cudaError_t e = cudaMalloc(&F->raster_ws, bytes);
+    if (e == cudaSuccess) e = cudaMallocAsync(&F->raster_ws, bytes, as);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
+        F->raster_ws = nullptr;
         return vcl_fail(f->ctx, VCL_ERR_NOMEM, "raster workspace of %zu bytes: %s", bytes, cudaGetErrorString(e));
     }
     F->raster_ws_bytes = bytes;
@@ -557,9 +563,10 @@ TuneKey tune_key(const vcl_fit_desc& d) {
 // overflowing tile takes the slow every-triangle path.
 long long cap_floor(const vcl_fit_desc& d, int tile) { return raster_auto_capacity(d.views, d.nt, d.W, d.H, tile); }
 
-// Raster autotuner.  Times the binning schedules -- tile edge {8, 16, 32} x
-// direct-rasterization box area {0, 64, 256, 1024} pixels -- on this job's
-// own geometry, keeps the fastest, then sizes the bin-list capacity to twice
+// Raster autotuner.  Times the binning schedules on this job's own
+// geometry -- tile edge {8, 16, 32} at the default direct-rasterization box
+// area, then box areas {0, 64, 1024} pixels at the best tile -- keeps the
+// fastest, then sizes the bin-list capacity to twice
 // the entries that schedule asked for, never below the automatic capacity
 // (the mesh moves during the fit; an overflowing tile still gets exact
 // results through the all-triangle fallback, only slower).  Jobs of the same size bucket reuse the cached choice.  Runs
@@ -604,23 +611,34 @@ vcl_status autotune_raster(vcl_fit* f) {
     float best = 1e30f;
     RasterSched pick{16, cap, raster_default_small_area()};
     for (int i = 0; i < 3; ++i) F->tune_ms[i] = 1e30f;
-    for (int ti = 0; ti < 3 && st == VCL_OK; ++ti) {
-        for (int sa : smalls) {
-            RasterSched rs{tiles[ti], cap, sa};
-            for (int rep = 0; rep < 4 && st == VCL_OK; ++rep) {
-                if (rep == 1) cudaEventRecord(e0, s);
-                st = raster_fwd_ws(ctx, F->raster_ws, rs, F->flags, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views,
-                                   f->rast, f->db, s);
-            }
-            cudaEventRecord(e1, s);
-            if (st) break;
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= 3.f;
-            if (ms < F->tune_ms[ti]) F->tune_ms[ti] = ms;
-            if (ms < best) { best = ms; pick = rs; }
+    auto time_sched = [&](const RasterSched& rs, float& ms) -> vcl_status {
+        vcl_status r = VCL_OK;
+        for (int rep = 0; rep < 3 && r == VCL_OK; ++rep) {
+            if (rep == 1) cudaEventRecord(e0, s);
+            r = raster_fwd_ws(ctx, F->raster_ws, rs, F->flags, f->clip, d.nv, f->tri, d.nt, d.W, d.H, d.views,
+                              f->rast, f->db, s);
         }
+        cudaEventRecord(e1, s);
+        if (r) return r;
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 2.f;
+        return VCL_OK;
+    };
+    // tile edge at the default direct area, then the direct area at that tile
+    for (int ti = 0; ti < 3 && st == VCL_OK; ++ti) {
+        RasterSched rs{tiles[ti], cap, raster_default_small_area()};
+        float ms = 0.f;
+        st = time_sched(rs, ms);
+        F->tune_ms[ti] = ms;
+        if (!st && ms < best) { best = ms; pick = rs; }
+    }
+    for (int sa : smalls) {
+        if (st || sa == raster_default_small_area()) continue;
+        RasterSched rs{pick.tile, cap, sa};
+        float ms = 0.f;
+        st = time_sched(rs, ms);
+        if (!st && ms < best) { best = ms; pick = rs; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -838,15 +856,20 @@ int fit_fused_launches(const vcl_fit* f) {
     return n;
 }
 
-void fit_fused_release(vcl_fit* f) {
+void fit_fused_release(vcl_fit* f, cudaStream_t s, bool async) {
     Fused* F = (Fused*)f->fused;
     if (!F) return;
     if (F->graph) cudaGraphExecDestroy(F->graph);
     if (F->graph_def) cudaGraphDestroy(F->graph_def);
-    if (F->raster_ws) cudaFree(F->raster_ws);
-    if (F->flags) cudaFree(F->flags);
-    if (F->d_step) cudaFree(F->d_step);
-    if (F->d_corr) cudaFree(F->d_corr);
+    auto release = [&](void* p) {
+        if (!p) return;
+        if (async) cudaFreeAsync(p, s);
+        else cudaFree(p);
+    };
+    release(F->raster_ws);
+    release(F->flags);
+    release(F->d_step);
+    release(F->d_corr);
     if (F->side) cudaStreamDestroy(F->side);
     if (F->fork) cudaEventDestroy(F->fork);
     if (F->join) cudaEventDestroy(F->join);

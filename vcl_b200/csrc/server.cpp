@@ -1,31 +1,39 @@
 // Serving loop for inverse-rendering fit jobs, built on the public C ABI
 // (vcl_fit_* and vcl_batch_*).
 //
-//   submit   copies the job's host arrays and target images, queues it
+//   submit   copies the job's host arrays and target images and queues it
 //            (FIFO) with its iteration count;
 //   tick     1. retires the jobs whose last iteration ran in a tick that
 //               has been seen to complete: optional copy of the final
-//               parameters, the job's device memory released (its
-//               completion time was stamped when the tick was seen done);
+//               parameters, the job's device memory returned in stream order
+//               (its completion time was stamped when the tick was seen);
 //            2. admits queued jobs in arrival order while their device
-//               footprint (vcl_fit_footprint) fits the remaining budget and
-//               a live slot is free -- the job's mesh, texture pyramid,
-//               lobes, Adam moments and per-view buffers become resident;
-//            3. advances every live job by one iteration with ONE batched
+//               footprint (vcl_fit_footprint) fits the remaining budget and a
+//               slot is free, reserving the footprint and handing the job to
+//               the set-up worker;
+//            3. moves the jobs the worker has set up into the batch;
+//            4. advances every live job by one iteration with ONE batched
 //               launch (vcl_batch_step) and records an event;
-//            4. waits for the PREVIOUS tick's event, so that one tick is
-//               always queued behind the running one (continuous batching:
-//               the device never waits for the host in steady state).
-// Jobs that arrive while others run join at the next tick; finished jobs
-// leave the batch before the next launch.  Latency = completion - submit on
-// the host's steady clock.
+//            5. waits for the PREVIOUS tick's event, so that one tick is
+//               always queued behind the running one.
+//   worker   a host thread with its own context on the same device: creates
+//            the job's resident state (mesh, texture pyramid, lobes, Adam
+//            moments, per-view buffers), uploads its target, tunes its
+//            raster schedule and captures its step graph, all on its own
+//            streams, while the tick loop keeps the device busy.
+// Jobs that arrive while others run join at a later tick (continuous
+// batching); finished jobs leave the batch before the next launch.  Latency
+// = completion - submission on the host's steady clock.
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -63,24 +71,34 @@ std::vector<T> copy_of(const T* p, size_t n) {
 }  // namespace
 
 struct vcl_server {
-    vcl_ctx* ctx = nullptr;
+    vcl_ctx* ctx = nullptr;          // the caller's context: batch and ticks
+    vcl_ctx* wctx = nullptr;         // the set-up worker's context
+    int device = 0;
     vcl_batch* batch = nullptr;
-    size_t budget = 0, used = 0;
+    size_t budget = 0, used = 0;     // bytes reserved by admitted jobs
     int max_live = 0;
     long long next_id = 1;
-    std::deque<Job*> queue;
-    std::vector<Job*> live;
+    std::deque<Job*> queue;          // submitted, not admitted
+    std::vector<Job*> live;          // in the batch
+    int in_setup = 0;                // admitted, handed to the worker, not live yet
     // jobs whose last iteration has been launched, with that tick's index
     std::vector<std::pair<Job*, long long>> finishing;
     std::map<long long, std::unique_ptr<Job>> jobs;
-    cudaStream_t aux = nullptr;          // result readback
+    cudaStream_t aux = nullptr;      // result readback
     cudaEvent_t ev[2] = {nullptr, nullptr};   // completion of tick t is ev[t & 1]
     Clock::time_point t0;
     long long iters_total = 0;
-    long long ticks = 0;        // ticks launched
-    long long done_tick = -1;   // highest tick known to have completed
+    long long ticks = 0;             // ticks launched
+    long long done_tick = -1;        // highest tick known to have completed
     std::vector<double> latencies;
     std::string err;
+    // set-up worker
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Job*> to_setup;       // guarded by mu
+    std::deque<Job*> set_up;         // guarded by mu: ready (or failed) jobs
+    bool stop = false;               // guarded by mu
 
     double now_ms() const { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 };
@@ -92,12 +110,55 @@ vcl_status fail(vcl_server* s, vcl_status code, const std::string& msg) {
     return code;
 }
 
-vcl_status fit_error(vcl_server* s, vcl_status st, const char* what) {
-    s->err = std::string(what) + ": " + vcl_last_error(s->ctx);
+vcl_status fit_error(vcl_server* s, vcl_ctx* ctx, vcl_status st, const char* what) {
+    s->err = std::string(what) + ": " + vcl_last_error(ctx);
     return st;
 }
 
-vcl_status retire(vcl_server* s, Job* j) {
+// Worker: resident state, target upload, raster tuning and graph capture of
+// one job, on the worker's own context and stream.
+void set_up_job(vcl_server* s, Job* j, cudaStream_t ws) {
+    vcl_fit* f = nullptr;
+    vcl_status st = vcl_fit_create(s->wctx, &j->d, &f);
+    if (!st) st = vcl_fit_set_target(f, j->target.data(), 0, ws);
+    if (!st) st = vcl_fit_set_strategy(f, VCL_FIT_FUSED);
+    if (!st) st = vcl_fit_prepare(f, ws);
+    if (!st && cudaStreamSynchronize(ws) != cudaSuccess) st = VCL_ERR_CUDA;
+    if (st) {
+        j->error = vcl_last_error(s->wctx);
+        if (f) vcl_fit_destroy(f);
+        j->state = FAILED;
+        return;
+    }
+    j->target.clear(); j->target.shrink_to_fit();
+    j->tex.clear(); j->tex.shrink_to_fit();
+    j->fit = f;
+}
+
+void worker_main(vcl_server* s) {
+    cudaSetDevice(s->device);
+    cudaStream_t ws = nullptr;
+    cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking);
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait(lk, [&] { return s->stop || !s->to_setup.empty(); });
+            if (s->stop) break;
+            j = s->to_setup.front();
+            s->to_setup.pop_front();
+        }
+        set_up_job(s, j, ws);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->set_up.push_back(j);
+        }
+        s->cv.notify_all();
+    }
+    if (ws) cudaStreamDestroy(ws);
+}
+
+vcl_status retire(vcl_server* s, Job* j, cudaStream_t cs) {
     vcl_status st = VCL_OK;
     if (j->keep) {
         const vcl_fit_desc& d = j->d;
@@ -109,9 +170,10 @@ vcl_status retire(vcl_server* s, Job* j) {
         st = vcl_fit_read_params(j->fit, j->r_pos.data(), j->r_tex.data(), j->r_axis.data(), j->r_sharp.data(),
                                  j->r_amp.data(), s->aux);
         if (!st) st = vcl_fit_read_loss(j->fit, &j->loss, s->aux);
-        if (st) fit_error(s, st, "job result readback");
+        if (st) fit_error(s, s->wctx, st, "job result readback");
     }
-    vcl_fit_destroy(j->fit);
+    // stream-ordered release: no device synchronization in the tick loop
+    vcl_fit_destroy_async(j->fit, cs);
     j->fit = nullptr;
     s->used -= j->footprint;
     j->state = st ? FAILED : DONE;
@@ -119,31 +181,39 @@ vcl_status retire(vcl_server* s, Job* j) {
     return st;
 }
 
-vcl_status admit(vcl_server* s, Job* j) {
-    vcl_fit* f = nullptr;
-    vcl_status st = vcl_fit_create(s->ctx, &j->d, &f);
-    if (st) {
-        j->state = FAILED;
-        j->error = vcl_last_error(s->ctx);
-        return VCL_OK;   // the job fails; the server keeps going
+// Moves the jobs the worker finished into the batch (or releases a failed
+// job's reservation).  `wait`: block until at least one arrives.
+vcl_status collect(vcl_server* s, bool wait) {
+    std::deque<Job*> ready;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (wait) s->cv.wait(lk, [&] { return !s->set_up.empty(); });
+        ready.swap(s->set_up);
     }
-    st = vcl_fit_set_target(f, j->target.data(), 0, s->aux);
-    if (!st) st = vcl_batch_add(s->batch, f);
-    if (!st) st = cudaStreamSynchronize(s->aux) == cudaSuccess ? VCL_OK : VCL_ERR_CUDA;
-    if (st) {
-        j->state = FAILED;
-        j->error = vcl_last_error(s->ctx);
-        vcl_fit_destroy(f);
-        return VCL_OK;
+    for (Job* j : ready) {
+        --s->in_setup;
+        if (j->state == FAILED) {
+            s->used -= j->footprint;
+            continue;
+        }
+        vcl_status st = vcl_batch_add(s->batch, j->fit);
+        if (st) return fit_error(s, s->ctx, st, "batch add");
+        j->state = LIVE;
+        j->t_admit = s->now_ms();
+        s->live.push_back(j);
     }
-    // host copies are no longer needed once the job is resident
-    j->target.clear(); j->target.shrink_to_fit();
-    j->tex.clear(); j->tex.shrink_to_fit();
-    j->fit = f;
-    j->state = LIVE;
-    j->t_admit = s->now_ms();
-    s->used += j->footprint;
-    s->live.push_back(j);
+    return VCL_OK;
+}
+
+// Waits for tick `t` and stamps the completion time of the jobs that ended in
+// it or earlier.
+vcl_status observe(vcl_server* s, long long t) {
+    if (t <= s->done_tick) return VCL_OK;
+    if (cudaEventSynchronize(s->ev[t & 1]) != cudaSuccess) return fail(s, VCL_ERR_CUDA, "tick wait");
+    s->done_tick = t;
+    const double now = s->now_ms();
+    for (auto& p : s->finishing)
+        if (p.second <= t && p.first->t_done < 0) p.first->t_done = now;
     return VCL_OK;
 }
 
@@ -154,35 +224,50 @@ extern "C" {
 VCL_API vcl_status vcl_server_create(vcl_ctx* ctx, size_t budget_bytes, int max_live, vcl_server** out) {
     if (!ctx || !out || max_live <= 0 || budget_bytes == 0) return VCL_ERR_ARG;
     *out = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return VCL_ERR_CUDA;
     auto* s = new vcl_server();
     s->ctx = ctx;
+    s->device = dev;
     s->budget = budget_bytes;
     s->max_live = max_live;
     vcl_status st = vcl_batch_create(ctx, &s->batch);
+    if (!st) st = vcl_create(dev, &s->wctx);
+    if (!st) st = vcl_set_mode(s->wctx, vcl_get_mode(ctx));
     if (!st && cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess) st = VCL_ERR_CUDA;
     for (int i = 0; i < 2 && !st; ++i)
         if (cudaEventCreateWithFlags(&s->ev[i], cudaEventDisableTiming) != cudaSuccess) st = VCL_ERR_CUDA;
     if (st) {
         if (s->batch) vcl_batch_destroy(s->batch);
+        if (s->wctx) vcl_destroy(s->wctx);
         delete s;
         return st;
     }
     s->t0 = Clock::now();
+    s->worker = std::thread(worker_main, s);
     *out = s;
     return VCL_OK;
 }
 
 VCL_API void vcl_server_destroy(vcl_server* s) {
     if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
     cudaDeviceSynchronize();
     for (Job* j : s->live) {
         vcl_batch_remove(s->batch, j->fit);
         vcl_fit_destroy(j->fit);
     }
     for (auto& p : s->finishing) if (p.first->fit) vcl_fit_destroy(p.first->fit);
+    for (Job* j : s->set_up) if (j->fit) vcl_fit_destroy(j->fit);
     vcl_batch_destroy(s->batch);
     if (s->aux) cudaStreamDestroy(s->aux);
     for (auto& e : s->ev) if (e) cudaEventDestroy(e);
+    vcl_destroy(s->wctx);
     delete s;
 }
 
@@ -232,22 +317,6 @@ VCL_API vcl_status vcl_server_submit(vcl_server* s, const vcl_fit_desc* desc, co
     return VCL_OK;
 }
 
-namespace {
-
-// Waits for tick `t` and stamps the completion time of the jobs that ended in
-// it or earlier.
-vcl_status observe(vcl_server* s, long long t) {
-    if (t <= s->done_tick) return VCL_OK;
-    if (cudaEventSynchronize(s->ev[t & 1]) != cudaSuccess) return fail(s, VCL_ERR_CUDA, "tick wait");
-    s->done_tick = t;
-    const double now = s->now_ms();
-    for (auto& p : s->finishing)
-        if (p.second <= t && p.first->t_done < 0) p.first->t_done = now;
-    return VCL_OK;
-}
-
-}  // namespace
-
 VCL_API vcl_status vcl_server_tick(vcl_server* s, void* stream, int* live_out, int* completed_out) {
     if (!s) return VCL_ERR_ARG;
     cudaStream_t cs = (cudaStream_t)stream;
@@ -257,7 +326,7 @@ VCL_API vcl_status vcl_server_tick(vcl_server* s, void* stream, int* live_out, i
     std::vector<std::pair<Job*, long long>> keep;
     for (auto& p : s->finishing) {
         if (p.second <= s->done_tick) {
-            vcl_status r = retire(s, p.first);
+            vcl_status r = retire(s, p.first, cs);
             if (r && !st) st = r;
             ++completed;
         } else {
@@ -265,19 +334,31 @@ VCL_API vcl_status vcl_server_tick(vcl_server* s, void* stream, int* live_out, i
         }
     }
     s->finishing.swap(keep);
-    // 2. admission, in arrival order
-    while (!s->queue.empty() && (int)s->live.size() < s->max_live &&
+    // 2. admission in arrival order: reserve the footprint, hand to the worker
+    int handed = 0;
+    while (!s->queue.empty() && (int)s->live.size() + s->in_setup < s->max_live &&
            s->used + s->queue.front()->footprint <= s->budget) {
         Job* j = s->queue.front();
         s->queue.pop_front();
-        vcl_status r = admit(s, j);
-        if (r) return fit_error(s, r, "admission");
+        s->used += j->footprint;
+        ++s->in_setup;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->to_setup.push_back(j);
+        }
+        ++handed;
     }
-    // 3. one batched iteration of every live job
+    if (handed) s->cv.notify_all();
+    // 3. jobs set up since the last tick join the batch; with nothing live and
+    //    nothing in flight, wait for the worker instead of spinning
+    const bool idle = s->live.empty() && s->in_setup > 0 && s->done_tick == s->ticks - 1;
+    vcl_status r = collect(s, idle);
+    if (r) return r;
+    // 4. one batched iteration of every live job
     if (!s->live.empty()) {
         const long long t = s->ticks;
-        vcl_status r = vcl_batch_step(s->batch, cs);
-        if (r) return fit_error(s, r, "batch step");
+        r = vcl_batch_step(s->batch, cs);
+        if (r) return fit_error(s, s->ctx, r, "batch step");
         if (cudaEventRecord(s->ev[t & 1], cs) != cudaSuccess) return fail(s, VCL_ERR_CUDA, "tick event");
         ++s->ticks;
         s->iters_total += (long long)s->live.size();
@@ -291,13 +372,13 @@ VCL_API vcl_status vcl_server_tick(vcl_server* s, void* stream, int* live_out, i
             }
         }
         s->live.swap(still);
-        // 4. wait for the previous tick; this one stays queued behind it
+        // 5. wait for the previous tick; this one stays queued behind it
         if (t >= 1) {
             r = observe(s, t - 1);
             if (r) return r;
         }
     } else if (s->ticks > 0) {
-        vcl_status r = observe(s, s->ticks - 1);
+        r = observe(s, s->ticks - 1);
         if (r) return r;
     }
     if (live_out) *live_out = (int)s->live.size();
@@ -312,7 +393,9 @@ VCL_API vcl_status vcl_server_drain(vcl_server* s, void* stream) {
         int live = 0;
         vcl_status st = vcl_server_tick(s, stream, &live, nullptr);
         if (st) return st;
-        if (live == 0 && s->queue.empty() && s->finishing.empty() && s->done_tick == s->ticks - 1) return VCL_OK;
+        if (live == 0 && s->queue.empty() && s->in_setup == 0 && s->finishing.empty() &&
+            s->done_tick == s->ticks - 1)
+            return VCL_OK;
     }
 }
 
@@ -320,7 +403,7 @@ VCL_API double vcl_server_now_ms(const vcl_server* s) { return s ? s->now_ms() :
 
 VCL_API int vcl_server_pending(const vcl_server* s) {
     if (!s) return 0;
-    return (int)(s->queue.size() + s->live.size() + s->finishing.size());
+    return (int)(s->queue.size() + s->live.size() + s->finishing.size()) + s->in_setup;
 }
 
 VCL_API vcl_status vcl_server_job_status(const vcl_server* s, long long id, int* state, int* iters_done,
@@ -352,7 +435,7 @@ VCL_API vcl_status vcl_server_job_result(const vcl_server* s, long long id, floa
 }
 
 /* Latency percentiles (ms, nearest rank) over completed jobs, total
- * iterations run, completed jobs, ticks, bytes resident now. */
+ * iterations run, completed jobs, ticks, bytes reserved now. */
 VCL_API vcl_status vcl_server_stats(const vcl_server* s, double* p50_ms, double* p99_ms, long long* iterations,
                                     int* completed, long long* ticks, size_t* resident_bytes) {
     if (!s) return VCL_ERR_ARG;
