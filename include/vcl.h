@@ -69,6 +69,10 @@ VCL_API int vcl_get_mode(const vcl_ctx* ctx);
  * rasterizer configuration of rasterize.cpp:206-254. */
 VCL_API vcl_status vcl_set_raster_config(vcl_ctx* ctx, int tile, long long bin_capacity);
 VCL_API vcl_status vcl_get_raster_config(const vcl_ctx* ctx, int* tile, long long* bin_capacity);
+/* Box areas (pixels) below which a triangle skips the tile bins: up to
+ * `small_area` it is rasterized by its setup thread, up to `medium_area` by
+ * one warp (-1: the defaults 256 and 4096; 0 and 0 bin every triangle). */
+VCL_API vcl_status vcl_set_raster_areas(vcl_ctx* ctx, int small_area, int medium_area);
 /* Number of tiles that overflowed the bin list in the last raster call
  * (they were rasterized by the slower all-triangles path; results are
  * unaffected).  Reading it synchronizes `stream`. */
@@ -111,7 +115,7 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
  * not allocate device memory or synchronize the device on their per-frame
  * path.  No counterpart in the reference (its rasterizer has no workspace).
  * Same arguments and results as vcl_rasterize_fwd.  Requests whose depth
- * keys (8 B per pixel and view), triangle records (80 B per view and
+ * keys (8 B per pixel and view), triangle records (84 B per view and
  * triangle) and tile counters exceed the limit return VCL_ERR_ARG.  No part
  * of the scratch needs to start at zero.  One scratch per device: calls
  * whose work overlaps on the device race, so serialize them.  The first call

@@ -90,9 +90,11 @@ def test_chained_pipeline_matches_oracle(ctx, mode):
 
 @pytest.mark.parametrize("tile,cap", [(8, 0), (16, 0), (32, 0), (16, 64), (8, 1)])
 @pytest.mark.parametrize("subdiv", [1, 4])
-def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap, subdiv):
-    # subdiv 1: large triangles (tile binner, bins overflow when capped);
-    # subdiv 4: mostly small triangles (direct path) mixed with a few large
+@pytest.mark.parametrize("areas", [(-1, -1), (0, 0), (64, 1024)])
+def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap, subdiv, areas):
+    # subdiv 1: large triangles, subdiv 4: mostly small ones; areas (0, 0)
+    # bins every triangle (bins overflow when capped), the others send small
+    # and medium triangles to the thread / warp paths
     import gpu_chain as G
     S = scenes.make_scene("raster", mesh=("ico", subdiv), W=200, H=150, views=2, tex=16, K=1, dist=(2.0, 3.5),
                           disp=0.05, seed=9)
@@ -101,18 +103,20 @@ def test_raster_tiles_and_bin_overflow_bit_exact(ctx, tile, cap, subdiv):
     rast = np.zeros((N, 4), np.float32); db = np.zeros((N, 4), np.float32)
     O.orc().rasterize_fwd(S.W, S.H, S.views, clip, S.nv, S.tri, S.nt, 1, rast, db)
     ctx.set_raster_config(tile, cap)
+    ctx.set_raster_areas(*areas)
     try:
         gr = G.zeros(N, 4); gd = G.zeros(N, 4)
         ctx.rasterize_fwd(G.dev(clip), S.nv, G.dev(S.tri.astype(np.int32)), S.nt, S.W, S.H, S.views, gr, gd, None)
         ov = ctx.raster_overflow_count()
         assert np.array_equal(G.host(gr), rast)
         assert np.array_equal(G.host(gd), db)
-        if cap and subdiv == 1:
+        if cap and areas == (0, 0):
             assert ov > 0
         elif not cap:
             assert ov == 0
     finally:
         ctx.set_raster_config(16, 0)
+        ctx.set_raster_areas(-1, -1)
 
 
 def test_raster_config1_scale_bit_exact(ctx):
@@ -208,3 +212,44 @@ def test_adam_bit_exact_over_steps(ctx, mode):
     assert np.array_equal(G.host(tp), p)
     assert np.array_equal(G.host(tm), m)
     assert np.array_equal(G.host(tv), v)
+
+
+@pytest.mark.parametrize("areas", [(-1, -1), (4096, 4096), (0, 0)])
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_raster_random_triangles_bit_exact(ctx, areas, seed):
+    """Random clip-space triangles -- slivers, near-degenerate, large,
+    partly behind the camera, overlapping at random depths -- through every
+    raster path (per-thread, per-warp row spans, tile bins) against the
+    CPU restatement, bit for bit."""
+    import gpu_chain as G
+    rng = np.random.default_rng(100 + seed)
+    nt = 600
+    W, H, V = 173, 131, 2
+    ctr = rng.uniform(-1.2, 1.2, size=(nt, 1, 2))
+    size = np.exp(rng.uniform(np.log(0.002), np.log(1.5), size=(nt, 1, 1)))
+    pts = ctr + size * rng.normal(size=(nt, 3, 2))
+    sliver = rng.random(nt) < 0.3          # long thin triangles
+    pts[sliver, 2] = pts[sliver, 0] + (pts[sliver, 1] - pts[sliver, 0]) * rng.uniform(0.2, 0.8, size=(sliver.sum(), 1)) \
+        + rng.normal(scale=1e-3, size=(sliver.sum(), 2))
+    w = rng.uniform(0.3, 3.0, size=(nt, 3))
+    w[rng.random((nt, 3)) < 0.03] *= -1     # a few vertices behind the camera
+    z = rng.uniform(-1.0, 1.0, size=(nt, 3))
+    clip1 = np.concatenate([pts * w[..., None], (z * w)[..., None], w[..., None]], axis=-1).reshape(-1, 4)
+    clip = np.stack([clip1, clip1[::-1].copy()]).astype(np.float32)   # second view: same points, other order
+    nv = nt * 3
+    tri = np.arange(nv, dtype=np.uint32).reshape(nt, 3)
+    N = W * H * V
+    r = np.zeros((N, 4), np.float32); d = np.zeros((N, 4), np.float32)
+    O.orc().rasterize_fwd(W, H, V, clip.reshape(-1, 4), nv, tri, nt, 1, r, d)
+    assert (r[:, 3] > 0).sum() > 1000
+    ctx.set_raster_areas(*areas)
+    try:
+        for tile in (8, 16, 32):
+            ctx.set_raster_config(tile, 0)
+            gr = G.zeros(N, 4); gd = G.zeros(N, 4)
+            ctx.rasterize_fwd(G.dev(clip.reshape(-1, 4)), nv, G.dev(tri.astype(np.int32)), nt, W, H, V, gr, gd, None)
+            assert np.array_equal(G.host(gr), r), (areas, tile)
+            assert np.array_equal(G.host(gd), d), (areas, tile)
+    finally:
+        ctx.set_raster_config(16, 0)
+        ctx.set_raster_areas(-1, -1)

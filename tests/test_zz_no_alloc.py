@@ -72,11 +72,13 @@ def test_static_scratch_bins_overflow_to_exact_result(ctx):
     S = _scenes()[1]
     wr, wd = _raster(ctx, S, "rasterize_fwd")
     ctx.set_raster_config(16, 1)
+    ctx.set_raster_areas(0, 0)      # every triangle through the bins
     try:
         gr, gd = _raster(ctx, S, "rasterize_fwd_static")
         assert ctx.raster_overflow_count() > 0
     finally:
         ctx.set_raster_config(16, 0)
+        ctx.set_raster_areas(-1, -1)
     assert np.array_equal(gr, wr)
     assert np.array_equal(gd, wd)
 

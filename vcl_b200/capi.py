@@ -28,6 +28,7 @@ SIGNATURES = {
     "vcl_set_mode": (c_int, [P, c_int]),
     "vcl_get_mode": (c_int, [P]),
     "vcl_set_raster_config": (c_int, [P, c_int, c_ll]),
+    "vcl_set_raster_areas": (c_int, [P, c_int, c_int]),
     "vcl_get_raster_config": (c_int, [P, ctypes.POINTER(c_int), ctypes.POINTER(c_ll)]),
     "vcl_raster_overflow_count": (c_int, [P, P, ctypes.POINTER(c_ll)]),
     "vcl_check_indices": (c_int, [P, P, ctypes.POINTER(c_int)]),

@@ -15,6 +15,8 @@ struct vcl_ctx {
     // raster binning schedule
     int tile = 16;
     long long bin_capacity = 0;   // 0 = automatic
+    int small_area = -1;          // direct-raster box areas, -1 = defaults
+    int med_area = -1;
     // raster workspace (grown on demand, owned here)
     void* ws = nullptr;
     size_t ws_bytes = 0;

@@ -102,6 +102,14 @@ VCL_API vcl_status vcl_set_raster_config(vcl_ctx* ctx, int tile, long long bin_c
     return VCL_OK;
 }
 
+VCL_API vcl_status vcl_set_raster_areas(vcl_ctx* ctx, int small_area, int medium_area) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(small_area >= -1 && medium_area >= -1, "areas must be >= 0, or -1 for the defaults");
+    ctx->small_area = small_area;
+    ctx->med_area = medium_area;
+    return VCL_OK;
+}
+
 VCL_API vcl_status vcl_get_raster_config(const vcl_ctx* ctx, int* tile, long long* bin_capacity) {
     if (!ctx) return VCL_ERR_ARG;
     if (tile) *tile = ctx->tile;

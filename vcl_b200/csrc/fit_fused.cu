@@ -39,7 +39,7 @@ namespace {
 struct Fused {
     void* raster_ws = nullptr;
     size_t raster_ws_bytes = 0;
-    RasterSched sched{16, 0, 0};
+    RasterSched sched{16, 0, 0, 0};
     bool sched_cached = false;                 // schedule taken from the tuning cache
     int* flags = nullptr;                      // [0] overflowed raster tiles of the last step
     int* d_step = nullptr;
@@ -582,7 +582,7 @@ vcl_status autotune_raster(vcl_fit* f) {
         if (it != g_tune.end()) {
             long long cap = (long long)(it->second.cap_per_tri * d.views * d.nt);
             if (cap < cap_floor(d, it->second.tile)) cap = cap_floor(d, it->second.tile);
-            F->sched = RasterSched{it->second.tile, cap, it->second.small_area};
+            F->sched = RasterSched{it->second.tile, cap, it->second.small_area, raster_default_medium_area()};
             for (int i = 0; i < 3; ++i) F->tune_ms[i] = it->second.ms[i];
             F->sched_cached = true;
             return raster_ws_ensure(f, raster_ws_size(d.W, d.H, d.views, d.nt, F->sched.tile, cap));
@@ -609,7 +609,7 @@ vcl_status autotune_raster(vcl_fit* f) {
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
         return vcl_fail(ctx, VCL_ERR_CUDA, "autotune events");
     float best = 1e30f;
-    RasterSched pick{16, cap, raster_default_small_area()};
+    RasterSched pick{16, cap, raster_default_small_area(), raster_default_medium_area()};
     for (int i = 0; i < 3; ++i) F->tune_ms[i] = 1e30f;
     auto time_sched = [&](const RasterSched& rs, float& ms) -> vcl_status {
         vcl_status r = VCL_OK;
@@ -627,7 +627,7 @@ vcl_status autotune_raster(vcl_fit* f) {
     };
     // tile edge at the default direct area, then the direct area at that tile
     for (int ti = 0; ti < 3 && st == VCL_OK; ++ti) {
-        RasterSched rs{tiles[ti], cap, raster_default_small_area()};
+        RasterSched rs{tiles[ti], cap, raster_default_small_area(), raster_default_medium_area()};
         float ms = 0.f;
         st = time_sched(rs, ms);
         F->tune_ms[ti] = ms;
@@ -635,7 +635,7 @@ vcl_status autotune_raster(vcl_fit* f) {
     }
     for (int sa : smalls) {
         if (st || sa == raster_default_small_area()) continue;
-        RasterSched rs{pick.tile, cap, sa};
+        RasterSched rs{pick.tile, cap, sa, raster_default_medium_area()};
         float ms = 0.f;
         st = time_sched(rs, ms);
         if (!st && ms < best) { best = ms; pick = rs; }

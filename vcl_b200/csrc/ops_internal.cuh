@@ -23,8 +23,12 @@ struct RasterSched {
     int tile;
     long long cap;
     int small_area;
+    int med_area;    // box area (pixels) up to which a triangle is rasterized by one warp
 };
 int raster_default_small_area();
+int raster_default_medium_area();
+// The context's schedule: tile, capacity, and its direct-raster areas.
+RasterSched ctx_sched(const vcl_ctx* ctx, int tile, long long cap);
 // `flags[0]` receives the number of tiles whose bins overflowed.
 vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* flags, const float* clip, int nv,
                          const uint32_t* tri, int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s);

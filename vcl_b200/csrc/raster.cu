@@ -48,8 +48,10 @@ struct __align__(16) RTri {
 };
 
 constexpr int CHUNK = 128;
-// default box area (pixels) up to which a triangle is rasterized by its setup thread
+// default box areas (pixels): up to SMALL_AREA a triangle is rasterized by its
+// setup thread, up to MEDIUM_AREA by one warp, above that through the bins
 constexpr int SMALL_AREA = 256;
+constexpr int MEDIUM_AREA = 4096;
 constexpr unsigned long long KEY_NONE = ~0ull;
 
 // Order-preserving 64-bit key: depth bits (monotone map of the float, -0
@@ -64,7 +66,10 @@ DEV float key_depth(unsigned long long k) {
     u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
     return __uint_as_float(u);
 }
-DEV bool is_small(int4 b, int small_area) { return (long long)(b.y - b.x + 1) * (b.w - b.z + 1) <= small_area; }
+DEV long long box_area(int4 b) { return (long long)(b.y - b.x + 1) * (b.w - b.z + 1); }
+DEV bool is_small(int4 b, int small_area) { return box_area(b) <= small_area; }
+// not binned: rasterized by its setup thread or by a warp
+DEV bool is_direct(int4 b, int small_area, int med_area) { return box_area(b) <= (small_area > med_area ? small_area : med_area); }
 
 // Pixel-centre NDC coordinate (2p+1-W)/W: exact numerator, one rounding.
 DEV float ndc(int p, int W) { return dvd((float)(2 * p + 1 - W), (float)W); }
@@ -119,6 +124,37 @@ DEV bool tile_overlaps(const RTri& r, int tx, int ty, int T, int W, int H) {
     return true;
 }
 
+// Conservative column range [x0, x1] of pixel row `sy` for a triangle: each
+// edge function is linear in sx, so every edge bounds sx from one side.  The
+// bound is relaxed by a margin far above the rounding of the per-pixel edge
+// evaluation and widened by one pixel each way; pixels outside the range
+// cannot be covered, pixels inside still go through the exact test.  False
+// when the row certainly has no covered pixel.
+DEV bool row_span(const RTri& r, float sy, int W, int& x0, int& x1) {
+    const float sg = r.a.w;
+    const float ea[3] = {r.a.x, r.a.y, r.a.z}, eb[3] = {r.b.x, r.b.y, r.b.z}, ek[3] = {r.k.x, r.k.y, r.k.z};
+    float lo = -2.f, hi = 2.f;     // sx range of interest (the screen is [-1, 1])
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float a = sg * ea[i], c = sg * (eb[i] * sy + ek[i]);
+        const float m = 1e-5f * (fabsf(ea[i]) + fabsf(eb[i]) + fabsf(ek[i]));
+        if (a > 0.f) lo = fmaxf(lo, (-c - m) / a);
+        else if (a < 0.f) hi = fminf(hi, (-c - m) / a);
+        else if (c < -m) return false;
+    }
+    if (lo > hi) return false;     // (fmaxf/fminf drop NaN bounds, so lo and hi are numbers)
+    const float fw = (float)W;
+    x0 = max(r.box.x, (int)floorf(fmaf(lo, fw, fw - 1.f) * 0.5f) - 1);
+    x1 = min(r.box.y, (int)ceilf(fmaf(hi, fw, fw - 1.f) * 0.5f) + 1);
+    return x0 <= x1;
+}
+
+// Pixel-centre coordinates of every column and row, staged in shared memory
+// once per block (the exactly rounded divisions of ndc()).
+DEV void stage_ndc(float* tab, int W, int H) {
+    for (int i = threadIdx.x; i < W + H; i += blockDim.x) tab[i] = i < W ? ndc(i, W) : ndc(i - W, H);
+}
+
 DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool& valid) {
     float x0 = c0.x, y0 = c0.y, x1 = c1.x, y1 = c1.y, x2 = c2.x, y2 = c2.y;
     float w0 = c0.w, w1 = c1.w, w2 = c2.w;
@@ -158,7 +194,11 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
 
 __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W, int H,
                         int views, int tile, int tiles_x, int ntiles, RTri* __restrict__ setup, int* __restrict__ count,
-                        int* __restrict__ flags, unsigned long long* __restrict__ keys, int small_area) {
+                        int* __restrict__ flags, unsigned long long* __restrict__ keys, int small_area, int med_area,
+                        int* __restrict__ med_list, int* __restrict__ med_count) {
+    extern __shared__ float s_ndc[];   // [W] column centres, [H] row centres
+    stage_ndc(s_ndc, W, H);
+    __syncthreads();
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
@@ -177,13 +217,19 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
     if (is_small(r.box, small_area)) {
         unsigned long long* kv = keys + (size_t)view * W * H;
         for (int py = r.box.z; py <= r.box.w; ++py) {
-            const float sy = ndc(py, H);
-            for (int px = r.box.x; px <= r.box.y; ++px) {
+            const float sy = s_ndc[W + py];
+            int x0, x1;
+            if (!row_span(r, sy, W, x0, x1)) continue;
+            for (int px = x0; px <= x1; ++px) {
                 float zw;
-                if (pixel_test(r.a, r.b, r.k, r.z, r.w, ndc(px, W), sy, zw))
+                if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
                     atomicMin(&kv[(size_t)py * W + px], depth_key(zw, t));
             }
         }
+        return;
+    }
+    if (box_area(r.box) <= med_area) {
+        med_list[atomicAdd(med_count, 1)] = (int)gid;   // one warp rasterizes it (k_medium)
         return;
     }
     int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
@@ -193,43 +239,39 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
             if (tile_overlaps(r, tx, ty, tile, W, H)) atomicAdd(&cnt[ty * tiles_x + tx], 1);
 }
 
-// Exclusive scan of n ints by one CTA of 1024 threads (chunked).
+// Exclusive scan of n ints by one CTA of 1024 threads: each thread sums a
+// contiguous run, the run sums are scanned across the block, each thread
+// writes its run.
 __global__ void k_scan(const int* __restrict__ in, int* __restrict__ out, int n) {
     __shared__ int warp_sums[32];
-    __shared__ int carry;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    if (tid == 0) carry = 0;
+    const int per = (n + 1023) / 1024;
+    const int beg = min(tid * per, n), end = min(beg + per, n);
+    int sum = 0;
+    for (int i = beg; i < end; ++i) sum += in[i];
+    int x = sum;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) warp_sums[wid] = x;
     __syncthreads();
-    for (int base = 0; base < n; base += 1024) {
-        int i = base + tid;
-        int v = i < n ? in[i] : 0;
-        int x = v;
-        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
-        if (lane == 31) warp_sums[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            int s = warp_sums[lane];
-            for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, s, o); if (lane >= o) s += y; }
-            warp_sums[lane] = s;
-        }
-        __syncthreads();
-        int excl = carry + (wid ? warp_sums[wid - 1] : 0) + x - v;
-        if (i < n) out[i] = excl;
-        __syncthreads();
-        if (tid == 1023) carry = excl + v;
-        __syncthreads();
+    if (wid == 0) {
+        int v = warp_sums[lane];
+        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
+        warp_sums[lane] = v;
     }
+    __syncthreads();
+    int excl = (wid ? warp_sums[wid - 1] : 0) + x - sum;
+    for (int i = beg; i < end; ++i) { out[i] = excl; excl += in[i]; }
 }
 
 __global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int W, int H, int tile, int tiles_x,
                        int ntiles, const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list,
-                       long long cap, int small_area) {
+                       long long cap, int small_area, int med_area) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long long)views * nt) return;
     int view = (int)(gid / nt), t = (int)(gid % nt);
     const RTri r = setup[gid];
     const int4 box = r.box;
-    if (box.x > box.y || box.z > box.w || is_small(box, small_area)) return;
+    if (box.x > box.y || box.z > box.w || is_direct(box, small_area, med_area)) return;
     int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
@@ -271,7 +313,7 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
                                                 const int* __restrict__ offset, const int* __restrict__ list,
                                                 long long cap, int nt, int W, int H, int tiles_x, int ntiles,
                                                 unsigned long long* __restrict__ keys, int* __restrict__ flags,
-                                                int small_area) {
+                                                int small_area, int med_area) {
     __shared__ RTri s_tri[CHUNK];
     __shared__ int s_id[CHUNK];
     const int view = blockIdx.y, tile_id = blockIdx.x;
@@ -296,7 +338,7 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
             s_id[tid] = t;
             s_tri[tid] = vs[t];
             // in the all-triangles fallback the small ones are done already
-            if (overflow && is_small(s_tri[tid].box, small_area)) s_tri[tid].box = make_int4(1, 0, 1, 0);
+            if (overflow && is_direct(s_tri[tid].box, small_area, med_area)) s_tri[tid].box = make_int4(1, 0, 1, 0);
         }
         __syncthreads();
         const int m = min(CH, n_iter - i0);
@@ -314,6 +356,40 @@ __global__ void __launch_bounds__(T * T) k_fine(const RTri* __restrict__ setup, 
     }
     if (overflow && tid == 0) atomicAdd(&flags[0], 1);
     if (inside && best != KEY_NONE) atomicMin(&keys[((size_t)view * H + py) * W + px], best);
+}
+
+// Medium triangles: one warp per triangle, one lane per pixel row of its
+// box; a lane tests the pixels of its row's conservative span and keeps the
+// nearest (depth, id) per pixel with a 64-bit atomicMin (same coverage and
+// depth arithmetic as the other paths).  Persistent warps stride over the
+// list the setup pass filled.
+__global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, int nt, int W, int H,
+                                                const int* __restrict__ med_list, const int* __restrict__ med_count,
+                                                unsigned long long* __restrict__ keys) {
+    extern __shared__ float s_ndc[];   // [W] column centres, [H] row centres
+    stage_ndc(s_ndc, W, H);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    const int n = *med_count;
+    for (int i = warp; i < n; i += nwarps) {
+        const int gid = med_list[i];
+        const int view = gid / nt, t = gid - view * nt;
+        const RTri r = setup[gid];
+        unsigned long long* kv = keys + (size_t)view * W * H;
+        // lane per row; each lane walks only its row's conservative span
+        for (int py = r.box.z + lane; py <= r.box.w; py += 32) {
+            const float sy = s_ndc[W + py];
+            int x0, x1;
+            if (!row_span(r, sy, W, x0, x1)) continue;
+            for (int px = x0; px <= x1; ++px) {
+                float zw;
+                if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
+                    atomicMin(&kv[(size_t)py * W + px], depth_key(zw, t));
+            }
+        }
+    }
 }
 
 // Winning key -> (u, v, z/w, id+1) and DB per pixel.
@@ -396,7 +472,8 @@ __global__ void k_raster_bwd(const float* __restrict__ clip, int nv, const uint3
 struct RasterWS {
     unsigned long long* keys;
     RTri* setup;
-    int* count;
+    int* med_list;     // [views * nt] medium triangles (view * nt + t)
+    int* count;        // [ntiles + 1]; count[ntiles] = number of medium triangles
     int* offset;
     int* cursor;
     int* list;
@@ -412,8 +489,9 @@ long long auto_capacity_(long long views, long long nt, int W, int H, int tile) 
 }
 
 size_t ws_bytes(long long npix, long long views, long long nt, long long ntiles, long long cap) {
-    return align256(sizeof(unsigned long long) * (size_t)npix) +
-           align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1)) + 3 * align256(sizeof(int) * (size_t)ntiles) +
+    const size_t vt = (size_t)(views * nt > 0 ? views * nt : 1);
+    return align256(sizeof(unsigned long long) * (size_t)npix) + align256(sizeof(RTri) * vt) +
+           align256(sizeof(int) * vt) + 3 * align256(sizeof(int) * (size_t)(ntiles + 1)) +
            align256(sizeof(int) * (size_t)cap);
 }
 
@@ -421,10 +499,12 @@ RasterWS carve(void* base, long long npix, long long views, long long nt, long l
     char* p = (char*)base;
     RasterWS w;
     w.keys = (unsigned long long*)p; p += align256(sizeof(unsigned long long) * (size_t)npix);
-    w.setup = (RTri*)p; p += align256(sizeof(RTri) * (size_t)(views * nt > 0 ? views * nt : 1));
-    w.count = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
-    w.offset = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
-    w.cursor = (int*)p; p += align256(sizeof(int) * (size_t)ntiles);
+    const size_t vt = (size_t)(views * nt > 0 ? views * nt : 1);
+    w.setup = (RTri*)p; p += align256(sizeof(RTri) * vt);
+    w.med_list = (int*)p; p += align256(sizeof(int) * vt);
+    w.count = (int*)p; p += align256(sizeof(int) * (size_t)(ntiles + 1));
+    w.offset = (int*)p; p += align256(sizeof(int) * (size_t)(ntiles + 1));
+    w.cursor = (int*)p; p += align256(sizeof(int) * (size_t)(ntiles + 1));
     w.list = (int*)p;
     w.cap = cap;
     return w;
@@ -441,15 +521,16 @@ size_t raster_ws_size(int W, int H, int views, int nt, int tile, long long cap) 
     return ws_bytes((long long)W * H * views, views, nt, ntiles, cap);
 }
 
-int raster_fwd_launches() { return 5; }
+int raster_fwd_launches() { return 6; }
 
 int raster_default_small_area() { return SMALL_AREA; }
+int raster_default_medium_area() { return MEDIUM_AREA; }
 
 vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* flags, const float* clip, int nv,
                          const uint32_t* tri, int nt, int W, int H, int views, float* rast, float* db, cudaStream_t s) {
     const int T = rs.tile;
     const long long cap = rs.cap;
-    const int sa = rs.small_area;
+    const int sa = rs.small_area, ma = rs.med_area;
     const int tiles_x = (W + T - 1) / T, tiles_y = (H + T - 1) / T;
     const long long ntiles_view = (long long)tiles_x * tiles_y;
     const long long ntiles = ntiles_view * views;
@@ -457,7 +538,7 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     RasterWS w = carve(ws, npix, views, nt, ntiles, cap);
     vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(w.keys, 0xff, sizeof(unsigned long long) * npix, s), "raster memset");
     if (st) return st;
-    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * ntiles, s), "raster memset");
+    st = vcl_cuda_check(ctx, cudaMemsetAsync(w.count, 0, sizeof(int) * (ntiles + 1), s), "raster memset");
     if (st) return st;
     st = vcl_cuda_check(ctx, cudaMemsetAsync(w.cursor, 0, sizeof(int) * ntiles, s), "raster memset");
     if (st) return st;
@@ -465,27 +546,39 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     if (st) return st;
     long long work = (long long)views * nt;
     if (work > 0) {
-        k_setup<<<vcl_blocks(work, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
-                                                       (int)ntiles_view, w.setup, w.count, flags, w.keys, sa);
+        const size_t tab = sizeof(float) * (size_t)(W + H);
+        if (tab > 48 * 1024) {
+            cudaFuncSetAttribute(k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+            cudaFuncSetAttribute(k_medium, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+        }
+        k_setup<<<vcl_blocks(work, 256), 256, tab, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
+                                                         (int)ntiles_view, w.setup, w.count, flags, w.keys, sa, ma,
+                                                         w.med_list, w.count + ntiles);
+        k_medium<<<ctx->sm_count * 8, 256, tab, s>>>(w.setup, nt, W, H, w.med_list, w.count + ntiles, w.keys);
     }
     k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
     if (work > 0) {
         k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, W, H, T, tiles_x, (int)ntiles_view,
-                                                      w.offset, w.cursor, w.list, cap, sa);
+                                                      w.offset, w.cursor, w.list, cap, sa, ma);
     }
     dim3 grid((unsigned)ntiles_view, (unsigned)views);
     if (T == 8)
         k_fine<8><<<grid, dim3(8, 8), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                             (int)ntiles_view, w.keys, flags, sa);
+                                             (int)ntiles_view, w.keys, flags, sa, ma);
     else if (T == 16)
         k_fine<16><<<grid, dim3(16, 16), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, w.keys, flags, sa);
+                                               (int)ntiles_view, w.keys, flags, sa, ma);
     else
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
-                                               (int)ntiles_view, w.keys, flags, sa);
+                                               (int)ntiles_view, w.keys, flags, sa, ma);
     k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, (const float4*)clip, nv, tri,
                                                      (float4*)rast, (float4*)db);
     return vcl_launch_check(ctx, "rasterize_fwd");
+}
+
+RasterSched ctx_sched(const vcl_ctx* ctx, int T, long long cap) {
+    return RasterSched{T, cap, ctx->small_area >= 0 ? ctx->small_area : SMALL_AREA,
+                       ctx->med_area >= 0 ? ctx->med_area : MEDIUM_AREA};
 }
 
 vcl_status raster_bin_demand(vcl_ctx* ctx, void* ws, const RasterSched& rs, int W, int H, int views, int nt,
@@ -537,7 +630,7 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     long long cap = ctx->bin_capacity ? ctx->bin_capacity : auto_capacity_(views, nt, W, H, T);
     vcl_status st = vcl_ws_reserve(ctx, ws_bytes((long long)W * H * views, views, nt, ntiles, cap));
     if (st) return st;
-    return raster_fwd_ws(ctx, ctx->ws, RasterSched{T, cap, SMALL_AREA}, ctx->dev_flags, clip, nv, tri, nt, W, H, views,
+    return raster_fwd_ws(ctx, ctx->ws, ctx_sched(ctx, T, cap), ctx->dev_flags, clip, nv, tri, nt, W, H, views,
                          rast, db, s);
 }
 

@@ -97,7 +97,7 @@ VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int
     const size_t fixed = raster_ws_size(W, H, views, nt, T, 0);
     VCL_REQUIRE(fixed <= RASTER_SCRATCH_BYTES,
                 "rasterize_fwd_static: W=%d H=%d views=%d nt=%d needs %zu bytes of scratch "
-                "(8 B per pixel + 80 B per view and triangle + tile counters), the static limit is %zu; "
+                "(8 B per pixel + 84 B per view and triangle + tile counters), the static limit is %zu; "
                 "use vcl_rasterize_fwd",
                 W, H, views, nt, fixed, RASTER_SCRATCH_BYTES);
     const long long want = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(views, nt, W, H, T);
@@ -106,8 +106,8 @@ VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int
     void* scratch = nullptr;
     vcl_status st = scratch_address(ctx, &scratch);
     if (st) return st;
-    return raster_fwd_ws(ctx, scratch, RasterSched{T, cap, raster_default_small_area()}, ctx->dev_flags, clip, nv, tri,
-                         nt, W, H, views, rast, db, (cudaStream_t)stream);
+    return raster_fwd_ws(ctx, scratch, ctx_sched(ctx, T, cap), ctx->dev_flags, clip, nv, tri, nt, W, H, views, rast,
+                         db, (cudaStream_t)stream);
 }
 
 }  // extern "C"
