@@ -42,6 +42,7 @@ struct Fused {
     RasterSched sched{16, 0, 0, 0};
     bool sched_cached = false;                 // schedule taken from the tuning cache
     int* flags = nullptr;                      // [0] overflowed raster tiles of the last step
+    float* scr = nullptr;                      // per view-vertex screen terms for the antialias kernels
     int* d_step = nullptr;
     double* d_corr = nullptr;    // 1 - beta1^t', 1 - beta2^t'
     cudaGraph_t graph_def = nullptr;           // the captured step (child of batch graphs)
@@ -490,6 +491,7 @@ vcl_status fused_init(vcl_fit* f) {
     cudaError_t e = cudaMallocAsync(&F->d_step, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->d_corr, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->flags, 64, as);
+    if (e == cudaSuccess) e = cudaMallocAsync(&F->scr, sizeof(float) * 8 * (size_t)d.views * d.nv, as);
     if (e == cudaSuccess) e = cudaMemsetAsync(F->flags, 0, 64, as);
     if (e == cudaSuccess) e = cudaMemcpyAsync(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice, as);
     if (e == cudaSuccess) e = cudaStreamSynchronize(as);
@@ -735,13 +737,14 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_clip, 0, sizeof(float) * V * d.nv * 4, s), "clear"));
     if (npyr > n0) TRY(vcl_cuda_check(ctx, cudaMemsetAsync(f->g_pyr + n0, 0, sizeof(float) * (npyr - n0), s), "clear"));
     TRY(vcl_project_fwd(ctx, f->mvp, V, f->pos, d.nv, 4, f->clip, s));
+    launch_aa_screen(f->clip, (long long)V * d.nv, W, H, F->scr, s);
     TRY(raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H, V, f->rast, f->db, s));
     const ShadeIn a = shade_in(f);
     const TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
     TRY(stage_shade(f, a, td, s));
-    TRY(aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
+    TRY(aa_edges_fwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
     TRY(stage_mse(f, s));
-    TRY(aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
+    TRY(aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
                      d.learn_pos ? f->g_clip : nullptr, s));
     const bool lobes = d.learn_lobes && d.K;
     // the lobe gradients run beside the per-pixel backward on a forked stream
@@ -842,7 +845,8 @@ vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
 
 int fit_fused_launches(const vcl_fit* f) {
     const vcl_fit_desc& d = f->d;
-    int n = 1 /* begin */ + 1 /* project */ + raster_fwd_launches() + 1 /* shade */ + 1 /* aa */ + 1 /* mse */ +
+    int n = 1 /* begin */ + 1 /* project */ + 1 /* aa screen terms */ + raster_fwd_launches() + 1 /* shade */ +
+            1 /* aa */ + 1 /* mse */ +
             1 /* aa bwd */;
     if (d.learn_tex || d.learn_pos) n += 1; /* per-pixel backward */
     if (d.learn_lobes && d.K) n += 1;       /* lobe gradients */
@@ -868,6 +872,7 @@ void fit_fused_release(vcl_fit* f, cudaStream_t s, bool async) {
     };
     release(F->raster_ws);
     release(F->flags);
+    release(F->scr);
     release(F->d_step);
     release(F->d_corr);
     if (F->side) cudaStreamDestroy(F->side);
@@ -945,9 +950,10 @@ vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* m
                 case 0: return raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H,
                                              V, f->rast, f->db, s);
                 case 1: return stage_shade(f, a, td, s);
-                case 2: return aa_edges_fwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s);
+                case 2: return aa_edges_fwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa,
+                                            s);
                 case 3: return stage_mse(f, s);
-                case 4: return aa_edges_bwd(ctx, f->clip, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
+                case 4: return aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
                                             f->g_color, d.learn_pos ? f->g_clip : nullptr, s);
                 case 5: return stage_bwd_pix(f, a, td, s);
                 default: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;

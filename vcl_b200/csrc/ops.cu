@@ -320,19 +320,43 @@ struct AATri { float2 v[3]; float2 ndc[3]; float iw[3]; uint32_t id[3]; };
 
 // antialias.cu:37-55 / :240-257.  Screen positions use exactly rounded
 // arithmetic so that the edge decisions match the CPU restatement.
-DEV bool aa_fetch(const float4* __restrict__ proj, int nv, const uint32_t* __restrict__ tri, int nt,
-                  const float4* __restrict__ rast, long long pidx, float2 s, float2 f, AATri& t, int* flags) {
+// `scr` (optional): the per-vertex screen terms of this view precomputed by
+// k_aa_screen -- [2v] = ((x/w + 1) s.x, (y/w + 1) s.y, 1/w, -), [2v+1] =
+// (x/w, y/w, -, -) -- with the same rounded operations as computed here.
+DEV bool aa_fetch(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv,
+                  const uint32_t* __restrict__ tri, int nt, const float4* __restrict__ rast, long long pidx, float2 s,
+                  float2 f, AATri& t, int* flags, bool need_ndc) {
     uint32_t i[3];
     if (!tri_ok(rast_id(rast[pidx].w), nt, tri, nv, i[0], i[1], i[2], flags)) return false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        float4 c = proj[i[k]];
         t.id[k] = i[k];
-        t.iw[k] = __fdiv_rn(1.f, c.w);
-        t.ndc[k] = make_float2(mul(c.x, t.iw[k]), mul(c.y, t.iw[k]));
-        t.v[k] = make_float2(sub(mul(add(t.ndc[k].x, 1.f), s.x), f.x), sub(mul(add(t.ndc[k].y, 1.f), s.y), f.y));
+        if (scr) {
+            const float4 S = scr[2 * (size_t)i[k]];
+            t.iw[k] = S.z;
+            if (need_ndc) {
+                const float4 Q = scr[2 * (size_t)i[k] + 1];
+                t.ndc[k] = make_float2(Q.x, Q.y);
+            }
+            t.v[k] = make_float2(sub(S.x, f.x), sub(S.y, f.y));
+        } else {
+            float4 c = proj[i[k]];
+            t.iw[k] = __fdiv_rn(1.f, c.w);
+            t.ndc[k] = make_float2(mul(c.x, t.iw[k]), mul(c.y, t.iw[k]));
+            t.v[k] = make_float2(sub(mul(add(t.ndc[k].x, 1.f), s.x), f.x), sub(mul(add(t.ndc[k].y, 1.f), s.y), f.y));
+        }
     }
     return true;
+}
+
+__global__ void k_aa_screen(const float4* __restrict__ clip, long long n, float sx, float sy, float4* __restrict__ scr) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 c = clip[i];
+    const float iw = __fdiv_rn(1.f, c.w);
+    const float nx = mul(c.x, iw), ny = mul(c.y, iw);
+    scr[2 * i] = make_float4(mul(add(nx, 1.f), sx), mul(add(ny, 1.f), sy), iw, 0.f);
+    scr[2 * i + 1] = make_float4(nx, ny, 0.f, 0.f);
 }
 
 DEV float cross_rn(float ax, float ay, float bx, float by) { return sub(mul(ax, by), mul(ay, bx)); }
@@ -365,9 +389,9 @@ struct AAPair {
     AATri t;
 };
 
-DEV bool aa_pair(const float4* __restrict__ proj, int nv, const uint32_t* __restrict__ tri, int nt,
+DEV bool aa_pair(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv, const uint32_t* __restrict__ tri, int nt,
                  const float4* __restrict__ rast, long long q, int qx, int qy, int W, int dir, bool typo, float2 s,
-                 AAPair& P, int* flags) {
+                 AAPair& P, int* flags, bool need_ndc) {
     const long long oidx = dir == 0 ? q - 1 : q - W;
     const float4 tr = rast[q], to = rast[oidx];
     if (to.w == tr.w) return false;
@@ -379,7 +403,7 @@ DEV bool aa_pair(const float4* __restrict__ proj, int nv, const uint32_t* __rest
     else { f = make_float2((float)qx + .5f, (float)qy + (pp > op ? .5f : -.5f)); P.o = make_float2(0.f, pp > op ? -1.f : 1.f); }
     P.pp = pp;
     P.op = op;
-    return aa_fetch(proj, nv, tri, nt, rast, pp, s, f, P.t, flags);
+    return aa_fetch(proj, scr, nv, tri, nt, rast, pp, s, f, P.t, flags, need_ndc);
 }
 
 // Forward antialias as a gather: each pixel evaluates the (up to four)
@@ -387,7 +411,8 @@ DEV bool aa_pair(const float4* __restrict__ proj, int nv, const uint32_t* __rest
 // (antialias.cu:28-34), in a fixed order -- deterministic, no atomics, and
 // out = in + terms in one pass (the reference's init store, :62-65).
 template <int C4>
-__global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
+__global__ void k_aa_fwd(const float4* __restrict__ clip, const float4* __restrict__ scr_all, int nv,
+                         const uint32_t* __restrict__ tri, int nt,
                          const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
                          float* __restrict__ out, int* flags) {
     long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -398,6 +423,7 @@ __global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t
     int rem = (int)(pidx - view * hw);
     int py = rem / W, px = rem - py * W;
     const float4* proj = clip + (size_t)view * nv;
+    const float4* scr = scr_all ? scr_all + 2 * (size_t)view * nv : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
     float acc[8];
     for (int i = 0; i < C && i < 8; ++i) acc[i] = in[pidx * C + i];
@@ -410,7 +436,7 @@ __global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t
         if (dir == 0 ? (qx == 0 || qx >= W) : (qy == 0 || qy >= H)) continue;
         const long long q = self ? pidx : (dir == 0 ? pidx + 1 : pidx + W);
         AAPair P;
-        if (!aa_pair(proj, nv, tri, nt, rast, q, qx, qy, W, dir, false, s, P, flags)) continue;
+        if (!aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, false, s, P, flags, false)) continue;
         if (P.pp != pidx && P.op != pidx) continue;
 #pragma unroll
         for (int e = 0; e < 3; ++e) {
@@ -435,7 +461,8 @@ __global__ void k_aa_fwd(const float4* __restrict__ clip, int nv, const uint32_t
 // (antialias.cu:216-220, deterministic); clip-position gradients scattered
 // once per pair, by the pair's own pixel q (antialias.cu:222-245).
 template <int C4>
-__global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt,
+__global__ void k_aa_bwd(const float4* __restrict__ clip, const float4* __restrict__ scr_all, int nv,
+                         const uint32_t* __restrict__ tri, int nt,
                          const float4* __restrict__ rast, int W, int H, long long npix, int Cr, const float* __restrict__ in,
                          const float* __restrict__ gout, float* __restrict__ gin, float* __restrict__ gclip, int exact,
                          int* flags) {
@@ -447,6 +474,7 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
     int rem = (int)(pidx - view * hw);
     int py = rem / W, px = rem - py * W;
     const float4* proj = clip + (size_t)view * nv;
+    const float4* scr = scr_all ? scr_all + 2 * (size_t)view * nv : nullptr;
     float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
     float acc[8];
@@ -459,7 +487,7 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, int nv, const uint32_t
         if (dir == 0 ? (qx == 0 || qx >= W) : (qy == 0 || qy >= H)) continue;
         const long long q = self ? pidx : (dir == 0 ? pidx + 1 : pidx + W);
         AAPair P;
-        if (!aa_pair(proj, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags)) continue;
+        if (!aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags, exact && gv)) continue;
         // the reference's horizontal typo can give pp == op: its two colour
         // terms cancel and the clip term is zero (antialias.cu:279, :216-223)
         if (P.pp == P.op) continue;
@@ -565,30 +593,38 @@ int grid_for(long long n, int threads, int sm) {
 
 }  // namespace
 
-vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
-                        int H, int views, int C, const float* in, float* out, cudaStream_t s) {
+vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                        const float* rast, int W, int H, int views, int C, const float* in, float* out, cudaStream_t s) {
     long long npix = (long long)W * H * views;
+    const float4* sc = (const float4*)scr;
     if (C == 4 && aligned16(in) && aligned16(out))
-        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, out, ctx->dev_flags);
+        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                         H, npix, C, in, out, ctx->dev_flags);
     else
-        k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, out, ctx->dev_flags);
+        k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                         H, npix, C, in, out, ctx->dev_flags);
     return vcl_launch_check(ctx, "antialias_fwd");
 }
 
-vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
-                        int H, int views, int C, const float* in, const float* grad_out, float* grad_in,
-                        float* grad_clip, cudaStream_t s) {
+vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                        const float* rast, int W, int H, int views, int C, const float* in, const float* grad_out,
+                        float* grad_in, float* grad_clip, cudaStream_t s) {
     long long npix = (long long)W * H * views;
     int exact = ctx->mode == VCL_MODE_EXACT;
+    const float4* sc = (const float4*)scr;
     if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in))
-        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                         H, npix, C, in, grad_out, grad_in, grad_clip, exact,
+                                                         ctx->dev_flags);
     else
-        k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, nv, tri, nt, (const float4*)rast, W, H,
-                                                         npix, C, in, grad_out, grad_in, grad_clip, exact, ctx->dev_flags);
+        k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                         H, npix, C, in, grad_out, grad_in, grad_clip, exact,
+                                                         ctx->dev_flags);
     return vcl_launch_check(ctx, "antialias_bwd");
+}
+
+void launch_aa_screen(const float* clip, long long n, int W, int H, float* scr, cudaStream_t s) {
+    k_aa_screen<<<vcl_blocks(n, 256), 256, 0, s>>>((const float4*)clip, n, W / 2.f, H / 2.f, (float4*)scr);
 }
 
 void launch_mip_down(const float* src, float* dst, int w, int h, int C, cudaStream_t s) {
@@ -749,7 +785,7 @@ VCL_API vcl_status vcl_antialias_fwd(vcl_ctx* ctx, const float* clip, int nv, co
     VCL_REQUIRE(aligned16(clip) && aligned16(rast), "misaligned buffer");
     VCL_REQUIRE(in != out, "antialias_fwd cannot run in place");
     VCL_REQUIRE(C <= 8, "antialias supports up to 8 channels");
-    return aa_edges_fwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, out, (cudaStream_t)stream);
+    return aa_edges_fwd(ctx, clip, nullptr, nv, tri, nt, rast, W, H, views, C, in, out, (cudaStream_t)stream);
 }
 
 VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
@@ -761,7 +797,7 @@ VCL_API vcl_status vcl_antialias_bwd(vcl_ctx* ctx, const float* clip, int nv, co
     VCL_REQUIRE(aligned16(clip) && aligned16(rast) && aligned16(grad_clip), "misaligned buffer");
     VCL_REQUIRE(grad_in != grad_out, "antialias_bwd cannot run in place");
     VCL_REQUIRE(C <= 8, "antialias supports up to 8 channels");
-    return aa_edges_bwd(ctx, clip, nv, tri, nt, rast, W, H, views, C, in, grad_out, grad_in, grad_clip,
+    return aa_edges_bwd(ctx, clip, nullptr, nv, tri, nt, rast, W, H, views, C, in, grad_out, grad_in, grad_clip,
                         (cudaStream_t)stream);
 }
 

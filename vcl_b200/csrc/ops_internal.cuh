@@ -4,11 +4,14 @@
 
 // Antialias forward / backward (gather form: `out` / `grad_in` are written
 // completely, the reference's initial copy included).
-vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
-                        int H, int views, int C, const float* in, float* out, cudaStream_t s);
-vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, const float* rast, int W,
-                        int H, int views, int C, const float* in, const float* grad_out, float* grad_in,
-                        float* grad_clip, cudaStream_t s);
+vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                        const float* rast, int W, int H, int views, int C, const float* in, float* out, cudaStream_t s);
+vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                        const float* rast, int W, int H, int views, int C, const float* in, const float* grad_out,
+                        float* grad_in, float* grad_clip, cudaStream_t s);
+// Per-vertex screen terms for the antialias kernels (`scr` above, 8 floats
+// per view-vertex; NULL there computes them per pixel pair instead).
+void launch_aa_screen(const float* clip, long long n, int W, int H, float* scr, cudaStream_t s);
 // Mip level l from level l-1 (buffer.cu:449-472).
 void launch_mip_down(const float* src, float* dst, int w, int h, int C, cudaStream_t s);
 
