@@ -69,6 +69,10 @@ VCL_API int vcl_get_mode(const vcl_ctx* ctx);
  * rasterizer configuration of rasterize.cpp:206-254. */
 VCL_API vcl_status vcl_set_raster_config(vcl_ctx* ctx, int tile, long long bin_capacity);
 VCL_API vcl_status vcl_get_raster_config(const vcl_ctx* ctx, int* tile, long long* bin_capacity);
+/* Whether fit jobs of this context time the raster schedules on their first
+ * fused step (1, the default) or take a size-based one (0: tile 32 for
+ * images of at least 512x512, else 16; default direct-raster areas). */
+VCL_API vcl_status vcl_set_raster_autotune(vcl_ctx* ctx, int enable);
 /* Box areas (pixels) below which a triangle skips the tile bins: up to
  * `small_area` it is rasterized by its setup thread, up to `medium_area` by
  * one warp (-1: the defaults 256 and 4096; 0 and 0 bin every triangle). */
@@ -380,6 +384,8 @@ VCL_API vcl_status vcl_batch_remove(vcl_batch* batch, vcl_fit* fit);
 VCL_API int vcl_batch_size(const vcl_batch* batch);
 VCL_API vcl_status vcl_batch_step(vcl_batch* batch, void* stream);
 VCL_API int vcl_batch_launches_per_step(const vcl_batch* batch);
+/* Number of batch-graph rebuilds so far and the host time they took. */
+VCL_API vcl_status vcl_batch_rebuild_stats(const vcl_batch* batch, long long* rebuilds, double* host_ms);
 
 /* -------------------------------------------------------------- serving */
 /* Serving loop: fit jobs are submitted with their host data and an
@@ -410,6 +416,10 @@ VCL_API vcl_status vcl_server_tick(vcl_server* server, void* stream, int* live, 
 VCL_API vcl_status vcl_server_drain(vcl_server* server, void* stream);
 /* The server's clock (ms since creation; the clock of the job times). */
 VCL_API double vcl_server_now_ms(const vcl_server* server);
+/* Host time inside vcl_server_tick with the waits for the device excluded,
+ * the waits, and the batch-graph rebuilds with their host time (ms). */
+VCL_API vcl_status vcl_server_host_stats(const vcl_server* server, double* host_ms, double* wait_ms,
+                                         long long* rebuilds, double* rebuild_ms);
 /* Jobs queued, live or finishing. */
 VCL_API int vcl_server_pending(const vcl_server* server);
 VCL_API vcl_status vcl_server_job_status(const vcl_server* server, long long job_id, int* state, int* iters_done,

@@ -29,6 +29,7 @@ SIGNATURES = {
     "vcl_get_mode": (c_int, [P]),
     "vcl_set_raster_config": (c_int, [P, c_int, c_ll]),
     "vcl_set_raster_areas": (c_int, [P, c_int, c_int]),
+    "vcl_set_raster_autotune": (c_int, [P, c_int]),
     "vcl_get_raster_config": (c_int, [P, ctypes.POINTER(c_int), ctypes.POINTER(c_ll)]),
     "vcl_raster_overflow_count": (c_int, [P, P, ctypes.POINTER(c_ll)]),
     "vcl_check_indices": (c_int, [P, P, ctypes.POINTER(c_int)]),
@@ -88,6 +89,8 @@ SIGNATURES = {
     "vcl_batch_size": (c_int, [P]),
     "vcl_batch_step": (c_int, [P, P]),
     "vcl_batch_launches_per_step": (c_int, [P]),
+    "vcl_batch_rebuild_stats": (c_int, [P, P, P]),
+    "vcl_server_host_stats": (c_int, [P, P, P, P, P]),
     "vcl_server_create": (c_int, [P, c_size, c_int, ctypes.POINTER(c_void_p)]),
     "vcl_server_destroy": (None, [P]),
     "vcl_server_last_error": (c_char_p, [P]),
@@ -455,6 +458,13 @@ class Server:
                 "vcl_server_stats")
         return dict(p50_ms=p50.value, p99_ms=p99.value, iterations=iters.value, completed=comp.value,
                     ticks=ticks.value, resident_bytes=res.value)
+
+    def host_stats(self):
+        h, w, r = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = c_ll()
+        self._c(self.ctx.lib.vcl_server_host_stats(self.h, ctypes.byref(h), ctypes.byref(w), ctypes.byref(n),
+                                                   ctypes.byref(r)), "vcl_server_host_stats")
+        return dict(host_ms=h.value, wait_ms=w.value, rebuilds=n.value, rebuild_ms=r.value)
 
     def close(self):
         if self.h:

@@ -14,6 +14,7 @@
 // Caller rules: a job may belong to one batch at a time; remove it from the
 // batch before destroying it; one host thread drives a batch.
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "fit.cuh"
@@ -25,12 +26,15 @@ struct vcl_batch {
     cudaGraphExec_t exec = nullptr;
     bool dirty = true;
     int mode = -1;
+    long long rebuilds = 0;
+    double rebuild_ms = 0.0;             // host time spent rebuilding the batch graph
 };
 
 namespace {
 
 vcl_status rebuild(vcl_batch* b) {
     vcl_ctx* ctx = b->ctx;
+    const auto t0 = std::chrono::steady_clock::now();
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
     cudaGraph_t parent = nullptr;
     vcl_status st = vcl_cuda_check(ctx, cudaGraphCreate(&parent, 0), "batch graph");
@@ -48,6 +52,8 @@ vcl_status rebuild(vcl_batch* b) {
     if (st) { b->exec = nullptr; return st; }
     b->dirty = false;
     b->mode = ctx->mode;
+    ++b->rebuilds;
+    b->rebuild_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return VCL_OK;
 }
 
@@ -112,6 +118,13 @@ VCL_API vcl_status vcl_batch_step(vcl_batch* b, void* stream) {
     vcl_status st = vcl_cuda_check(ctx, cudaGraphLaunch(b->exec, s), "batch launch");
     if (st) return st;
     for (vcl_fit* f : b->jobs) ++f->step_count;
+    return VCL_OK;
+}
+
+VCL_API vcl_status vcl_batch_rebuild_stats(const vcl_batch* b, long long* rebuilds, double* host_ms) {
+    if (!b) return VCL_ERR_ARG;
+    if (rebuilds) *rebuilds = b->rebuilds;
+    if (host_ms) *host_ms = b->rebuild_ms;
     return VCL_OK;
 }
 

@@ -17,6 +17,7 @@ struct vcl_ctx {
     long long bin_capacity = 0;   // 0 = automatic
     int small_area = -1;          // direct-raster box areas, -1 = defaults
     int med_area = -1;
+    int autotune = 1;             // fit jobs time raster schedules (0: size-based choice)
     // raster workspace (grown on demand, owned here)
     void* ws = nullptr;
     size_t ws_bytes = 0;

@@ -64,6 +64,15 @@ VCL_API vcl_status vcl_create(int device, vcl_ctx** out) {
         delete c;
         return VCL_ERR_NOMEM;
     }
+    // jobs are allocated from the device's default stream-ordered pool; keep
+    // freed blocks in this process's pool for reuse instead of handing them
+    // back to the driver at every synchronization (a per-process attribute)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    (void)cudaGetLastError();
     if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
         cudaFree(c->dev_flags);
         delete c;
@@ -107,6 +116,12 @@ VCL_API vcl_status vcl_set_raster_areas(vcl_ctx* ctx, int small_area, int medium
     VCL_REQUIRE(small_area >= -1 && medium_area >= -1, "areas must be >= 0, or -1 for the defaults");
     ctx->small_area = small_area;
     ctx->med_area = medium_area;
+    return VCL_OK;
+}
+
+VCL_API vcl_status vcl_set_raster_autotune(vcl_ctx* ctx, int enable) {
+    VCL_CTX_CHECK();
+    ctx->autotune = enable ? 1 : 0;
     return VCL_OK;
 }
 

@@ -590,6 +590,14 @@ vcl_status autotune_raster(vcl_fit* f) {
             return raster_ws_ensure(f, raster_ws_size(d.W, d.H, d.views, d.nt, F->sched.tile, cap));
         }
     }
+    if (!ctx->autotune) {
+        // size-based schedule (no timing): large tiles for large images
+        const int t = (d.W >= 512 && d.H >= 512) ? 32 : 16;
+        long long cap = raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
+        F->sched = RasterSched{t, cap, raster_default_small_area(), raster_default_medium_area()};
+        F->sched_cached = false;
+        return raster_ws_ensure(f, raster_ws_size(d.W, d.H, d.views, d.nt, t, cap));
+    }
     const int tiles[3] = {8, 16, 32};
     const int smalls[4] = {0, 64, 256, 1024};
     long long cap = 0;

@@ -90,6 +90,8 @@ struct vcl_server {
     long long iters_total = 0;
     long long ticks = 0;             // ticks launched
     long long done_tick = -1;        // highest tick known to have completed
+    double host_ms = 0.0;            // host time inside ticks, waits excluded
+    double wait_ms = 0.0;            // host time waiting for the previous tick
     std::vector<double> latencies;
     std::string err;
     // set-up worker
@@ -209,7 +211,9 @@ vcl_status collect(vcl_server* s, bool wait) {
 // it or earlier.
 vcl_status observe(vcl_server* s, long long t) {
     if (t <= s->done_tick) return VCL_OK;
+    const double w0 = s->now_ms();
     if (cudaEventSynchronize(s->ev[t & 1]) != cudaSuccess) return fail(s, VCL_ERR_CUDA, "tick wait");
+    s->wait_ms += s->now_ms() - w0;
     s->done_tick = t;
     const double now = s->now_ms();
     for (auto& p : s->finishing)
@@ -234,6 +238,9 @@ VCL_API vcl_status vcl_server_create(vcl_ctx* ctx, size_t budget_bytes, int max_
     vcl_status st = vcl_batch_create(ctx, &s->batch);
     if (!st) st = vcl_create(dev, &s->wctx);
     if (!st) st = vcl_set_mode(s->wctx, vcl_get_mode(ctx));
+    // jobs are set up while other jobs run: timing raster schedules then
+    // measures the other jobs, so the worker uses the size-based schedule
+    if (!st) st = vcl_set_raster_autotune(s->wctx, 0);
     if (!st && cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess) st = VCL_ERR_CUDA;
     for (int i = 0; i < 2 && !st; ++i)
         if (cudaEventCreateWithFlags(&s->ev[i], cudaEventDisableTiming) != cudaSuccess) st = VCL_ERR_CUDA;
@@ -317,8 +324,17 @@ VCL_API vcl_status vcl_server_submit(vcl_server* s, const vcl_fit_desc* desc, co
     return VCL_OK;
 }
 
+vcl_status tick_impl(vcl_server* s, void* stream, int* live_out, int* completed_out);
+
 VCL_API vcl_status vcl_server_tick(vcl_server* s, void* stream, int* live_out, int* completed_out) {
     if (!s) return VCL_ERR_ARG;
+    const double t0 = s->now_ms(), w0 = s->wait_ms;
+    vcl_status st = tick_impl(s, stream, live_out, completed_out);
+    s->host_ms += (s->now_ms() - t0) - (s->wait_ms - w0);
+    return st;
+}
+
+vcl_status tick_impl(vcl_server* s, void* stream, int* live_out, int* completed_out) {
     cudaStream_t cs = (cudaStream_t)stream;
     int completed = 0;
     vcl_status st = VCL_OK;
@@ -400,6 +416,14 @@ VCL_API vcl_status vcl_server_drain(vcl_server* s, void* stream) {
 }
 
 VCL_API double vcl_server_now_ms(const vcl_server* s) { return s ? s->now_ms() : 0.0; }
+
+VCL_API vcl_status vcl_server_host_stats(const vcl_server* s, double* host_ms, double* wait_ms, long long* rebuilds,
+                                         double* rebuild_ms) {
+    if (!s) return VCL_ERR_ARG;
+    if (host_ms) *host_ms = s->host_ms;
+    if (wait_ms) *wait_ms = s->wait_ms;
+    return vcl_batch_rebuild_stats(s->batch, rebuilds, rebuild_ms);
+}
 
 VCL_API int vcl_server_pending(const vcl_server* s) {
     if (!s) return 0;

@@ -12,9 +12,10 @@ serve  Poisson arrivals of fit jobs (rate swept), each job running
        footprint under a 150 GB budget and interleaved by vcl_server_tick;
        p50/p99 latency from arrival to completion and iterations per second.
        Beside it, the same jobs one at a time through the plain pipeline:
-       each job's plain iteration time and set-up time are measured, and the
-       first-come-first-served timeline of one job at a time is computed
-       from those measurements and the same arrival times.
+       every job is run to completion alone (set-up, all its iterations,
+       loss read back) and timed, and the first-come-first-served timeline of
+       one job at a time is computed from those durations and the same
+       arrival times.
 Targets are the true scene rendered on the device plus N(0, 0.05) noise.
 """
 import time
@@ -133,23 +134,17 @@ def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_ran
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     targets = render_targets(ctx, capi, torch, S_list, stream, host=True)
-    # plain, one job at a time: set-up and per-iteration time of every job
-    plain_iter_ms, setup_ms = [], []
-    for S, t in zip(S_list, targets):
+    # plain, one job at a time: every job run to completion (set-up, all its
+    # iterations, the loss read back), timed on the host clock
+    plain_job_ms = []
+    for S, t, n_it in zip(S_list, targets, iters):
         t0 = time.perf_counter()
         f = capi.Fit(ctx, S, strategy=capi.FIT_PLAIN)
         f.set_target(t)
-        stream.synchronize()
-        setup_ms.append((time.perf_counter() - t0) * 1e3)
-        f.step(sh)
-        stream.synchronize()
-        a, b = _events(torch)
-        a.record(stream)
-        for _ in range(2):
+        for _ in range(n_it):
             f.step(sh)
-        b.record(stream)
-        stream.synchronize()
-        plain_iter_ms.append(a.elapsed_time(b) / 2)
+        f.read_loss(sh)
+        plain_job_ms.append((time.perf_counter() - t0) * 1e3)
         f.close()
     out = {"jobs": n_jobs, "iterations_total": int(sum(iters)), "budget_gb": budget_gb, "max_live": max_live,
            "sweep": []}
@@ -178,12 +173,13 @@ def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_ran
             if s["state"] == capi.JOB_DONE:
                 lat.append(s["done_ms"] - (base + arr[i]))
         st = srv.stats()
+        hs = srv.host_stats()
         srv.close()
         # plain one at a time, first come first served
         end, plat = 0.0, []
         for i in range(n_jobs):
             start = max(arr[i], end)
-            end = start + setup_ms[i] + iters[i] * plain_iter_ms[i]
+            end = start + plain_job_ms[i]
             plat.append(end - arr[i])
         span_plain = end - arr[0]
         lat = np.array(lat)
@@ -192,6 +188,7 @@ def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_ran
             "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
             "iters_per_s": st["iterations"] / wall, "ticks": st["ticks"], "wall_s": wall,
+            "host": {k: round(v, 1) for k, v in hs.items()},
             "plain_one_at_a_time": {"p50_ms": float(np.percentile(plat, 50)), "p99_ms": float(np.percentile(plat, 99)),
                                     "iters_per_s": sum(iters) / (span_plain / 1000.0)},
         })
