@@ -382,6 +382,9 @@ VCL_API void vcl_batch_destroy(vcl_batch* batch);
 VCL_API vcl_status vcl_batch_add(vcl_batch* batch, vcl_fit* fit);
 VCL_API vcl_status vcl_batch_remove(vcl_batch* batch, vcl_fit* fit);
 VCL_API int vcl_batch_size(const vcl_batch* batch);
+/* Iterations (1..64) the member advances per vcl_batch_step, chained inside
+ * the batch graph (default 1). */
+VCL_API vcl_status vcl_batch_set_repeat(vcl_batch* batch, vcl_fit* fit, int iterations);
 VCL_API vcl_status vcl_batch_step(vcl_batch* batch, void* stream);
 VCL_API int vcl_batch_launches_per_step(const vcl_batch* batch);
 /* Number of batch-graph rebuilds so far and the host time they took. */

@@ -121,6 +121,30 @@ def test_batch_membership_changes_between_steps(ctx):
         x.close()
 
 
+def test_batch_repeat_runs_several_iterations_per_step(ctx):
+    """A member set to three iterations per batch step advances three
+    iterations each step (chained in the batch graph), the others one."""
+    from vcl_b200 import capi
+    mix = _mix()[:2]
+    want = [_alone(ctx, mix[0], 6), _alone(ctx, mix[1], 2)]
+    batch = capi.Batch(ctx)
+    st = torch.cuda.Stream()
+    f = [capi.Fit(ctx, S) for S in mix]
+    for x, S in zip(f, mix):
+        x.set_target(_target(S))
+        batch.add(x)
+    batch.set_repeat(f[0], 3)
+    assert batch.launches_per_step() == 3 * f[0].launches_per_step() + f[1].launches_per_step()
+    batch.step(st.cuda_stream)
+    batch.step(st.cuda_stream)
+    for S, x, w, n in zip(mix, f, want, (6, 2)):
+        got = (x.read_loss(st.cuda_stream),) + x.read_params(st.cuda_stream)
+        _compare(S, got, w, n)
+    batch.close()
+    for x in f:
+        x.close()
+
+
 def test_server_results_same_alone_and_in_mix(ctx):
     """Jobs submitted together, admitted under a budget that holds only part
     of them at once, interleaved in batched ticks: each job's final

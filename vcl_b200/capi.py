@@ -87,6 +87,7 @@ SIGNATURES = {
     "vcl_batch_add": (c_int, [P, P]),
     "vcl_batch_remove": (c_int, [P, P]),
     "vcl_batch_size": (c_int, [P]),
+    "vcl_batch_set_repeat": (c_int, [P, P, c_int]),
     "vcl_batch_step": (c_int, [P, P]),
     "vcl_batch_launches_per_step": (c_int, [P]),
     "vcl_batch_rebuild_stats": (c_int, [P, P, P]),
@@ -363,6 +364,9 @@ class Batch:
 
     def step(self, stream=None):
         self.ctx._check(self.ctx.lib.vcl_batch_step(self.h, stream), "vcl_batch_step")
+
+    def set_repeat(self, fit, iterations):
+        self.ctx._check(self.ctx.lib.vcl_batch_set_repeat(self.h, fit.h, int(iterations)), "vcl_batch_set_repeat")
 
     def launches_per_step(self):
         return self.ctx.lib.vcl_batch_launches_per_step(self.h)

@@ -11,6 +11,10 @@
 // arithmetic mode changes.  Each job's step counter lives on the device, so
 // replaying the graph advances every job by exactly one iteration.
 //
+// A member may run several iterations per batch step (vcl_batch_set_repeat):
+// its step graph appears as a chain of child nodes, so small jobs need not
+// advance at the pace of the largest one.
+//
 // Caller rules: a job may belong to one batch at a time; remove it from the
 // batch before destroying it; one host thread drives a batch.
 #include <algorithm>
@@ -22,6 +26,7 @@
 struct vcl_batch {
     vcl_ctx* ctx = nullptr;
     std::vector<vcl_fit*> jobs;
+    std::vector<int> reps;               // iterations per batch step of each job
     cudaStream_t capture = nullptr;      // stream the member graphs are captured on
     cudaGraphExec_t exec = nullptr;
     bool dirty = true;
@@ -39,13 +44,19 @@ vcl_status rebuild(vcl_batch* b) {
     cudaGraph_t parent = nullptr;
     vcl_status st = vcl_cuda_check(ctx, cudaGraphCreate(&parent, 0), "batch graph");
     if (st) return st;
-    for (vcl_fit* f : b->jobs) {
+    for (size_t i = 0; i < b->jobs.size() && !st; ++i) {
         cudaGraph_t g = nullptr;
-        st = fit_fused_graph(f, b->capture, &g);
+        st = fit_fused_graph(b->jobs[i], b->capture, &g);
         if (st) break;
-        cudaGraphNode_t node;
-        st = vcl_cuda_check(ctx, cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, g), "batch child graph");
-        if (st) break;
+        // a job with several iterations per step: its step graph repeated as
+        // a chain of child nodes
+        cudaGraphNode_t prev = nullptr;
+        for (int r = 0; r < b->reps[i] && !st; ++r) {
+            cudaGraphNode_t node;
+            st = vcl_cuda_check(ctx, cudaGraphAddChildGraphNode(&node, parent, prev ? &prev : nullptr, prev ? 1 : 0, g),
+                                "batch child graph");
+            prev = node;
+        }
     }
     if (!st) st = vcl_cuda_check(ctx, cudaGraphInstantiate(&b->exec, parent, 0), "batch graph instantiate");
     cudaGraphDestroy(parent);
@@ -88,6 +99,7 @@ VCL_API vcl_status vcl_batch_add(vcl_batch* b, vcl_fit* f) {
     vcl_status st = vcl_fit_set_strategy(f, VCL_FIT_FUSED);
     if (st) return st;
     b->jobs.push_back(f);
+    b->reps.push_back(1);
     b->dirty = true;
     return VCL_OK;
 }
@@ -97,8 +109,23 @@ VCL_API vcl_status vcl_batch_remove(vcl_batch* b, vcl_fit* f) {
     vcl_ctx* ctx = b->ctx;
     auto it = std::find(b->jobs.begin(), b->jobs.end(), f);
     VCL_REQUIRE(it != b->jobs.end(), "job is not in the batch");
+    b->reps.erase(b->reps.begin() + (it - b->jobs.begin()));
     b->jobs.erase(it);
     b->dirty = true;
+    return VCL_OK;
+}
+
+VCL_API vcl_status vcl_batch_set_repeat(vcl_batch* b, vcl_fit* f, int iterations) {
+    if (!b) return VCL_ERR_ARG;
+    vcl_ctx* ctx = b->ctx;
+    VCL_REQUIRE(iterations >= 1 && iterations <= 64, "iterations per step must be 1..64 (got %d)", iterations);
+    auto it = std::find(b->jobs.begin(), b->jobs.end(), f);
+    VCL_REQUIRE(it != b->jobs.end(), "job is not in the batch");
+    int& r = b->reps[it - b->jobs.begin()];
+    if (r != iterations) {
+        r = iterations;
+        b->dirty = true;
+    }
     return VCL_OK;
 }
 
@@ -117,7 +144,7 @@ VCL_API vcl_status vcl_batch_step(vcl_batch* b, void* stream) {
     }
     vcl_status st = vcl_cuda_check(ctx, cudaGraphLaunch(b->exec, s), "batch launch");
     if (st) return st;
-    for (vcl_fit* f : b->jobs) ++f->step_count;
+    for (size_t i = 0; i < b->jobs.size(); ++i) b->jobs[i]->step_count += b->reps[i];
     return VCL_OK;
 }
 
@@ -131,7 +158,7 @@ VCL_API vcl_status vcl_batch_rebuild_stats(const vcl_batch* b, long long* rebuil
 VCL_API int vcl_batch_launches_per_step(const vcl_batch* b) {
     if (!b) return 0;
     int n = 0;
-    for (const vcl_fit* f : b->jobs) n += fit_fused_launches(f);
+    for (size_t i = 0; i < b->jobs.size(); ++i) n += b->reps[i] * fit_fused_launches(b->jobs[i]);
     return n;
 }
 

@@ -12,8 +12,10 @@
 //               slot is free, reserving the footprint and handing the job to
 //               the set-up worker;
 //            3. moves the jobs the worker has set up into the batch;
-//            4. advances every live job by one iteration with ONE batched
-//               launch (vcl_batch_step) and records an event;
+//            4. advances every live job with ONE batched launch
+//               (vcl_batch_step) -- one iteration for the largest jobs, up
+//               to 8 for jobs with a fraction of their pixels -- and records
+//               an event;
 //            5. waits for the PREVIOUS tick's event, so that one tick is
 //               always queued behind the running one.
 //   worker   a host thread with its own context on the same device: creates
@@ -26,6 +28,7 @@
 // = completion - submission on the host's steady clock.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -52,6 +55,7 @@ struct Job {
     std::vector<float> pos, uv, normal, tex, axis, sharp, amp, mvp, pvinv, rot, target;
     std::vector<uint32_t> tri;
     int iters = 0, done = 0;
+    int rep = 1;                     // iterations per tick
     size_t footprint = 0;
     double t_submit = 0, t_admit = -1, t_done = -1;
     int state = QUEUED;
@@ -106,6 +110,12 @@ struct vcl_server {
 };
 
 namespace {
+
+constexpr int MAX_REPEAT = 8;
+
+// Relative device work of one iteration: pixels, plus a constant for the
+// per-iteration launches of a small job.
+double job_cost(const vcl_fit_desc& d) { return (double)d.W * d.H * d.views + 65536.0; }
 
 vcl_status fail(vcl_server* s, vcl_status code, const std::string& msg) {
     s->err = msg;
@@ -370,17 +380,30 @@ vcl_status tick_impl(vcl_server* s, void* stream, int* live_out, int* completed_
     const bool idle = s->live.empty() && s->in_setup > 0 && s->done_tick == s->ticks - 1;
     vcl_status r = collect(s, idle);
     if (r) return r;
-    // 4. one batched iteration of every live job
+    // 4. one batched launch advances every live job; a job whose per-pixel
+    //    work is a fraction of the largest live job's runs several
+    //    iterations in it (at most MAX_REPEAT, never past its count)
     if (!s->live.empty()) {
+        double big = 0.0;
+        for (Job* j : s->live) big = std::max(big, job_cost(j->d));
+        for (Job* j : s->live) {
+            int k = (int)std::min<double>(MAX_REPEAT, std::max(1.0, std::floor(big / job_cost(j->d))));
+            k = std::min(k, j->iters - j->done);
+            if (k != j->rep) {
+                r = vcl_batch_set_repeat(s->batch, j->fit, k);
+                if (r) return fit_error(s, s->ctx, r, "batch repeat");
+                j->rep = k;
+            }
+        }
         const long long t = s->ticks;
         r = vcl_batch_step(s->batch, cs);
         if (r) return fit_error(s, s->ctx, r, "batch step");
         if (cudaEventRecord(s->ev[t & 1], cs) != cudaSuccess) return fail(s, VCL_ERR_CUDA, "tick event");
         ++s->ticks;
-        s->iters_total += (long long)s->live.size();
         std::vector<Job*> still;
         for (Job* j : s->live) {
-            if (++j->done >= j->iters) {
+            s->iters_total += j->rep;
+            if ((j->done += j->rep) >= j->iters) {
                 vcl_batch_remove(s->batch, j->fit);
                 s->finishing.push_back({j, t});
             } else {
