@@ -367,6 +367,45 @@ VCL_API size_t vcl_fit_footprint(const vcl_fit_desc* desc);
  * strategy (memsets and copies not counted). */
 VCL_API int vcl_fit_launches_per_step(const vcl_fit* fit);
 
+/* --------------------------------------------------------------- assets */
+/* Wavefront OBJ (Attribute::loadOBJ, buffer.cu:203-306): `v`, `vt`, `vn`
+ * and `f` lines with corners p, p/t, p//n or p/t/n (1-based, negative =
+ * from the end); polygons are split into triangle fans; other statements
+ * are skipped.  The result keeps one index array per attribute, as the
+ * reference does (absent attributes: NULL arrays), and a welded form with
+ * one vertex per distinct (position, texel, normal) corner and one shared
+ * index array, the layout of vcl_fit_desc (missing texels / normals are 0).
+ * Arrays are host memory owned by the object until vcl_obj_free.  The
+ * loaders need no device; `ctx` may be NULL, and the message of a failed
+ * load is also kept per thread in vcl_asset_error(). */
+typedef struct vcl_obj vcl_obj;
+VCL_API const char* vcl_asset_error(void);
+VCL_API vcl_status vcl_obj_load(vcl_ctx* ctx, const char* path, vcl_obj** out);
+VCL_API void vcl_obj_free(vcl_obj* obj);
+VCL_API vcl_status vcl_obj_counts(const vcl_obj* obj, int* n_pos, int* n_tri, int* n_texel, int* n_normal,
+                                  int* n_welded);
+VCL_API vcl_status vcl_obj_arrays(const vcl_obj* obj, const float** pos, const uint32_t** pos_idx,
+                                  const float** texel, const uint32_t** texel_idx, const float** normal,
+                                  const uint32_t** normal_idx);
+VCL_API vcl_status vcl_obj_welded(const vcl_obj* obj, const float** pos, const float** uv, const float** normal,
+                                  const uint32_t** tri);
+/* BMP (Texture::loadBMP, buffer.cu:498-541): 8-, 24- or 32-bit uncompressed
+ * pixels to floats in [0, 1], [height][width][channels], rows bottom-up as
+ * the file stores them, channels in reverse byte order within a pixel as
+ * the reference converts them (24-bit BGR gives RGB).  Rows are read with
+ * their 4-byte padding (the reference reads them unpadded, which agrees
+ * when width x channels is a multiple of 4); top-down (negative height)
+ * files are flipped to bottom-up.  With out = NULL only the size is
+ * returned. */
+VCL_API vcl_status vcl_bmp_load(vcl_ctx* ctx, const char* path, int* width, int* height, int* channels, float* out);
+/* Spherical-Gaussian lobe list (SGBuffer::loadTXT, buffer.cu:706-732):
+ * whitespace-separated records of 7 numbers -- axis x y z, sharpness,
+ * amplitude r g b -- until the end of the file (the reference reads exactly
+ * 256).  *lobes = records in the file; with axis = NULL only the count is
+ * returned, else at most max_lobes records are stored (more is an error). */
+VCL_API vcl_status vcl_sg_load(vcl_ctx* ctx, const char* path, int max_lobes, int* lobes, float* axis,
+                               float* sharpness, float* amplitude);
+
 /* ------------------------------------------------------------- batches */
 /* Batched engine: resident fit jobs of any sizes advanced together, one
  * iteration each per vcl_batch_step, as ONE CUDA graph launch.  Every member

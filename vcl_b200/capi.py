@@ -82,6 +82,14 @@ SIGNATURES = {
     "vcl_fit_kernel_count": (c_int, []),
     "vcl_fit_kernel_name": (c_char_p, [c_int]),
     "vcl_fit_time_kernels": (c_int, [P, P, c_int, P, c_int]),
+    "vcl_asset_error": (c_char_p, []),
+    "vcl_obj_load": (c_int, [P, c_char_p, ctypes.POINTER(c_void_p)]),
+    "vcl_obj_free": (None, [P]),
+    "vcl_obj_counts": (c_int, [P, P, P, P, P, P]),
+    "vcl_obj_arrays": (c_int, [P, P, P, P, P, P, P]),
+    "vcl_obj_welded": (c_int, [P, P, P, P, P]),
+    "vcl_bmp_load": (c_int, [P, c_char_p, P, P, P, P]),
+    "vcl_sg_load": (c_int, [P, c_char_p, c_int, P, P, P, P]),
     "vcl_batch_create": (c_int, [P, ctypes.POINTER(c_void_p)]),
     "vcl_batch_destroy": (None, [P]),
     "vcl_batch_add": (c_int, [P, P]),
@@ -480,3 +488,89 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ assets
+class _Loader:
+    """Runs loader calls (no device needed) and raises with their message."""
+
+    def __init__(self, ctx):
+        self.lib = lib()
+        self.h = ctx.h if ctx is not None else None
+
+    def check(self, st, name):
+        if st:
+            msg = self.lib.vcl_asset_error()
+            raise VclError(f"{name} failed (status {st}): {msg.decode() if msg else ''}")
+
+    def close(self):
+        pass
+
+
+def load_obj(path, ctx=None):
+    """OBJ mesh: dict with the file's arrays (pos, pos_idx, texel, texel_idx,
+    normal, normal_idx; absent attributes None) and the welded arrays
+    (w_pos, w_uv, w_normal, w_tri) with one shared index."""
+    import numpy as np
+    ld = _Loader(ctx)
+    L = ld.lib
+    try:
+        o = c_void_p()
+        ld.check(L.vcl_obj_load(ld.h, str(path).encode(), ctypes.byref(o)), "vcl_obj_load")
+        cnt = [ctypes.c_int() for _ in range(5)]
+        L.vcl_obj_counts(o, *[ctypes.byref(c) for c in cnt])
+        npos, ntri, ntex, nnrm, nw = [c.value for c in cnt]
+        ptr = [c_void_p() for _ in range(6)]
+        L.vcl_obj_arrays(o, *[ctypes.byref(p) for p in ptr])
+        wp = [c_void_p() for _ in range(4)]
+        L.vcl_obj_welded(o, *[ctypes.byref(p) for p in wp])
+
+        def arr(p, n, cols, dt):
+            if not p.value or n == 0:
+                return None
+            ct = ctypes.c_float if dt == np.float32 else ctypes.c_uint32
+            return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ct)), shape=(n, cols)).copy()
+
+        out = dict(pos=arr(ptr[0], npos, 3, np.float32), pos_idx=arr(ptr[1], ntri, 3, np.uint32),
+                   texel=arr(ptr[2], ntex, 2, np.float32), texel_idx=arr(ptr[3], ntri if ntex else 0, 3, np.uint32),
+                   normal=arr(ptr[4], nnrm, 3, np.float32), normal_idx=arr(ptr[5], ntri if nnrm else 0, 3, np.uint32),
+                   w_pos=arr(wp[0], nw, 3, np.float32), w_uv=arr(wp[1], nw, 2, np.float32),
+                   w_normal=arr(wp[2], nw, 3, np.float32), w_tri=arr(wp[3], ntri, 3, np.uint32))
+        L.vcl_obj_free(o)
+        return out
+    finally:
+        ld.close()
+
+
+def load_bmp(path, ctx=None):
+    """BMP image as float32 [height][width][channels] in [0, 1], rows bottom-up."""
+    import numpy as np
+    ld = _Loader(ctx)
+    L = ld.lib
+    try:
+        w, h, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ld.check(L.vcl_bmp_load(ld.h, str(path).encode(), ctypes.byref(w), ctypes.byref(h), ctypes.byref(c), None),
+                 "vcl_bmp_load")
+        out = np.zeros((h.value, w.value, c.value), np.float32)
+        ld.check(L.vcl_bmp_load(ld.h, str(path).encode(), ctypes.byref(w), ctypes.byref(h), ctypes.byref(c),
+                                out.ctypes.data), "vcl_bmp_load")
+        return out
+    finally:
+        ld.close()
+
+
+def load_sg(path, ctx=None):
+    """Lobe list: (axis [K][3], sharpness [K], amplitude [K][3])."""
+    import numpy as np
+    ld = _Loader(ctx)
+    L = ld.lib
+    try:
+        k = ctypes.c_int()
+        ld.check(L.vcl_sg_load(ld.h, str(path).encode(), 0, ctypes.byref(k), None, None, None), "vcl_sg_load")
+        K = k.value
+        ax, sh, am = np.zeros((K, 3), np.float32), np.zeros(K, np.float32), np.zeros((K, 3), np.float32)
+        ld.check(L.vcl_sg_load(ld.h, str(path).encode(), K, ctypes.byref(k), ax.ctypes.data, sh.ctypes.data,
+                               am.ctypes.data), "vcl_sg_load")
+        return ax, sh, am
+    finally:
+        ld.close()

@@ -234,6 +234,68 @@ def make_scene(name, *, mesh, W, H, views, tex, K, dist=(3.0, 3.0), disp=0.0, se
         rot=colmajor(R4), iters=iters, seed=seed, lr_pos=lr_pos)
 
 
+def vertex_normals(pos, tri):
+    """Area-weighted vertex normals (for meshes whose file has none)."""
+    p = np.asarray(pos, np.float64)
+    f = np.asarray(tri, np.int64)
+    n = np.cross(p[f[:, 1]] - p[f[:, 0]], p[f[:, 2]] - p[f[:, 0]])
+    out = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(out, f[:, k], n)
+    ln = np.linalg.norm(out, axis=1, keepdims=True)
+    return out / np.where(ln > 0, ln, 1.0)
+
+
+def scene_from_assets(name, mesh, texture, lobes, *, W, H, views, dist=(2.5, 4.0), seed=0, C=4, iters=100,
+                      fov=45.0, lr_pos=0.0, tex_init=0.5):
+    """A fit job from loaded assets (vcl_b200.capi.load_obj / load_bmp /
+    load_sg): the welded mesh (normals computed when the file has none),
+    the image as the target texture (channels padded with 1 up to C; the
+    fit starts from a constant texture), the lobes as the target lighting
+    (amplitude channels padded with 0; the fit starts from the same lobes),
+    seeded cameras around the mesh's bounding sphere."""
+    rng = np.random.default_rng(seed)
+    pos = np.asarray(mesh["w_pos"], np.float64)
+    tri = np.ascontiguousarray(mesh["w_tri"], dtype=np.uint32)
+    ctr = 0.5 * (pos.min(0) + pos.max(0))
+    rad = max(float(np.linalg.norm(pos - ctr, axis=1).max()), 1e-6)
+    v = (pos - ctr) / rad                       # unit bounding sphere at the origin
+    nrm = np.asarray(mesh["w_normal"], np.float64)
+    if not np.any(nrm):
+        nrm = vertex_normals(v, tri)
+    uv = np.asarray(mesh["w_uv"], np.float64)
+    img = np.asarray(texture, np.float32)
+    if img.ndim == 2:
+        img = img[..., None]
+    th, tw = img.shape[:2]
+    if img.shape[2] < C:
+        img = np.concatenate([img, np.ones((th, tw, C - img.shape[2]), np.float32)], axis=2)
+    img = np.ascontiguousarray(img[..., :C])
+    axis, sharp, amp = (np.asarray(x, np.float64) for x in lobes)
+    K = axis.shape[0]
+    if amp.shape[1] < C:
+        amp = np.concatenate([amp, np.zeros((K, C - amp.shape[1]))], axis=1)
+    amp = amp[:, :C]
+    R = random_rotation(rng)
+    P = perspective(fov)
+    R4 = np.eye(4)
+    R4[:3, :3] = R
+    mvps, pvinvs = [], []
+    for _ in range(views):
+        V = look_at(random_dir(rng) * rng.uniform(dist[0], dist[1]))
+        mvps.append(colmajor(P @ V @ R4))
+        pvinvs.append(np.ascontiguousarray(np.linalg.inv(P[:3, :3] @ V[:3, :3]).T.reshape(-1)).astype(np.float32))
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    return Scene(
+        name=name, W=W, H=H, views=views, pos=f32(v), pos_target=f32(v), tri=tri, uv=f32(uv), normal=f32(nrm),
+        tex_w=tw, tex_h=th, C=C, levels=tex_levels(tw, th), tex_target=img,
+        tex_init=np.full((th, tw, C), tex_init, np.float32), K=K,
+        lobe_axis=f32(axis), lobe_sharp=f32(sharp), lobe_amp=f32(amp),
+        lobe_axis_init=f32(axis), lobe_sharp_init=f32(sharp), lobe_amp_init=f32(amp),
+        mvp=np.stack(mvps).astype(np.float32), pvinv=np.stack(pvinvs).astype(np.float32),
+        rot=colmajor(R4), iters=iters, seed=seed, lr_pos=lr_pos)
+
+
 # The five workloads (sizes as the fit configurations state them).  Adam
 # runs at 1e-2 on texture and lobes; on vertex positions of the larger meshes
 # at 1e-3 (each parameter group has its own Adam, as in the reference's
