@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--strategy", default="both", choices=["both", "plain", "fused"])
+    ap.add_argument("--raster-schedule", default="tuned", choices=["tuned", "size"],
+                    help="fit jobs time raster schedules (tuned) or take the size-based one (size; "
+                         "deterministic, e.g. under a profiler)")
     return ap.parse_args()
 
 
@@ -173,6 +176,8 @@ def run_vcl(args, rank, world):
     torch.cuda.set_device(dev)
     S = make_scene(args)
     ctx = capi.Context(dev)
+    if args.raster_schedule == "size":
+        ctx.set_raster_autotune(0)
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     N = S.W * S.H * S.views

@@ -239,28 +239,35 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
             if (tile_overlaps(r, tx, ty, tile, W, H)) atomicAdd(&cnt[ty * tiles_x + tx], 1);
 }
 
-// Exclusive scan of n ints by one CTA of 1024 threads: each thread sums a
-// contiguous run, the run sums are scanned across the block, each thread
-// writes its run.
-__global__ void k_scan(const int* __restrict__ in, int* __restrict__ out, int n) {
-    __shared__ int warp_sums[32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int per = (n + 1023) / 1024;
-    const int beg = min(tid * per, n), end = min(beg + per, n);
+// Exclusive scan of n ints by one CTA of 32 warps: warp w owns a contiguous
+// segment; it sums the segment with coalesced loads, the 32 segment sums are
+// scanned, then each warp rescans its segment 32 elements at a time (warp
+// inclusive scan + running carry), again with coalesced loads and stores.
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ in, int* __restrict__ out, int n) {
+    __shared__ int seg_sum[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int seg = (n + 31) / 32;
+    const int beg = min(wid * seg, n), end = min(beg + seg, n);
     int sum = 0;
-    for (int i = beg; i < end; ++i) sum += in[i];
-    int x = sum;
-    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
-    if (lane == 31) warp_sums[wid] = x;
+    for (int i = beg + lane; i < end; i += 32) sum += in[i];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) seg_sum[wid] = sum;
     __syncthreads();
     if (wid == 0) {
-        int v = warp_sums[lane];
+        int v = seg_sum[lane];
         for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v += y; }
-        warp_sums[lane] = v;
+        seg_sum[lane] = v;   // inclusive
     }
     __syncthreads();
-    int excl = (wid ? warp_sums[wid - 1] : 0) + x - sum;
-    for (int i = beg; i < end; ++i) { out[i] = excl; excl += in[i]; }
+    int carry = wid ? seg_sum[wid - 1] : 0;
+    for (int base = beg; base < end; base += 32) {
+        const int i = base + lane;
+        const int v = i < end ? in[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (i < end) out[i] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
 }
 
 __global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int W, int H, int tile, int tiles_x,
