@@ -42,9 +42,11 @@ static void plan(const vcl_fit_desc& d, vcl_fit* f, Layout& L) {
     o[i++] = L.add(F * N * 2);                // uv
     o[i++] = L.add(F * N * 4);                // uv_da
     o[i++] = L.add(F * N * d.C);              // diffuse
+    o[i++] = L.add(F * N);                    // rough
+    // normal .. spec amp: one stretch of plain-strategy intermediates (11
+    // floats per pixel) that the fused step reuses for its shading records
     o[i++] = L.add(F * N * 3);                // normal
     o[i++] = L.add(F * N * 3);                // view
-    o[i++] = L.add(F * N);                    // rough
     o[i++] = L.add(F * N * 3);                // spec axis
     o[i++] = L.add(F * N);                    // spec sharp
     o[i++] = L.add(F * N);                    // spec amp
@@ -72,8 +74,8 @@ static void plan(const vcl_fit_desc& d, vcl_fit* f, Layout& L) {
         f->mvp = (float*)(b + o[j++]);
         f->pvinv = (float*)(b + o[j++]); f->rot = (float*)(b + o[j++]); f->clip = (float*)(b + o[j++]);
         f->rast = (float*)(b + o[j++]); f->db = (float*)(b + o[j++]); f->uv = (float*)(b + o[j++]);
-        f->uv_da = (float*)(b + o[j++]); f->diffuse = (float*)(b + o[j++]); f->normal = (float*)(b + o[j++]);
-        f->view = (float*)(b + o[j++]); f->rough = (float*)(b + o[j++]); f->sax = (float*)(b + o[j++]);
+        f->uv_da = (float*)(b + o[j++]); f->diffuse = (float*)(b + o[j++]); f->rough = (float*)(b + o[j++]);
+        f->normal = (float*)(b + o[j++]); f->view = (float*)(b + o[j++]); f->sax = (float*)(b + o[j++]);
         f->ssh = (float*)(b + o[j++]); f->sam = (float*)(b + o[j++]); f->color = (float*)(b + o[j++]);
         f->aa = (float*)(b + o[j++]); f->target = (float*)(b + o[j++]); f->g_aa = (float*)(b + o[j++]);
         f->g_color = (float*)(b + o[j++]); f->g_diffuse = (float*)(b + o[j++]); f->g_uv = (float*)(b + o[j++]);

@@ -43,7 +43,7 @@ struct Fused {
     bool sched_cached = false;                 // schedule taken from the tuning cache
     int* flags = nullptr;                      // [0] overflowed raster tiles of the last step
     float* scr = nullptr;                      // per view-vertex screen terms for the antialias kernels
-    int* d_step = nullptr;
+    int* d_step = nullptr;                     // [0] step counter, [8] shading records of this step
     double* d_corr = nullptr;    // 1 - beta1^t', 1 - beta2^t'
     cudaGraph_t graph_def = nullptr;           // the captured step (child of batch graphs)
     cudaGraphExec_t graph = nullptr;
@@ -77,6 +77,17 @@ struct ShadeIn {
 struct PixIn {
     float2 uv; float4 uvda; float4 dfs; float3 n, pax; float ss, sa;
     uint32_t i0, i1, i2; float4 r;
+};
+
+// Shading records of the covered pixels, written by k_shade_fwd and read by
+// k_sg_lobes in the same step: (n, ss), (p, sa), the diffuse texture colour
+// and the pixel index, compacted in the order the blocks claim their slots.
+// The lobe pass then reads three coalesced vectors and one gathered dL/dout
+// per pixel instead of redoing interpolation, the texture fetch and the
+// normal / view / specular set-up.
+struct ShadeRec {
+    float4* nss; float4* psa; float4* dfs; uint32_t* pix;
+    int* count;          // records written this step (reset before the shading pass)
 };
 
 template <int C4>
@@ -144,18 +155,42 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
 }
 
 // Forward shading of every pixel; writes the color and the diffuse
-// environment sum (kept for the backward's diffuse gradient).  C = 4.
+// environment sum (kept for the backward's diffuse gradient) and, when
+// rec.count is set, the shading record of each covered pixel (one slot
+// claim per block).  C = 4; 256 threads.
 __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
-                                                   float4* __restrict__ diffenv) {
+                                                   float4* __restrict__ diffenv, ShadeRec rec) {
     extern __shared__ float4 sm4[];
+    __shared__ int s_off[8], s_base;
     sg_stage_lobes4(sm4, a.K, a.axis, a.sharp, a.amp);
-    __syncthreads();
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.npix) return;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     PixIn q;
-    if (!shade_inputs<1>(a, td, p, q)) {
+    const bool live = p < a.npix && shade_inputs<1>(a, td, p, q);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned ball = __ballot_sync(0xffffffffu, live);
+    if (rec.count && lane == 0) s_off[wid] = __popc(ball);
+    __syncthreads();
+    if (rec.count && threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            const int c = s_off[w];
+            s_off[w] = t;
+            t += c;
+        }
+        s_base = t ? atomicAdd(rec.count, t) : 0;
+    }
+    __syncthreads();
+    if (p >= a.npix) return;
+    if (!live) {
         color[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
+    }
+    if (rec.count) {
+        const int k = s_base + s_off[wid] + __popc(ball & ((1u << lane) - 1u));
+        rec.nss[k] = make_float4(q.n.x, q.n.y, q.n.z, q.ss);
+        rec.psa[k] = make_float4(q.pax.x, q.pax.y, q.pax.z, q.sa);
+        rec.dfs[k] = q.dfs;
+        rec.pix[k] = (uint32_t)p;
     }
     float4 de, se;
     sg_env4(sm4, a.K, q.n, q.pax, q.ss, q.sa, de, se);
@@ -303,45 +338,62 @@ __global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const fl
     red_add4(gcv + (size_t)i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
 }
 
-// Lobe gradients (material.cu:428-433), lobe-parallel: a warp stages up to
-// 32 covered pixels (their shading inputs recomputed from the raster output,
-// reduced to the per-pixel factors every lobe reuses), then each lane walks
-// them for its lobe(s); sums stay in registers until the end.  C = 4.
+// Lobe gradients (material.cu:428-433), lobe-parallel: a warp stages 32
+// shading records as 16 pixel pairs, then each lane walks the pairs for its
+// lobe(s) on paired FP32 instructions; sums stay in registers until the end.
+// The next chunk's records and dL/dout are loaded while the current one is
+// consumed (its pixel indices one chunk earlier still).  C = 4.
 template <int NL, bool EXACT>
-__global__ void __launch_bounds__(128, NL == 1 ? 8 : 1) k_sg_lobes(ShadeIn a, TexDesc td, const float4* __restrict__ g_color, int Kp,
+__global__ void __launch_bounds__(128, NL == 1 ? 4 : 1) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color, int Kp,
                                                   float* __restrict__ g_axis, float* __restrict__ g_sharp,
                                                   float* __restrict__ g_amp) {
     extern __shared__ float sm[];
     const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int K = a.K;
     float* s_acc = sm;                                               // [K][8]
-    SPix4* s_pix = reinterpret_cast<SPix4*>(sm + ((size_t)K * 8 + 3) / 4 * 4);
+    SPair* s_pix = reinterpret_cast<SPair*>(sm + ((size_t)K * 8 + 3) / 4 * 4);
     for (int i = threadIdx.x; i < K * 8; i += blockDim.x) s_acc[i] = 0.f;
     __syncthreads();
     const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
-    Lobe4 LL[NL];
+    Lobe4x2 LL[NL];
 #pragma unroll
-    for (int sl = 0; sl < NL; ++sl) lobe4_load(LL[sl], li + sl * Kp, K, a.axis, a.sharp, a.amp);
-    SPix4* st = s_pix + wid * 32;
-    const long long nchunks = (a.npix + 31) / 32;
-    for (long long chunk = (long long)blockIdx.x * nwarps + wid; chunk < nchunks; chunk += (long long)gridDim.x * nwarps) {
-        const long long p = chunk * 32 + lane;
-        PixIn q;
-        const bool live = p < a.npix && shade_inputs<1>(a, td, p, q);
-        const unsigned ball = __ballot_sync(0xffffffffu, live);
-        const int m = __popc(ball);
-        if (live) st[__popc(ball & ((1u << lane) - 1u))] = spix4(q.n, q.pax, q.ss, q.sa, q.dfs, g_color[p]);
+    for (int sl = 0; sl < NL; ++sl) lobe4x2_load(LL[sl], li + sl * Kp, K, a.axis, a.sharp, a.amp);
+    SPair* st = s_pix + wid * 16;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int n = *rec.count;
+    const int nchunks = (n + 31) >> 5, stride = gridDim.x * nwarps;
+    int c = blockIdx.x * nwarps + wid;
+    float4 ra = z4, rb = z4, rc = z4, rg = z4;
+    uint32_t pnext = 0;
+    if (c < nchunks && c * 32 + lane < n) {
+        const int k = c * 32 + lane;
+        ra = rec.nss[k]; rb = rec.psa[k]; rc = rec.dfs[k]; rg = g_color[rec.pix[k]];
+    }
+    if (c + stride < nchunks && (c + stride) * 32 + lane < n) pnext = rec.pix[(c + stride) * 32 + lane];
+    for (; c < nchunks; c += stride) {
+        const int m = min(32, n - c * 32);
+        if (lane < m) spair_put(st + (lane >> 1), lane & 1, ra, rb, rc, rg);
+        if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
+        if (c + stride < nchunks) {
+            const int k1 = (c + stride) * 32 + lane;
+            if (k1 < n) { ra = rec.nss[k1]; rb = rec.psa[k1]; rc = rec.dfs[k1]; rg = g_color[pnext]; }
+        }
+        if (c + 2 * stride < nchunks) {
+            const int k2 = (c + 2 * stride) * 32 + lane;
+            if (k2 < n) pnext = rec.pix[k2];
+        }
         __syncwarp();
-        for (int j = g; j < m; j += G) {
-            const SPix4 P = st[j];
+        const int npair = (m + 1) >> 1;
+        for (int j = g; j < npair; j += G) {
+            const SPair P = st[j];
 #pragma unroll
             for (int sl = 0; sl < NL; ++sl)
-                if (LL[sl].valid) lobe4_accumulate<EXACT>(LL[sl], P);
+                if (LL[sl].valid) lobe4x2_accumulate<EXACT>(LL[sl], P);
         }
         __syncwarp();
     }
 #pragma unroll
-    for (int sl = 0; sl < NL; ++sl) lobe4_flush(LL[sl], li + sl * Kp, Kp, s_acc);
+    for (int sl = 0; sl < NL; ++sl) lobe4x2_flush(LL[sl], li + sl * Kp, Kp, s_acc);
     __syncthreads();
     for (int j = threadIdx.x; j < K * 8; j += blockDim.x) {
         const float v = s_acc[j];
@@ -477,7 +529,7 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
 
 size_t shade_smem(int K) { return sizeof(float4) * (size_t)K * 2; }
 size_t lobes_smem(int K, int threads) {
-    return sizeof(float) * (((size_t)K * 8 + 3) / 4 * 4) + (size_t)(threads / 32) * 32 * sizeof(SPix4);
+    return sizeof(float) * (((size_t)K * 8 + 3) / 4 * 4) + (size_t)(threads / 32) * 16 * sizeof(SPair);
 }
 
 vcl_status autotune_raster(vcl_fit* f);
@@ -486,6 +538,12 @@ vcl_status fused_init(vcl_fit* f) {
     if (f->fused) return VCL_OK;
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
+    const size_t N = (size_t)d.W * d.H * d.views;
+    VCL_REQUIRE(N <= (size_t)INT32_MAX - (1u << 24), "fused strategy: W*H*views = %zu pixels, above 2^31 - 2^24", N);
+    VCL_REQUIRE((size_t)((const char*)(f->sam + N) - (const char*)f->normal) >= (2 * sizeof(float4) + 4) * N &&
+                    f->normal < f->sam && ((uintptr_t)f->normal & 15) == 0 && ((uintptr_t)f->uv_da & 15) == 0 &&
+                    (f->rough < f->normal || f->rough >= f->sam + N),
+                "fused strategy: shading record area too small (internal layout error)");
     Fused* F = new Fused();
     cudaStream_t as = ctx->aux;
     cudaError_t e = cudaMallocAsync(&F->d_step, 64, as);
@@ -686,10 +744,28 @@ ShadeIn shade_in(const vcl_fit* f) {
     return a;
 }
 
+// The fused step does not use the plain strategy's per-pixel intermediates,
+// so its shading records live there: the stretch from `normal` to the end of
+// `sam` (11 floats per pixel, checked in fused_init) holds (n, ss), (p, sa)
+// and the pixel indices, `uv_da` (4 floats per pixel) the diffuse colours.
+ShadeRec shade_rec(const vcl_fit* f, bool want) {
+    const size_t N = (size_t)f->d.W * f->d.H * f->d.views;
+    float4* r = reinterpret_cast<float4*>(f->normal);
+    ShadeRec x;
+    x.nss = r; x.psa = r + N;
+    x.pix = reinterpret_cast<uint32_t*>(r + 2 * N);
+    x.dfs = reinterpret_cast<float4*>(f->uv_da);
+    x.count = want ? ((Fused*)f->fused)->d_step + 8 : nullptr;
+    return x;
+}
+
 // The fused stages, each one launch (shared by the captured step and the
 // per-kernel timing).
 vcl_status stage_shade(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
-    k_shade_fwd<<<vcl_blocks(a.npix, 256), 256, shade_smem(a.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse);
+    const ShadeRec rec = shade_rec(f, f->d.learn_lobes && f->d.K);
+    if (rec.count) TRY(vcl_cuda_check(f->ctx, cudaMemsetAsync(rec.count, 0, sizeof(int), s), "record count"));
+    k_shade_fwd<<<vcl_blocks(a.npix, 256), 256, shade_smem(a.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse,
+                                                                     rec);
     return vcl_launch_check(f->ctx, "fused shade");
 }
 
@@ -710,18 +786,19 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     const int lthreads = 128;
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
-    long long capg = (long long)ctx->sm_count * (NL == 1 ? 8 : 4);
+    long long capg = (long long)ctx->sm_count * (NL == 1 ? 4 : 2);
     int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
     size_t lsm = lobes_smem(d.K, lthreads);
     const float4* gc = (const float4*)f->g_color;
+    const ShadeRec rec = shade_rec(f, true);
     if (compat) {
-        if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
     } else {
-        if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, s>>>(a, td, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
+        else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
     }
     return vcl_launch_check(ctx, "fused lobe gradients");
 }

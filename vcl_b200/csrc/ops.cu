@@ -545,6 +545,188 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, const float4* __restri
     else for (int i = 0; i < C && i < 8; ++i) gin[pidx * C + i] = acc[i];
 }
 
+// Tile forms of the two passes for C = 4: a block owns a 32 x 8 pixel tile
+// and evaluates every pixel pair it needs ONCE -- the horizontal pairs whose
+// right pixel q lies in columns x0 .. x0+32 and the vertical pairs whose upper
+// pixel lies in rows y0 .. y0+8 (one column and one row of halo) -- keeping
+// per pair the summed edge terms sent to its lower pixel (q-1 or q-W) and to
+// q in shared memory; each pixel then adds the four pair terms that touch it.
+// The gather kernels above evaluate each pair once per pixel of the pair.
+// The kernels wait mostly on dependent loads (rast -> triangle -> vertex), so
+// they are held to 32 registers for eight resident blocks per SM: the few
+// spilled values stay in L1, and the extra warps hide the load latency.
+constexpr int AAT_X = 32, AAT_Y = 8;
+constexpr int AAT_NH = (AAT_X + 1) * AAT_Y;   // horizontal pairs of a tile (with halo column)
+constexpr int AAT_NP = AAT_NH + AAT_X * (AAT_Y + 1);
+
+// Pair i of the tile at (x0, y0): direction and the coordinates of q;
+// `own`: the pair belongs to this tile (not its halo).
+DEV void aat_pair_coords(int i, int x0, int y0, int& dir, int& qx, int& qy, bool& own) {
+    if (i < AAT_NH) {
+        const int r = i / (AAT_X + 1), c = i - r * (AAT_X + 1);
+        dir = 0; qx = x0 + c; qy = y0 + r; own = c < AAT_X;
+    } else {
+        const int j = i - AAT_NH, r = j / AAT_X, c = j - r * AAT_X;
+        dir = 1; qx = x0 + c; qy = y0 + r; own = r < AAT_Y;
+    }
+}
+
+// Lists the tile's pairs whose two pixels hold different triangle ids (the
+// only pairs with edge terms) in s_list and zeroes every pair's terms; the
+// pairs are then evaluated from the list with full warps.  Returns the count.
+DEV int aat_candidates(const float4* __restrict__ rast, long long vb, int W, int H, int x0, int y0, float4* s_lo,
+                       float4* s_hi, int* s_list, int* s_n) {
+    if (threadIdx.x == 0) *s_n = 0;
+    __syncthreads();
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int base = 0; base < AAT_NP; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        bool cand = false;
+        if (i < AAT_NP) {
+            int dir, qx, qy;
+            bool own;
+            aat_pair_coords(i, x0, y0, dir, qx, qy, own);
+            if (qx < W && qy < H && (dir == 0 ? qx > 0 : qy > 0)) {
+                const long long q = vb + (long long)qy * W + qx;
+                cand = rast[q].w != rast[dir == 0 ? q - 1 : q - W].w;
+            }
+            s_lo[i] = z;
+            s_hi[i] = z;
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, cand);
+        int slot = 0;
+        if ((threadIdx.x & 31) == 0 && ball) slot = atomicAdd(s_n, __popc(ball));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (cand) s_list[slot + __popc(ball & ((1u << (threadIdx.x & 31)) - 1u))] = i;
+    }
+    __syncthreads();
+    return *s_n;
+}
+
+DEV float4 f4add(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+DEV float4 f4sub(float4 a, float4 b) { return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+DEV float4 f4mul(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+
+// Sum of the four pair terms at pixel (tx, ty) of the tile.
+DEV float4 aat_gather(const float4* s_lo, const float4* s_hi, int tx, int ty) {
+    const int h = ty * (AAT_X + 1) + tx, v = AAT_NH + ty * AAT_X + tx;
+    return f4add(f4add(s_hi[h], s_lo[h + 1]), f4add(s_hi[v], s_lo[v + AAT_X]));
+}
+
+__global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict__ clip, const float4* __restrict__ scr_all,
+                                                     int nv, const uint32_t* __restrict__ tri, int nt,
+                                                     const float4* __restrict__ rast, int W, int H,
+                                                     const float4* __restrict__ in, float4* __restrict__ out, int* flags) {
+    __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
+    __shared__ int s_list[AAT_NP], s_n;
+    const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
+    const long long vb = (long long)view * W * H;
+    const float4* proj = clip + (size_t)view * nv;
+    const float4* scr = scr_all ? scr_all + 2 * (size_t)view * nv : nullptr;
+    const float2 s = make_float2(W / 2.f, H / 2.f);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
+    for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
+        const int i = s_list[k];
+        int dir, qx, qy;
+        bool own;
+        aat_pair_coords(i, x0, y0, dir, qx, qy, own);
+        float4 lo = z, hi = z;
+        AAPair P;
+        const long long q = vb + (long long)qy * W + qx;
+        if (aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, false, s, P, flags, false)) {
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                float a, alpha, ia, n;
+                float2 ev;
+                if (!aa_edge(P.t.v[e], P.t.v[(e + 1) % 3], P.o, a, alpha, ia, ev, n)) continue;
+                const float4 t = f4mul(f4sub(in[P.pp], in[P.op]), alpha);
+                if ((alpha > 0 ? P.op : P.pp) == q) hi = f4add(hi, t); else lo = f4add(lo, t);
+            }
+        }
+        s_lo[i] = lo;
+        s_hi[i] = hi;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % AAT_X, ty = threadIdx.x / AAT_X;
+    const int px = x0 + tx, py = y0 + ty;
+    if (px >= W || py >= H) return;
+    const long long p = vb + (long long)py * W + px;
+    out[p] = f4add(in[p], aat_gather(s_lo, s_hi, tx, ty));
+}
+
+__global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict__ clip, const float4* __restrict__ scr_all,
+                                                     int nv, const uint32_t* __restrict__ tri, int nt,
+                                                     const float4* __restrict__ rast, int W, int H,
+                                                     const float4* __restrict__ in, const float4* __restrict__ gout,
+                                                     float4* __restrict__ gin, float* __restrict__ gclip, int exact,
+                                                     int* flags) {
+    __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
+    __shared__ int s_list[AAT_NP], s_n;
+    const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
+    const long long vb = (long long)view * W * H;
+    const float4* proj = clip + (size_t)view * nv;
+    const float4* scr = scr_all ? scr_all + 2 * (size_t)view * nv : nullptr;
+    float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
+    const float2 s = make_float2(W / 2.f, H / 2.f);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
+    for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
+        const int i = s_list[k];
+        int dir, qx, qy;
+        bool own;
+        aat_pair_coords(i, x0, y0, dir, qx, qy, own);
+        own = own && gv;
+        float4 lo = z, hi = z;
+        AAPair P;
+        const long long q = vb + (long long)qy * W + qx;
+        // the reference's horizontal typo can give pp == op: its two colour
+        // terms cancel and the clip term is zero (antialias.cu:279, :216-223)
+        if (aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags, exact && own) &&
+            P.pp != P.op) {
+#pragma unroll
+            for (int e = 0; e < 3; ++e) {
+                const int ka = e, kb = (e + 1) % 3;
+                float a, alpha, ia, n;
+                float2 ev;
+                if (!aa_edge(P.t.v[ka], P.t.v[kb], P.o, a, alpha, ia, ev, n)) continue;
+                const float4 g = gout[alpha > 0 ? P.op : P.pp];
+                const float4 t = f4mul(g, alpha);
+                if (P.pp == q) { hi = f4add(hi, t); lo = f4sub(lo, t); }
+                else { lo = f4add(lo, t); hi = f4sub(hi, t); }
+                if (own) {
+                    const float4 ip = in[P.pp], io = in[P.op];
+                    float d = g.x * (ip.x - io.x) + g.y * (ip.y - io.y) + g.z * (ip.z - io.z) + g.w * (ip.w - io.w);
+                    float2 pa = P.t.v[ka], pb = P.t.v[kb];
+                    d *= ia;
+                    float2 da = make_float2(d * s.x * P.t.iw[ka], d * s.y * P.t.iw[ka]);
+                    float2 dbv = make_float2(d * s.x * P.t.iw[kb], d * s.y * P.t.iw[kb]);
+                    const float r = (n > 0 ? ev.x : -ev.y) * ia;
+                    if (n > 0) {
+                        da.x *= pb.y; da.y *= pb.y; da.y *= r;
+                        dbv.x *= -pa.y; dbv.y *= -pa.y; dbv.y *= r;
+                    } else {
+                        da.x *= -pb.x; da.y *= -pb.x; da.x *= r;
+                        dbv.x *= pa.x; dbv.y *= pa.x; dbv.x *= r;
+                    }
+                    // w: as in k_aa_bwd (antialias.cu:241-242 in COMPAT, x/w in EXACT)
+                    const float2 wa = exact ? P.t.ndc[ka] : pa, wb = exact ? P.t.ndc[kb] : pb;
+                    red_add4(gv + (size_t)P.t.id[ka] * 4, da.x, da.y, 0.f, -(da.x * wa.x + da.y * wa.y));
+                    red_add4(gv + (size_t)P.t.id[kb] * 4, dbv.x, dbv.y, 0.f, -(dbv.x * wb.x + dbv.y * wb.y));
+                }
+            }
+        }
+        s_lo[i] = lo;
+        s_hi[i] = hi;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % AAT_X, ty = threadIdx.x / AAT_X;
+    const int px = x0 + tx, py = y0 + ty;
+    if (px >= W || py >= H) return;
+    const long long p = vb + (long long)py * W + px;
+    gin[p] = f4add(gout[p], aat_gather(s_lo, s_hi, tx, ty));
+}
+
 // ----------------------------------------------------------------- loss
 __global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, long long n, float* __restrict__ grad,
                       float* __restrict__ loss) {
@@ -585,6 +767,10 @@ __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
+dim3 aat_grid(int W, int H, int views) {
+    return dim3((unsigned)((W + AAT_X - 1) / AAT_X), (unsigned)((H + AAT_Y - 1) / AAT_Y), (unsigned)views);
+}
+
 int grid_for(long long n, int threads, int sm) {
     long long b = (n + threads - 1) / threads;
     long long cap = (long long)sm * 8;
@@ -597,9 +783,9 @@ vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int n
                         const float* rast, int W, int H, int views, int C, const float* in, float* out, cudaStream_t s) {
     long long npix = (long long)W * H * views;
     const float4* sc = (const float4*)scr;
-    if (C == 4 && aligned16(in) && aligned16(out))
-        k_aa_fwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
-                                                         H, npix, C, in, out, ctx->dev_flags);
+    if (C == 4 && aligned16(in) && aligned16(out) && views <= 65535)
+        k_aa_fwd_tile<<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                             H, (const float4*)in, (float4*)out, ctx->dev_flags);
     else
         k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                          H, npix, C, in, out, ctx->dev_flags);
@@ -612,10 +798,10 @@ vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int n
     long long npix = (long long)W * H * views;
     int exact = ctx->mode == VCL_MODE_EXACT;
     const float4* sc = (const float4*)scr;
-    if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in))
-        k_aa_bwd<1><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
-                                                         H, npix, C, in, grad_out, grad_in, grad_clip, exact,
-                                                         ctx->dev_flags);
+    if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in) && views <= 65535)
+        k_aa_bwd_tile<<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
+                                                             H, (const float4*)in, (const float4*)grad_out,
+                                                             (float4*)grad_in, grad_clip, exact, ctx->dev_flags);
     else
         k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                          H, npix, C, in, grad_out, grad_in, grad_clip, exact,

@@ -604,63 +604,109 @@ DEV void sg_env4(const float4* L4, int K, float3 n, float3 pax, float ss, float 
     se = make_float4(ee[0], ee[1], ee[2], ee[3]);
 }
 
-// Pixel state of the lean lobe-gradient pass: the per-pixel factors every
-// lobe reuses, computed once by the staging lane.
-struct SPix4 {
-    float4 a;    // 2.133 n, ss
-    float4 b;    // ss p, sa
-    float4 g;    // dL/dout
-    float4 gd;   // dL/dout * diffuse
-    float4 c;    // ss log2 e, |2.133 n|^2, |ss p|^2, -
-};
+// ---------------------------------------------------------------------------
+// Lobe gradients of the fused step, two pixels per lane.
+//
+// sm_100 issues a pair of FP32 adds, multiplies or fmas as ONE instruction
+// (__fadd2_rn / __fmul2_rn / __ffma2_rn, round-to-nearest like the scalar
+// forms).  The lobe-gradient pass is issue-bound, so each lane walks pixel
+// PAIRS for its lobe: every FP32 step below serves two pixels; only the
+// rsqrt and ex2 steps run per pixel.
 
-DEV SPix4 spix4(float3 n, float3 pax, float ss, float sa, float4 dfs, float4 go) {
-    SPix4 z;
-    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
-    z.a = make_float4(dn.x, dn.y, dn.z, ss);
-    z.b = make_float4(sn.x, sn.y, sn.z, sa);
-    z.g = go;
-    z.gd = make_float4(go.x * dfs.x, go.y * dfs.y, go.z * dfs.z, go.w * dfs.w);
-    z.c = make_float4(ss * SG_L2E, dot3(dn, dn), dot3(sn, sn), 0.f);
-    return z;
+DEV float2 p2(float x) { return make_float2(x, x); }
+DEV float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+DEV float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+DEV float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+DEV float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+DEV float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+DEV float2 ex2_2(float2 a) { return make_float2(ex2_fast(a.x), ex2_fast(a.y)); }
+// 1/max(|v|, 1e-6) and |v| from |v|^2, per half (as sg_len).
+DEV void sg_len2(float2 d2, float2& l, float2& il) {
+    const float2 q = make_float2(fmaxf(d2.x, 1e-12f), fmaxf(d2.y, 1e-12f));
+    il = make_float2(rsqrtf(q.x), rsqrtf(q.y));
+    l = mul2(q, il);
 }
 
-// One lane's lobe (C = 4) with its gradient sums.  The axis gradient
-// sum_p c1 (u_d + s a) + c2 (u_s + s a) is kept as ax = sum (c1 u_d + c2 u_s)
-// plus axs = sum (c1 + c2), combined with s a when the lane flushes.
-struct Lobe4 {
+// Two staged pixels; each field holds (first pixel, second pixel).  The
+// per-pixel factors every lobe reuses are computed once by the staging lane.
+struct __align__(16) SPair {
+    float2 dnx, dny, dnz;    // 2.133 n
+    float2 snx, sny, snz;    // ss p
+    float2 sa, nssl;         // sa, -ss log2 e
+    float2 dn2, sn2;         // |2.133 n|^2, |ss p|^2
+    float2 gx, gy, gz, gw;   // dL/dout
+    float2 hx, hy, hz, hw;   // dL/dout * diffuse
+};
+constexpr int SPAIR_FIELDS = (int)(sizeof(SPair) / sizeof(float2));
+
+// Writes one pixel into half `h` of a staged pair from its shading record
+// (nss = (n, ss), psa = (p, sa), the diffuse texture colour dfs) and its
+// dL/dout.  All-zero inputs pad an odd count: a zero pixel adds exactly
+// nothing to any sum.
+DEV void spair_put(SPair* s, int h, float4 nss, float4 psa, float4 dfs, float4 go) {
+    const float3 dn = f3(nss.x, nss.y, nss.z) * SG_DIFF_SHARP, sn = f3(psa.x, psa.y, psa.z) * nss.w;
+    const float v[SPAIR_FIELDS] = {dn.x, dn.y, dn.z, sn.x, sn.y, sn.z, psa.w, -(nss.w * SG_L2E), dot3(dn, dn),
+                                   dot3(sn, sn), go.x, go.y, go.z, go.w, go.x * dfs.x, go.y * dfs.y, go.z * dfs.z,
+                                   go.w * dfs.w};
+    float* f = reinterpret_cast<float*>(s) + h;
+#pragma unroll
+    for (int i = 0; i < SPAIR_FIELDS; ++i) f[2 * i] = v[i];
+}
+
+// One lane's lobe (C = 4): its constants broadcast to both halves and its
+// gradient sums per half.  The axis gradient sum_p c1 (u_d + s a) + c2 (u_s + s a)
+// is kept as ax = sum (c1 u_d + c2 u_s) plus axs = sum (c1 + c2), combined with
+// s a when the lane flushes.
+struct Lobe4x2 {
     bool valid;
-    float3 sgn;
-    float3 a0;                 // raw axis (EXACT sharpness derivative)
-    float gs, gsl, cdl, agA;   // sharpness, s*log2e, (2.133 + s)*log2e, 2.34*s
-    float sg2, a02;            // |s a|^2, |a|^2
-    float4 a;
-    float3 ax;
-    float axs;
-    float sh;
-    float4 am;
+    float3 sgn;                  // s a (scalar, for the flush)
+    float2 sx, sy, sz;           // s a
+    float2 a0x, a0y, a0z, a02;   // raw axis and |a|^2 (EXACT sharpness derivative)
+    float2 gs, ngsl, ncdl, sg2;  // s, -s log2 e, -(2.133 + s) log2 e, |s a|^2
+    float2 ax4, ay4, az4, aw4;   // amplitude
+    float2 gax, gay, gaz, gaxs, gsh, gam0, gam1, gam2, gam3;   // sums
 };
 
-DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* sharp, const float* amp) {
+DEV void lobe4x2_load(Lobe4x2& L, int i, int K, const float* axis, const float* sharp, const float* amp) {
     L.valid = i < K;
     const int ii = L.valid ? i : 0;
     const float s = K ? sharp[ii] : 0.f;
-    L.gs = s;
-    L.gsl = s * SG_L2E;
-    L.cdl = (SG_DIFF_SHARP + s) * SG_L2E;
-    L.agA = SG_DIFF_AMP * s;
-    L.a0 = K ? f3(axis[3 * ii], axis[3 * ii + 1], axis[3 * ii + 2]) : f3(0.f, 0.f, 0.f);
-    L.sgn = L.a0 * s;
-    L.sg2 = dot3(L.sgn, L.sgn);
-    L.a02 = dot3(L.a0, L.a0);
-    L.a = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
-    L.ax = f3(0.f, 0.f, 0.f);
-    L.axs = 0.f;
-    L.sh = 0.f;
-    L.am = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float3 a0 = K ? f3(axis[3 * ii], axis[3 * ii + 1], axis[3 * ii + 2]) : f3(0.f, 0.f, 0.f);
+    L.sgn = a0 * s;
+    L.sx = p2(L.sgn.x); L.sy = p2(L.sgn.y); L.sz = p2(L.sgn.z);
+    L.a0x = p2(a0.x); L.a0y = p2(a0.y); L.a0z = p2(a0.z); L.a02 = p2(dot3(a0, a0));
+    L.gs = p2(s);
+    L.ngsl = p2(-(s * SG_L2E));
+    L.ncdl = p2(-((SG_DIFF_SHARP + s) * SG_L2E));
+    L.sg2 = p2(dot3(L.sgn, L.sgn));
+    const float4 am = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3])
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    L.ax4 = p2(am.x); L.ay4 = p2(am.y); L.az4 = p2(am.z); L.aw4 = p2(am.w);
+    L.gax = L.gay = L.gaz = L.gaxs = L.gsh = L.gam0 = L.gam1 = L.gam2 = L.gam3 = p2(0.f);
 }
 
-// Gradient contributions of one pixel to one lobe (material.cu:398-433),
+// One half's contributions with each checked (the reference's guarded adds,
+// common.h:181): the rare path when some contribution is not finite.
+DEV void lobe4x2_guarded(float& am0, float& am1, float& am2, float& am3, float& ax, float& ay, float& az, float& axs,
+                         float& sh, float dg, float sgv, float c1, float c2, float shc, float dnx, float dny, float dnz,
+                         float snx, float sny, float snz, float gx, float gy, float gz, float gw, float hx, float hy,
+                         float hz, float hw) {
+    if (isfinite(dg) && isfinite(sgv)) {
+        am0 = fmaf(sgv, gx, fmaf(dg, hx, am0));
+        am1 = fmaf(sgv, gy, fmaf(dg, hy, am1));
+        am2 = fmaf(sgv, gz, fmaf(dg, hz, am2));
+        am3 = fmaf(sgv, gw, fmaf(dg, hw, am3));
+    }
+    if (isfinite(c1) && isfinite(c2)) {
+        ax = fmaf(c2, snx, fmaf(c1, dnx, ax));
+        ay = fmaf(c2, sny, fmaf(c1, dny, ay));
+        az = fmaf(c2, snz, fmaf(c1, dnz, az));
+        axs += c1 + c2;
+    }
+    sh += finite_or0(shc);
+}
+
+// Gradient contributions of two pixels to one lobe (material.cu:398-433),
 // rearranged.  With v = u + s a (u = 2.133 n for the diffuse term, ss p for
 // the specular one), |v|^2 = |u|^2 + |s a|^2 + 2 u.(s a), and the dot product
 // is the one the reference's sharpness derivative uses.  With e-/e+ the two
@@ -668,69 +714,69 @@ DEV void lobe4_load(Lobe4& L, int i, int K, const float* axis, const float* shar
 // (d value/d|v|)/|v| = T il^2,  d value/ds = il (dotn T - Dm)  (the
 // reference's ((dotn (1-il) - 1) e- + (dotn (1+il) + 1) e+) il, expanded).
 // The reference's guarded adds (common.h:181) drop a non-finite
-// contribution; when the contributions sum to a finite value they are all
-// finite and are added plainly, else each is checked.
+// contribution; when a pixel's contributions sum to a finite value they are
+// all finite and are added plainly, else each is checked.
 template <bool EXACT>
-DEV void lobe4_accumulate(Lobe4& L, const SPix4& P) {
-    const float3 dn = f3(P.a.x, P.a.y, P.a.z), sn = f3(P.b.x, P.b.y, P.b.z);
-    const float sa = P.b.w;
+DEV void lobe4x2_accumulate(Lobe4x2& L, const SPair& P) {
     // diffuse lobe
-    const float dd = dot3(L.sgn, dn);
-    float dl, dil;
-    sg_len(fmaf(2.f, dd, P.c.y + L.sg2), dl, dil);
-    const float dotn = EXACT ? fmaf(L.gs, L.a02, dot3(L.a0, dn)) * dil : (L.gs + dd) * dil;
-    float x = dl * SG_L2E;
-    float em = ex2_fast(x - L.cdl), ep = ex2_fast(-x - L.cdl);
-    const float dDm = em - ep, dT = fmaf(-dil, dDm, em + ep);
+    const float2 dd = fma2(L.sz, P.dnz, fma2(L.sy, P.dny, mul2(L.sx, P.dnx)));
+    float2 dl, dil;
+    sg_len2(fma2(p2(2.f), dd, add2(P.dn2, L.sg2)), dl, dil);
+    const float2 dotn = EXACT ? mul2(fma2(L.gs, L.a02, fma2(L.a0z, P.dnz, fma2(L.a0y, P.dny, mul2(L.a0x, P.dnx)))), dil)
+                              : mul2(add2(L.gs, dd), dil);
+    float2 em = ex2_2(fma2(dl, p2(SG_L2E), L.ncdl)), ep = ex2_2(fma2(dl, p2(-SG_L2E), L.ncdl));
+    const float2 dDm = sub2(em, ep), dT = fma2(neg2(dil), dDm, add2(em, ep));
     // specular lobe
-    const float sd = dot3(L.sgn, sn);
-    float sl, sil;
-    sg_len(fmaf(2.f, sd, P.c.z + L.sg2), sl, sil);
-    const float dots = EXACT ? fmaf(L.gs, L.a02, dot3(L.a0, sn)) * sil : (L.gs + sd) * sil;
-    x = sl * SG_L2E;
-    const float c = P.c.x + L.gsl;
-    em = ex2_fast(x - c); ep = ex2_fast(-x - c);
-    const float sDm = em - ep, sT = fmaf(-sil, sDm, em + ep);
+    const float2 sd = fma2(L.sz, P.snz, fma2(L.sy, P.sny, mul2(L.sx, P.snx)));
+    float2 sl, sil;
+    sg_len2(fma2(p2(2.f), sd, add2(P.sn2, L.sg2)), sl, sil);
+    const float2 dots = EXACT ? mul2(fma2(L.gs, L.a02, fma2(L.a0z, P.snz, fma2(L.a0y, P.sny, mul2(L.a0x, P.snx)))), sil)
+                              : mul2(add2(L.gs, sd), sil);
+    const float2 nc = add2(P.nssl, L.ngsl);
+    em = ex2_2(fma2(sl, p2(SG_L2E), nc));
+    ep = ex2_2(fma2(sl, p2(-SG_L2E), nc));
+    const float2 sDm = sub2(em, ep), sT = fma2(neg2(sil), sDm, add2(em, ep));
     // channel sums
-    const float sum = P.g.x * L.a.x + P.g.y * L.a.y + P.g.z * L.a.z + P.g.w * L.a.w;
-    const float sumd = P.gd.x * L.a.x + P.gd.y * L.a.y + P.gd.z * L.a.z + P.gd.w * L.a.w;
-    const float dg = dDm * dil * SG_DIFF_AMP;
-    const float sgv = sDm * sil * sa;
-    const float c1 = sumd * (dT * dil * dil) * L.agA;
-    const float c2 = sum * (sT * sil * sil) * (sa * L.gs);
-    const float shc = fmaf(sumd * dil * SG_DIFF_AMP, fmaf(dotn, dT, -dDm), sum * sil * sa * fmaf(dots, sT, -sDm));
-    if (isfinite(dg + sgv + c1 + c2 + shc)) {
-        L.am.x = fmaf(sgv, P.g.x, fmaf(dg, P.gd.x, L.am.x));
-        L.am.y = fmaf(sgv, P.g.y, fmaf(dg, P.gd.y, L.am.y));
-        L.am.z = fmaf(sgv, P.g.z, fmaf(dg, P.gd.z, L.am.z));
-        L.am.w = fmaf(sgv, P.g.w, fmaf(dg, P.gd.w, L.am.w));
-        L.ax.x = fmaf(c2, sn.x, fmaf(c1, dn.x, L.ax.x));
-        L.ax.y = fmaf(c2, sn.y, fmaf(c1, dn.y, L.ax.y));
-        L.ax.z = fmaf(c2, sn.z, fmaf(c1, dn.z, L.ax.z));
-        L.axs += c1 + c2;
-        L.sh += shc;
+    const float2 sum = fma2(P.gw, L.aw4, fma2(P.gz, L.az4, fma2(P.gy, L.ay4, mul2(P.gx, L.ax4))));
+    const float2 sumd = fma2(P.hw, L.aw4, fma2(P.hz, L.az4, fma2(P.hy, L.ay4, mul2(P.hx, L.ax4))));
+    const float2 dilA = mul2(dil, p2(SG_DIFF_AMP));
+    const float2 dg = mul2(dDm, dilA);                        // diffuse value
+    const float2 sdA = mul2(sumd, dilA);
+    const float2 c1 = mul2(mul2(sdA, mul2(dT, dil)), L.gs);   // sumd T il^2 2.34 s
+    const float2 sils = mul2(sil, P.sa);
+    const float2 sgv = mul2(sDm, sils);                       // specular value
+    const float2 ssa = mul2(sum, sils);
+    const float2 c2 = mul2(mul2(ssa, mul2(sT, sil)), L.gs);   // sum T il^2 sa s
+    const float2 shc = fma2(sdA, fma2(dotn, dT, neg2(dDm)), mul2(ssa, fma2(dots, sT, neg2(sDm))));
+    const float2 t = add2(add2(add2(dg, sgv), add2(c1, c2)), shc);
+    if (isfinite(t.x) && isfinite(t.y)) {
+        L.gam0 = fma2(sgv, P.gx, fma2(dg, P.hx, L.gam0));
+        L.gam1 = fma2(sgv, P.gy, fma2(dg, P.hy, L.gam1));
+        L.gam2 = fma2(sgv, P.gz, fma2(dg, P.hz, L.gam2));
+        L.gam3 = fma2(sgv, P.gw, fma2(dg, P.hw, L.gam3));
+        L.gax = fma2(c2, P.snx, fma2(c1, P.dnx, L.gax));
+        L.gay = fma2(c2, P.sny, fma2(c1, P.dny, L.gay));
+        L.gaz = fma2(c2, P.snz, fma2(c1, P.dnz, L.gaz));
+        L.gaxs = add2(L.gaxs, add2(c1, c2));
+        L.gsh = add2(L.gsh, shc);
         return;
     }
-    if (isfinite(dg) && isfinite(sgv)) {
-        L.am.x = fmaf(sgv, P.g.x, fmaf(dg, P.gd.x, L.am.x));
-        L.am.y = fmaf(sgv, P.g.y, fmaf(dg, P.gd.y, L.am.y));
-        L.am.z = fmaf(sgv, P.g.z, fmaf(dg, P.gd.z, L.am.z));
-        L.am.w = fmaf(sgv, P.g.w, fmaf(dg, P.gd.w, L.am.w));
-    }
-    if (isfinite(c1) && isfinite(c2)) {
-        L.ax.x = fmaf(c2, sn.x, fmaf(c1, dn.x, L.ax.x));
-        L.ax.y = fmaf(c2, sn.y, fmaf(c1, dn.y, L.ax.y));
-        L.ax.z = fmaf(c2, sn.z, fmaf(c1, dn.z, L.ax.z));
-        L.axs += c1 + c2;
-    }
-    L.sh += finite_or0(shc);
+    lobe4x2_guarded(L.gam0.x, L.gam1.x, L.gam2.x, L.gam3.x, L.gax.x, L.gay.x, L.gaz.x, L.gaxs.x, L.gsh.x, dg.x, sgv.x,
+                    c1.x, c2.x, shc.x, P.dnx.x, P.dny.x, P.dnz.x, P.snx.x, P.sny.x, P.snz.x, P.gx.x, P.gy.x, P.gz.x,
+                    P.gw.x, P.hx.x, P.hy.x, P.hz.x, P.hw.x);
+    lobe4x2_guarded(L.gam0.y, L.gam1.y, L.gam2.y, L.gam3.y, L.gax.y, L.gay.y, L.gaz.y, L.gaxs.y, L.gsh.y, dg.y, sgv.y,
+                    c1.y, c2.y, shc.y, P.dnx.y, P.dny.y, P.dnz.y, P.snx.y, P.sny.y, P.snz.y, P.gx.y, P.gy.y, P.gz.y,
+                    P.gw.y, P.hx.y, P.hy.y, P.hz.y, P.hw.y);
 }
 
-// Folds the lobe groups of the warp together and adds the lane's sums into
-// the block accumulator s_acc [K][8] (axis xyz, sharpness, amplitude[4]).
-DEV void lobe4_flush(Lobe4& L, int i, int Kp, float* s_acc) {
-    float v[8] = {fmaf(L.axs, L.sgn.x, L.ax.x), fmaf(L.axs, L.sgn.y, L.ax.y), fmaf(L.axs, L.sgn.z, L.ax.z), L.sh,
-                  L.am.x, L.am.y, L.am.z, L.am.w};
+// Folds the two halves and the lobe groups of the warp together and adds the
+// lane's sums into the block accumulator s_acc [K][8] (axis xyz, sharpness,
+// amplitude[4]).
+DEV void lobe4x2_flush(Lobe4x2& L, int i, int Kp, float* s_acc) {
+    const float axs = L.gaxs.x + L.gaxs.y;
+    float v[8] = {fmaf(axs, L.sgn.x, L.gax.x + L.gax.y), fmaf(axs, L.sgn.y, L.gay.x + L.gay.y),
+                  fmaf(axs, L.sgn.z, L.gaz.x + L.gaz.y), L.gsh.x + L.gsh.y, L.gam0.x + L.gam0.y,
+                  L.gam1.x + L.gam1.y, L.gam2.x + L.gam2.y, L.gam3.x + L.gam3.y};
 #pragma unroll
     for (int q = 0; q < 8; ++q)
         for (int o = 16; o >= Kp; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
