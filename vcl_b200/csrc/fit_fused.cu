@@ -223,8 +223,10 @@ __global__ void k_mse_init(const float4* __restrict__ aa, const float4* __restri
 // grad ⊙ diffenv (material.cu:429 summed over the lobes), then texture
 // backward (texturemap.cu:229-284), interpolate backward to the
 // barycentrics (interpolate.cu:114-143) and raster backward
-// (rasterize.cu:84-141), scattered with vector reductions.
-__global__ void __launch_bounds__(256) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+// (rasterize.cu:84-141), scattered with vector reductions.  Held to 40
+// registers so that its blocks fit on the SMs beside the lobe-gradient
+// blocks it runs with.
+__global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
                                                  int want_tex, int want_geom) {
@@ -786,7 +788,9 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     const int lthreads = 128;
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
-    long long capg = (long long)ctx->sm_count * (NL == 1 ? 4 : 2);
+    // three lobe blocks per SM leave registers for two blocks of the per-pixel
+    // backward that runs beside this kernel (the two overlap on each SM)
+    long long capg = (long long)ctx->sm_count * (NL == 1 ? 3 : 2);
     int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
     size_t lsm = lobes_smem(d.K, lthreads);
     const float4* gc = (const float4*)f->g_color;
