@@ -529,7 +529,7 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
 
 #define TRY(x) do { vcl_status _s = (x); if (_s) return _s; } while (0)
 
-size_t shade_smem(int K) { return sizeof(float4) * (size_t)K * 2; }
+size_t shade_smem(int K) { return sg_lobes4_smem(K); }
 size_t lobes_smem(int K, int threads) {
     return sizeof(float) * (((size_t)K * 8 + 3) / 4 * 4) + (size_t)(threads / 32) * 16 * sizeof(SPair);
 }

@@ -21,9 +21,17 @@ constexpr float SG_DIFF_SHARP = 2.133f;
 constexpr float SG_DIFF_AMP = 2.34f;
 constexpr int SG_CMAX = 8;
 
+// Hardware reciprocal square root of a normal, positive x (the flush-to-zero
+// form: the same result as rsqrtf for such x, without the subnormal path).
+DEV float rsqrt_normal(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // 1/max(|v|, 1e-6) and |v| from |v|^2.
 DEV void sg_len(float d2, float& l, float& il) {
-    il = rsqrtf(fmaxf(d2, 1e-12f));
+    il = rsqrt_normal(fmaxf(d2, 1e-12f));
     l = d2 * il;
 }
 
@@ -556,63 +564,11 @@ DEV float ex2_fast(float x) {
     return y;
 }
 
-// Lobes packed for the pixel-parallel forward: (s*axis, s), (a0..a3).
-DEV void sg_stage_lobes4(float4* sm, int K, const float* axis, const float* sharp, const float* amp) {
-    for (int i = threadIdx.x; i < K; i += blockDim.x) {
-        float s = sharp[i];
-        sm[2 * i] = make_float4(axis[3 * i] * s, axis[3 * i + 1] * s, axis[3 * i + 2] * s, s);
-        sm[2 * i + 1] = make_float4(amp[4 * i], amp[4 * i + 1], amp[4 * i + 2], amp[4 * i + 3]);
-    }
-}
-
-// Forward environment sums of one pixel for C = 4 (material.cu:305-317);
-// same NaN-guard contract as sg_env (plain sums, guarded loop on overflow).
-DEV void sg_env4(const float4* L4, int K, float3 n, float3 pax, float ss, float sa, float4& de, float4& se) {
-    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
-    const float cdl = SG_DIFF_SHARP * SG_L2E, ssl = ss * SG_L2E;
-    float4 d = make_float4(0.f, 0.f, 0.f, 0.f), e = d;
-    for (int i = 0; i < K; ++i) {
-        const float4 A = L4[2 * i], B = L4[2 * i + 1];
-        const float3 g = f3(A.x, A.y, A.z);
-        const float gsl = A.w * SG_L2E;
-        float3 v = dn + g;
-        float l, il;
-        sg_len(dot3(v, v), l, il);
-        float x = l * SG_L2E, c = cdl + gsl;
-        const float dg = (ex2_fast(x - c) - ex2_fast(-x - c)) * il * SG_DIFF_AMP;
-        v = sn + g;
-        sg_len(dot3(v, v), l, il);
-        x = l * SG_L2E; c = ssl + gsl;
-        const float sg = (ex2_fast(x - c) - ex2_fast(-x - c)) * il * sa;
-        d.x = fmaf(dg, B.x, d.x); d.y = fmaf(dg, B.y, d.y); d.z = fmaf(dg, B.z, d.z); d.w = fmaf(dg, B.w, d.w);
-        e.x = fmaf(sg, B.x, e.x); e.y = fmaf(sg, B.y, e.y); e.z = fmaf(sg, B.z, e.z); e.w = fmaf(sg, B.w, e.w);
-    }
-    if (isfinite(d.x) && isfinite(d.y) && isfinite(d.z) && isfinite(d.w) && isfinite(e.x) && isfinite(e.y) &&
-        isfinite(e.z) && isfinite(e.w)) {
-        de = d; se = e;
-        return;
-    }
-    float dd[4] = {0.f, 0.f, 0.f, 0.f}, ee[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int i = 0; i < K; ++i) {
-        const float4 A = L4[2 * i], B = L4[2 * i + 1];
-        float dg, sg;
-        sg_terms(dn, sn, f3(A.x, A.y, A.z), A.w, ss, sa, dg, sg);
-        const float b[4] = {B.x, B.y, B.z, B.w};
-        for (int k = 0; k < 4; ++k) { add_nan_check(dd[k], dg * b[k]); add_nan_check(ee[k], sg * b[k]); }
-    }
-    de = make_float4(dd[0], dd[1], dd[2], dd[3]);
-    se = make_float4(ee[0], ee[1], ee[2], ee[3]);
-}
-
-// ---------------------------------------------------------------------------
-// Lobe gradients of the fused step, two pixels per lane.
-//
-// sm_100 issues a pair of FP32 adds, multiplies or fmas as ONE instruction
-// (__fadd2_rn / __fmul2_rn / __ffma2_rn, round-to-nearest like the scalar
-// forms).  The lobe-gradient pass is issue-bound, so each lane walks pixel
-// PAIRS for its lobe: every FP32 step below serves two pixels; only the
-// rsqrt and ex2 steps run per pixel.
-
+// Paired FP32 arithmetic: sm_100 issues a pair of FP32 adds, multiplies or
+// fmas as ONE instruction (__fadd2_rn / __fmul2_rn / __ffma2_rn,
+// round-to-nearest like the scalar forms).  The SG loops are issue-bound, so
+// they carry two lobes (forward) or two pixels (lobe gradients) per
+// instruction; only the rsqrt and ex2 steps run per element.
 DEV float2 p2(float x) { return make_float2(x, x); }
 DEV float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 DEV float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
@@ -623,9 +579,96 @@ DEV float2 ex2_2(float2 a) { return make_float2(ex2_fast(a.x), ex2_fast(a.y)); }
 // 1/max(|v|, 1e-6) and |v| from |v|^2, per half (as sg_len).
 DEV void sg_len2(float2 d2, float2& l, float2& il) {
     const float2 q = make_float2(fmaxf(d2.x, 1e-12f), fmaxf(d2.y, 1e-12f));
-    il = make_float2(rsqrtf(q.x), rsqrtf(q.y));
+    il = make_float2(rsqrt_normal(q.x), rsqrt_normal(q.y));
     l = mul2(q, il);
 }
+
+// Lobes packed in pairs for the pixel-parallel forward: pair j holds lobes
+// 2j and 2j+1 as (s a.x | s a.y), (s a.z | s), (amp.x | amp.y), (amp.z | amp.w),
+// each float4 = (first lobe, second lobe, first lobe, second lobe) of two
+// fields; an odd K is padded with a zero lobe (zero amplitude: it adds 0).
+inline size_t sg_lobes4_smem(int K) { return sizeof(float4) * 2 * (size_t)(K + (K & 1)); }
+
+DEV void sg_stage_lobes4(float4* sm, int K, const float* axis, const float* sharp, const float* amp) {
+    const int np = (K + 1) >> 1;
+    for (int j = threadIdx.x; j < np; j += blockDim.x) {
+        float v[2][8];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = 2 * j + h;
+            const bool ok = i < K;
+            const float s = ok ? sharp[i] : 0.f;
+            v[h][0] = ok ? axis[3 * i] * s : 0.f;
+            v[h][1] = ok ? axis[3 * i + 1] * s : 0.f;
+            v[h][2] = ok ? axis[3 * i + 2] * s : 0.f;
+            v[h][3] = s;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[h][4 + c] = ok ? amp[4 * i + c] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            sm[4 * j + q] = make_float4(v[0][2 * q], v[1][2 * q], v[0][2 * q + 1], v[1][2 * q + 1]);
+    }
+}
+
+// Forward environment sums of one pixel for C = 4 (material.cu:305-317),
+// two lobes per step; the same NaN-guard contract as sg_env (plain sums,
+// and the guarded loop when a sum is not finite).
+DEV void sg_env4(const float4* L4, int K, float3 n, float3 pax, float ss, float sa, float4& de, float4& se) {
+    const float3 dn = n * SG_DIFF_SHARP, sn = pax * ss;
+    const float2 dnx = p2(dn.x), dny = p2(dn.y), dnz = p2(dn.z), snx = p2(sn.x), sny = p2(sn.y), snz = p2(sn.z);
+    const float2 l2e = p2(SG_L2E), nl2e = p2(-SG_L2E), ncd = p2(-(SG_DIFF_SHARP * SG_L2E)), nss = p2(-(ss * SG_L2E));
+    const float2 amp = p2(SG_DIFF_AMP), sa2 = p2(sa);
+    float2 dx = p2(0.f), dy = dx, dz = dx, dw = dx, ex = dx, ey = dx, ez = dx, ew = dx;
+    const int np = (K + 1) >> 1;
+    for (int j = 0; j < np; ++j) {
+        const float4 P0 = L4[4 * j], P1 = L4[4 * j + 1], P2 = L4[4 * j + 2], P3 = L4[4 * j + 3];
+        const float2 gx = make_float2(P0.x, P0.y), gy = make_float2(P0.z, P0.w), gz = make_float2(P1.x, P1.y);
+        const float2 gs = make_float2(P1.z, P1.w);
+        // diffuse lobe
+        float2 vx = add2(dnx, gx), vy = add2(dny, gy), vz = add2(dnz, gz);
+        float2 l, il;
+        sg_len2(fma2(vz, vz, fma2(vy, vy, mul2(vx, vx))), l, il);
+        float2 nc = fma2(gs, nl2e, ncd);
+        float2 em = ex2_2(fma2(l, l2e, nc)), ep = ex2_2(fma2(l, nl2e, nc));
+        const float2 dg = mul2(mul2(sub2(em, ep), il), amp);
+        // specular lobe
+        vx = add2(snx, gx); vy = add2(sny, gy); vz = add2(snz, gz);
+        sg_len2(fma2(vz, vz, fma2(vy, vy, mul2(vx, vx))), l, il);
+        nc = fma2(gs, nl2e, nss);
+        em = ex2_2(fma2(l, l2e, nc)); ep = ex2_2(fma2(l, nl2e, nc));
+        const float2 sg = mul2(mul2(sub2(em, ep), il), sa2);
+        const float2 bx = make_float2(P2.x, P2.y), by = make_float2(P2.z, P2.w);
+        const float2 bz = make_float2(P3.x, P3.y), bw = make_float2(P3.z, P3.w);
+        dx = fma2(dg, bx, dx); dy = fma2(dg, by, dy); dz = fma2(dg, bz, dz); dw = fma2(dg, bw, dw);
+        ex = fma2(sg, bx, ex); ey = fma2(sg, by, ey); ez = fma2(sg, bz, ez); ew = fma2(sg, bw, ew);
+    }
+    const float4 d = make_float4(dx.x + dx.y, dy.x + dy.y, dz.x + dz.y, dw.x + dw.y);
+    const float4 e = make_float4(ex.x + ex.y, ey.x + ey.y, ez.x + ez.y, ew.x + ew.y);
+    if (isfinite(d.x) && isfinite(d.y) && isfinite(d.z) && isfinite(d.w) && isfinite(e.x) && isfinite(e.y) &&
+        isfinite(e.z) && isfinite(e.w)) {
+        de = d; se = e;
+        return;
+    }
+    float dd[4] = {0.f, 0.f, 0.f, 0.f}, ee[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int i = 0; i < K; ++i) {
+        const float4 P0 = L4[4 * (i >> 1)], P1 = L4[4 * (i >> 1) + 1], P2 = L4[4 * (i >> 1) + 2],
+                     P3 = L4[4 * (i >> 1) + 3];
+        const bool h = i & 1;
+        const float3 g = h ? f3(P0.y, P0.w, P1.y) : f3(P0.x, P0.z, P1.x);
+        const float gs = h ? P1.w : P1.z;
+        const float b[4] = {h ? P2.y : P2.x, h ? P2.w : P2.z, h ? P3.y : P3.x, h ? P3.w : P3.z};
+        float dg, sg;
+        sg_terms(dn, sn, g, gs, ss, sa, dg, sg);
+        for (int k = 0; k < 4; ++k) { add_nan_check(dd[k], dg * b[k]); add_nan_check(ee[k], sg * b[k]); }
+    }
+    de = make_float4(dd[0], dd[1], dd[2], dd[3]);
+    se = make_float4(ee[0], ee[1], ee[2], ee[3]);
+}
+
+// ---------------------------------------------------------------------------
+// Lobe gradients of the fused step, two pixels per lane: each lane walks
+// pixel PAIRS for its lobe, so every FP32 step below serves two pixels.
 
 // Two staged pixels; each field holds (first pixel, second pixel).  The
 // per-pixel factors every lobe reuses are computed once by the staging lane.

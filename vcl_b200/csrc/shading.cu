@@ -296,7 +296,7 @@ size_t sg_bwd_lp_smem(int K, int C, int nacc, int threads) {
            (size_t)(threads / 32) * 32 * (sizeof(SPix) + sizeof(SPixOut));
 }
 
-size_t sg_fwd_smem(int K, int C) { return sizeof(float) * (size_t)K * (C == 4 ? 8 : 4 + C); }
+size_t sg_fwd_smem(int K, int C) { return C == 4 ? sg_lobes4_smem(K) : sizeof(float) * (size_t)K * (4 + C); }
 size_t sg_bwd_smem(int K, int C, int nacc, int threads) {
     return sizeof(float) * ((size_t)K * (4 + C) + (size_t)(threads / 32) * K * nacc);
 }
