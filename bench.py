@@ -151,12 +151,11 @@ def fused_bytes(S, ncov):
     verts = S.views * S.nv * 16
     return {
         "raster": verts + S.nt * 12 + N * 32,                       # clip, indices -> rast + db
-        "shade_fwd": N * 32 + S.nv * 20 + texels + N * 32,          # rast, db, attributes, texels -> colour, diffuse env
-        "aa_fwd": N * 48 + verts,                                   # rast, colour -> image
-        "mse": N * 48,                                              # image, target -> grad
+        "shade_fwd": N * 32 + S.nv * 20 + texels + N * 32 + ncov * 52,  # ... -> colour, diffuse env, shading records
+        "aa_fwd_mse": N * 64 + verts,                               # rast, colour, target -> image gradient, loss
         "aa_bwd": N * 64 + verts * 2,                               # rast, colour, grad -> colour grad, clip grad
         "bwd_pix": N * 64 + texels + verts * 2,                     # rast, db, colour grad, diffuse env -> texel, clip grads
-        "sg_lobes": N * 48 + texels + S.K * 32,                     # rast, db, colour grad, texels -> lobe grads
+        "sg_lobes": ncov * (52 + 16) + S.K * 32,                    # shading records, colour grad -> lobe grads
     }
 
 

@@ -44,7 +44,7 @@ struct Fused {
     int* flags = nullptr;                      // [0] overflowed raster tiles of the last step
     float* scr = nullptr;                      // per view-vertex screen terms for the antialias kernels
     int* d_step = nullptr;                     // [0] step counter, [8] shading records of this step
-    double* d_corr = nullptr;    // 1 - beta1^t', 1 - beta2^t'
+    double* d_corr = nullptr;    // [0..1] 1 - beta1^t', 1 - beta2^t'; [2] loss sum, [3] its block counter
     cudaGraph_t graph_def = nullptr;           // the captured step (child of batch graphs)
     cudaGraphExec_t graph = nullptr;
     int graph_mode = -1;
@@ -196,27 +196,6 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
     sg_env4(sm4, a.K, q.n, q.pax, q.ss, q.sa, de, se);
     diffenv[p] = de;
     color[p] = make_float4(q.dfs.x * de.x + se.x, q.dfs.y * de.y + se.y, q.dfs.z * de.z + se.z, q.dfs.w * de.w + se.w);
-}
-
-// loss.cu:22-30: gradient and loss in one pass.
-__global__ void k_mse_init(const float4* __restrict__ aa, const float4* __restrict__ tgt, long long n4,
-                           float4* __restrict__ g_aa, float* __restrict__ loss) {
-    __shared__ double part[32];
-    double acc = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
-        float4 a = aa[i], t = tgt[i];
-        float4 g = make_float4(a.x - t.x, a.y - t.y, a.z - t.z, a.w - t.w);
-        g_aa[i] = g;
-        acc += (double)g.x * g.x + (double)g.y * g.y + (double)g.z * g.z + (double)g.w * g.w;
-    }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if (threadIdx.x == 0) atomicAdd(loss, (float)(acc * 0.5));
-    }
 }
 
 // Per-pixel backward below the SG stage: the diffuse gradient is
@@ -553,6 +532,7 @@ vcl_status fused_init(vcl_fit* f) {
     if (e == cudaSuccess) e = cudaMallocAsync(&F->flags, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->scr, sizeof(float) * 8 * (size_t)d.views * d.nv, as);
     if (e == cudaSuccess) e = cudaMemsetAsync(F->flags, 0, 64, as);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F->d_corr, 0, 64, as);
     if (e == cudaSuccess) e = cudaMemcpyAsync(F->d_step, &f->step_count, sizeof(int), cudaMemcpyHostToDevice, as);
     if (e == cudaSuccess) e = cudaStreamSynchronize(as);
     if (e != cudaSuccess) {
@@ -771,11 +751,14 @@ vcl_status stage_shade(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     return vcl_launch_check(f->ctx, "fused shade");
 }
 
-vcl_status stage_mse(vcl_fit* f, cudaStream_t s) {
-    const long long N = (long long)f->d.W * f->d.H * f->d.views;
-    k_mse_init<<<f->ctx->sm_count * 4, 256, 0, s>>>((const float4*)f->aa, (const float4*)f->target, N,
-                                                    (float4*)f->g_aa, f->loss);
-    return vcl_launch_check(f->ctx, "fused mse");
+// Antialias forward fused with the MSE (loss.cu:22-30): writes the loss
+// gradient of the antialiased image and the loss; the image itself is not
+// kept.  The double loss sum and its block counter live in d_corr[2..3].
+vcl_status stage_aa_mse(vcl_fit* f, cudaStream_t s) {
+    const vcl_fit_desc& d = f->d;
+    Fused* F = (Fused*)f->fused;
+    return aa_edges_fwd_mse(f->ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, d.W, d.H, d.views, f->color,
+                            f->target, f->g_aa, F->d_corr + 2, reinterpret_cast<unsigned*>(F->d_corr + 3), f->loss, s);
 }
 
 vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
@@ -831,8 +814,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     const ShadeIn a = shade_in(f);
     const TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
     TRY(stage_shade(f, a, td, s));
-    TRY(aa_edges_fwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa, s));
-    TRY(stage_mse(f, s));
+    TRY(stage_aa_mse(f, s));
     TRY(aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
                      d.learn_pos ? f->g_clip : nullptr, s));
     const bool lobes = d.learn_lobes && d.K;
@@ -935,8 +917,7 @@ vcl_status fit_step_fused(vcl_fit* f, cudaStream_t s) {
 int fit_fused_launches(const vcl_fit* f) {
     const vcl_fit_desc& d = f->d;
     int n = 1 /* begin */ + 1 /* project */ + 1 /* aa screen terms */ + raster_fwd_launches() + 1 /* shade */ +
-            1 /* aa */ + 1 /* mse */ +
-            1 /* aa bwd */;
+            1 /* aa + mse */ + 1 /* aa bwd */;
     if (d.learn_tex || d.learn_pos) n += 1; /* per-pixel backward */
     if (d.learn_lobes && d.K) n += 1;       /* lobe gradients */
     if (d.learn_pos) n += 1;
@@ -1009,8 +990,8 @@ vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, lon
     return VCL_OK;
 }
 
-const char* const kFusedKernelNames[] = {"raster", "shade_fwd", "aa_fwd", "mse", "aa_bwd", "bwd_pix", "sg_lobes"};
-constexpr int kFusedKernels = 7;
+const char* const kFusedKernelNames[] = {"raster", "shade_fwd", "aa_fwd_mse", "aa_bwd", "bwd_pix", "sg_lobes"};
+constexpr int kFusedKernels = 6;
 
 int fit_fused_kernel_count() { return kFusedKernels; }
 const char* fit_fused_kernel_name(int i) { return i >= 0 && i < kFusedKernels ? kFusedKernelNames[i] : nullptr; }
@@ -1039,12 +1020,10 @@ vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* m
                 case 0: return raster_fwd_ws(ctx, F->raster_ws, F->sched, F->flags, f->clip, d.nv, f->tri, d.nt, W, H,
                                              V, f->rast, f->db, s);
                 case 1: return stage_shade(f, a, td, s);
-                case 2: return aa_edges_fwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->aa,
-                                            s);
-                case 3: return stage_mse(f, s);
-                case 4: return aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
+                case 2: return stage_aa_mse(f, s);
+                case 3: return aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
                                             f->g_color, d.learn_pos ? f->g_clip : nullptr, s);
-                case 5: return stage_bwd_pix(f, a, td, s);
+                case 4: return stage_bwd_pix(f, a, td, s);
                 default: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;
             }
         };

@@ -613,10 +613,23 @@ DEV float4 aat_gather(const float4* s_lo, const float4* s_hi, int tx, int ty) {
     return f4add(f4add(s_hi[h], s_lo[h + 1]), f4add(s_hi[v], s_lo[v + AAT_X]));
 }
 
+// MSE: instead of the antialiased colour, write its loss gradient
+// out = aa - target and add 0.5 |aa - target|^2 to the loss (loss.cu:22-30):
+// block sums in double go to mse->sum; the last block to finish writes the
+// float loss and clears the sum and the block counter for the next pass.
+struct MseOut {
+    const float4* target;
+    double* sum;
+    unsigned* done;
+    float* loss;
+};
+
+template <bool MSE>
 __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict__ clip, const float4* __restrict__ scr_all,
                                                      int nv, const uint32_t* __restrict__ tri, int nt,
                                                      const float4* __restrict__ rast, int W, int H,
-                                                     const float4* __restrict__ in, float4* __restrict__ out, int* flags) {
+                                                     const float4* __restrict__ in, float4* __restrict__ out, int* flags,
+                                                     MseOut mse) {
     __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
     __shared__ int s_list[AAT_NP], s_n;
     const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
@@ -650,9 +663,36 @@ __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict
     __syncthreads();
     const int tx = threadIdx.x % AAT_X, ty = threadIdx.x / AAT_X;
     const int px = x0 + tx, py = y0 + ty;
-    if (px >= W || py >= H) return;
+    const bool inside = px < W && py < H;
     const long long p = vb + (long long)py * W + px;
-    out[p] = f4add(in[p], aat_gather(s_lo, s_hi, tx, ty));
+    if (!MSE) {
+        if (inside) out[p] = f4add(in[p], aat_gather(s_lo, s_hi, tx, ty));
+        return;
+    }
+    double acc = 0.0;
+    if (inside) {
+        const float4 a = f4add(in[p], aat_gather(s_lo, s_hi, tx, ty)), t = mse.target[p];
+        const float4 g = make_float4(a.x - t.x, a.y - t.y, a.z - t.z, a.w - t.w);
+        out[p] = g;
+        acc = (double)g.x * g.x + (double)g.y * g.y + (double)g.z * g.z + (double)g.w * g.w;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += part[w];
+        atomicAdd(mse.sum, b);
+        __threadfence();
+        const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
+        if (atomicAdd(mse.done, 1u) == nblk - 1) {
+            const double total = atomicAdd(mse.sum, 0.0);
+            *mse.loss = (float)(total * 0.5);
+            *mse.sum = 0.0;
+            *mse.done = 0u;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict__ clip, const float4* __restrict__ scr_all,
@@ -784,12 +824,25 @@ vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int n
     long long npix = (long long)W * H * views;
     const float4* sc = (const float4*)scr;
     if (C == 4 && aligned16(in) && aligned16(out) && views <= 65535)
-        k_aa_fwd_tile<<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
-                                                             H, (const float4*)in, (float4*)out, ctx->dev_flags);
+        k_aa_fwd_tile<false><<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt,
+                                                                    (const float4*)rast, W, H, (const float4*)in,
+                                                                    (float4*)out, ctx->dev_flags, MseOut{});
     else
         k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                          H, npix, C, in, out, ctx->dev_flags);
     return vcl_launch_check(ctx, "antialias_fwd");
+}
+
+vcl_status aa_edges_fwd_mse(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                            const float* rast, int W, int H, int views, const float* in, const float* target,
+                            float* grad, double* sum, unsigned* done, float* loss, cudaStream_t s) {
+    VCL_REQUIRE(aligned16(in) && aligned16(target) && aligned16(grad) && views <= 65535,
+                "antialias+mse: 16-byte aligned C = 4 buffers and at most 65535 views");
+    k_aa_fwd_tile<true><<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, (const float4*)scr, nv, tri, nt,
+                                                               (const float4*)rast, W, H, (const float4*)in,
+                                                               (float4*)grad, ctx->dev_flags,
+                                                               MseOut{(const float4*)target, sum, done, loss});
+    return vcl_launch_check(ctx, "antialias_fwd+mse");
 }
 
 vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,

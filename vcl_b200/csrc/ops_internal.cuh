@@ -6,6 +6,12 @@
 // completely, the reference's initial copy included).
 vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                         const float* rast, int W, int H, int views, int C, const float* in, float* out, cudaStream_t s);
+// Antialias forward (C = 4) fused with the MSE: writes grad = aa - target and
+// the loss 0.5 sum |aa - target|^2 (through the double `sum` and block counter
+// `done`, both zero before the first call and left zero after each call).
+vcl_status aa_edges_fwd_mse(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
+                            const float* rast, int W, int H, int views, const float* in, const float* target,
+                            float* grad, double* sum, unsigned* done, float* loss, cudaStream_t s);
 vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                         const float* rast, int W, int H, int views, int C, const float* in, const float* grad_out,
                         float* grad_in, float* grad_clip, cudaStream_t s);

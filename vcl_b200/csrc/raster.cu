@@ -125,24 +125,46 @@ DEV bool tile_overlaps(const RTri& r, int tx, int ty, int T, int W, int H) {
 }
 
 // Conservative column range [x0, x1] of pixel row `sy` for a triangle: each
-// edge function is linear in sx, so every edge bounds sx from one side.  The
+// edge function is linear in (sx, sy), so every edge with a non-zero sx
+// coefficient bounds sx from one side by a linear function of sy, set up
+// once per triangle (span_setup) and evaluated with one fma per row.  The
 // bound is relaxed by a margin far above the rounding of the per-pixel edge
-// evaluation and widened by one pixel each way; pixels outside the range
-// cannot be covered, pixels inside still go through the exact test.  False
-// when the row certainly has no covered pixel.
-DEV bool row_span(const RTri& r, float sy, int W, int& x0, int& x1) {
+// evaluation (and of the bound itself) and widened by one pixel each way;
+// pixels outside the range cannot be covered, pixels inside still go through
+// the exact test.  False when the row certainly has no covered pixel.
+struct SpanEq {
+    float al[3], be[3];   // sx bound of edge i: al*sy + be (lower when side > 0, upper when side < 0)
+    int side[3];          // 0: the edge does not depend on sx
+};
+
+DEV void span_setup(const RTri& r, SpanEq& q) {
     const float sg = r.a.w;
     const float ea[3] = {r.a.x, r.a.y, r.a.z}, eb[3] = {r.b.x, r.b.y, r.b.z}, ek[3] = {r.k.x, r.k.y, r.k.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float a = sg * ea[i];
+        const float m = 1e-5f * (fabsf(ea[i]) + fabsf(eb[i]) + fabsf(ek[i]));
+        const float ia = a != 0.f ? 1.f / a : 0.f;
+        q.al[i] = -(sg * eb[i]) * ia;
+        q.be[i] = (-(sg * ek[i]) - m) * ia;
+        q.side[i] = a > 0.f ? 1 : a < 0.f ? -1 : 0;
+    }
+}
+
+DEV bool row_span(const RTri& r, const SpanEq& q, float sy, int W, int& x0, int& x1) {
     float lo = -2.f, hi = 2.f;     // sx range of interest (the screen is [-1, 1])
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-        const float a = sg * ea[i], c = sg * (eb[i] * sy + ek[i]);
-        const float m = 1e-5f * (fabsf(ea[i]) + fabsf(eb[i]) + fabsf(ek[i]));
-        if (a > 0.f) lo = fmaxf(lo, (-c - m) / a);
-        else if (a < 0.f) hi = fminf(hi, (-c - m) / a);
-        else if (c < -m) return false;
+        if (q.side[i] > 0) lo = fmaxf(lo, fmaf(q.al[i], sy, q.be[i]));
+        else if (q.side[i] < 0) hi = fminf(hi, fmaf(q.al[i], sy, q.be[i]));
+        else {
+            const float eb = i == 0 ? r.b.x : i == 1 ? r.b.y : r.b.z, ek = i == 0 ? r.k.x : i == 1 ? r.k.y : r.k.z;
+            const float ea = i == 0 ? r.a.x : i == 1 ? r.a.y : r.a.z;
+            const float m = 1e-5f * (fabsf(ea) + fabsf(eb) + fabsf(ek));
+            if (r.a.w * (eb * sy + ek) < -m) return false;
+        }
     }
-    if (lo > hi) return false;     // (fmaxf/fminf drop NaN bounds, so lo and hi are numbers)
+    if (!(lo <= hi)) return false;     // (fmaxf/fminf drop NaN bounds; a NaN row bound leaves lo/hi as numbers)
     const float fw = (float)W;
     x0 = max(r.box.x, (int)floorf(fmaf(lo, fw, fw - 1.f) * 0.5f) - 1);
     x1 = min(r.box.y, (int)ceilf(fmaf(hi, fw, fw - 1.f) * 0.5f) + 1);
@@ -216,10 +238,12 @@ __global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t*
     if (r.box.x > r.box.y || r.box.z > r.box.w) return;
     if (is_small(r.box, small_area)) {
         unsigned long long* kv = keys + (size_t)view * W * H;
+        SpanEq q;
+        span_setup(r, q);
         for (int py = r.box.z; py <= r.box.w; ++py) {
             const float sy = s_ndc[W + py];
             int x0, x1;
-            if (!row_span(r, sy, W, x0, x1)) continue;
+            if (!row_span(r, q, sy, W, x0, x1)) continue;
             for (int px = x0; px <= x1; ++px) {
                 float zw;
                 if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
@@ -385,11 +409,13 @@ __global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, 
         const int view = gid / nt, t = gid - view * nt;
         const RTri r = setup[gid];
         unsigned long long* kv = keys + (size_t)view * W * H;
+        SpanEq q;
+        span_setup(r, q);
         // lane per row; each lane walks only its row's conservative span
         for (int py = r.box.z + lane; py <= r.box.w; py += 32) {
             const float sy = s_ndc[W + py];
             int x0, x1;
-            if (!row_span(r, sy, W, x0, x1)) continue;
+            if (!row_span(r, q, sy, W, x0, x1)) continue;
             for (int px = x0; px <= x1; ++px) {
                 float zw;
                 if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
