@@ -128,10 +128,12 @@ DEV bool tile_overlaps(const RTri& r, int tx, int ty, int T, int W, int H) {
 // edge function is linear in (sx, sy), so every edge with a non-zero sx
 // coefficient bounds sx from one side by a linear function of sy, set up
 // once per triangle (span_setup) and evaluated with one fma per row.  The
-// bound is relaxed by a margin far above the rounding of the per-pixel edge
-// evaluation (and of the bound itself) and widened by one pixel each way;
-// pixels outside the range cannot be covered, pixels inside still go through
-// the exact test.  False when the row certainly has no covered pixel.
+// bound is relaxed by a margin m = 1e-5 (|a| + |b| + |k|) in edge units, far
+// above both the rounding of the per-pixel edge evaluation (a few ulps of the
+// same sum) and that of the bound itself (a few ulps of (|b sy| + |k| + m)/|a|
+// in sx), then rounded outwards to whole pixels; pixels outside the range
+// cannot be covered, pixels inside still go through the exact test.  False
+// when the row certainly has no covered pixel.
 struct SpanEq {
     float al[3], be[3];   // sx bound of edge i: al*sy + be (lower when side > 0, upper when side < 0)
     int side[3];          // 0: the edge does not depend on sx
@@ -166,8 +168,8 @@ DEV bool row_span(const RTri& r, const SpanEq& q, float sy, int W, int& x0, int&
     }
     if (!(lo <= hi)) return false;     // (fmaxf/fminf drop NaN bounds; a NaN row bound leaves lo/hi as numbers)
     const float fw = (float)W;
-    x0 = max(r.box.x, (int)floorf(fmaf(lo, fw, fw - 1.f) * 0.5f) - 1);
-    x1 = min(r.box.y, (int)ceilf(fmaf(hi, fw, fw - 1.f) * 0.5f) + 1);
+    x0 = max(r.box.x, (int)floorf(fmaf(lo, fw, fw - 1.f) * 0.5f));
+    x1 = min(r.box.y, (int)ceilf(fmaf(hi, fw, fw - 1.f) * 0.5f));
     return x0 <= x1;
 }
 
@@ -214,53 +216,115 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
     t.box = make_int4(bx0, bx1, by0, by1);
 }
 
-__global__ void k_setup(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W, int H,
+// A small triangle staged in shared memory for the row-balanced raster loop
+// of k_setup: its record, its row-span bounds and (triangle, view).  144
+// bytes, so that lanes reading different slots spread over the banks.
+struct __align__(16) SmallTri {
+    float4 a, b, k, z, w;
+    float4 s0;     // al0 be0 al1 be1
+    float4 s1;     // al2 be2 (sides + 1: 2 bits each) | view << 8, triangle
+    int4 box;
+    float4 pad;
+};
+constexpr int SETUP_THREADS = 256;
+
+DEV void small_pack(SmallTri& o, const RTri& r, const SpanEq& q, int t, int view) {
+    o.a = r.a; o.b = r.b; o.k = r.k; o.z = r.z; o.w = r.w; o.box = r.box;
+    o.s0 = make_float4(q.al[0], q.be[0], q.al[1], q.be[1]);
+    const int code = (q.side[0] + 1) | ((q.side[1] + 1) << 2) | ((q.side[2] + 1) << 4) | (view << 8);
+    o.s1 = make_float4(q.al[2], q.be[2], __int_as_float(code), __int_as_float(t));
+}
+
+size_t setup_smem(int W, int H) {
+    return sizeof(float) * (size_t)((W + H + 3) & ~3) + sizeof(SmallTri) * SETUP_THREADS;
+}
+
+// 1. setup (see the file comment).  The small triangles of a warp are then
+// rasterized together: their rows are dealt round-robin to the 32 lanes, so
+// that a lane with a tall triangle does not hold up the others.
+__global__ void __launch_bounds__(SETUP_THREADS, 4) k_setup(const float4* __restrict__ clip, int nv,
+                        const uint32_t* __restrict__ tri, int nt, int W, int H,
                         int views, int tile, int tiles_x, int ntiles, RTri* __restrict__ setup, int* __restrict__ count,
                         int* __restrict__ flags, unsigned long long* __restrict__ keys, int small_area, int med_area,
                         int* __restrict__ med_list, int* __restrict__ med_count) {
-    extern __shared__ float s_ndc[];   // [W] column centres, [H] row centres
+    extern __shared__ float s_ndc[];   // [W] column centres, [H] row centres, then the small-triangle slots
+    SmallTri* s_tri = reinterpret_cast<SmallTri*>(s_ndc + ((W + H + 3) & ~3));
+    __shared__ int s_start[SETUP_THREADS / 32][32];
     stage_ndc(s_ndc, W, H);
     __syncthreads();
-    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)views * nt) return;
-    int view = (int)(gid / nt), t = (int)(gid % nt);
-    uint32_t i0 = tri[3 * (size_t)t], i1 = tri[3 * (size_t)t + 1], i2 = tri[3 * (size_t)t + 2];
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in_range = gid < (long long)views * nt;
+    const int view = in_range ? (int)(gid / nt) : 0, t = in_range ? (int)(gid % nt) : 0;
     RTri r;
-    bool valid = false;
-    if (i0 < (uint32_t)nv && i1 < (uint32_t)nv && i2 < (uint32_t)nv) {
-        const float4* cv = clip + (size_t)view * nv;
-        setup_tri(cv[i0], cv[i1], cv[i2], W, H, r, valid);
-    } else {
-        atomicOr(&flags[1], 1);  // out-of-range vertex index: triangle dropped
-        r.box = make_int4(1, 0, 1, 0);
+    r.box = make_int4(1, 0, 1, 0);
+    if (in_range) {
+        uint32_t i0 = tri[3 * (size_t)t], i1 = tri[3 * (size_t)t + 1], i2 = tri[3 * (size_t)t + 2];
+        bool valid = false;
+        if (i0 < (uint32_t)nv && i1 < (uint32_t)nv && i2 < (uint32_t)nv) {
+            const float4* cv = clip + (size_t)view * nv;
+            setup_tri(cv[i0], cv[i1], cv[i2], W, H, r, valid);
+        } else {
+            atomicOr(&flags[1], 1);  // out-of-range vertex index: triangle dropped
+            r.box = make_int4(1, 0, 1, 0);
+        }
+        setup[gid] = r;
     }
-    setup[gid] = r;
-    if (r.box.x > r.box.y || r.box.z > r.box.w) return;
-    if (is_small(r.box, small_area)) {
-        unsigned long long* kv = keys + (size_t)view * W * H;
+    const bool has = r.box.x <= r.box.y && r.box.z <= r.box.w;
+    const bool small = has && is_small(r.box, small_area);
+    if (has && !small) {
+        if (box_area(r.box) <= med_area) {
+            med_list[atomicAdd(med_count, 1)] = (int)gid;   // one warp rasterizes it (k_medium)
+        } else {
+            int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
+            int* cnt = count + (size_t)view * ntiles;
+            for (int ty = ty0; ty <= ty1; ++ty)
+                for (int tx = tx0; tx <= tx1; ++tx)
+                    if (tile_overlaps(r, tx, ty, tile, W, H)) atomicAdd(&cnt[ty * tiles_x + tx], 1);
+        }
+    }
+    // row-balanced raster of the warp's small triangles: every covered pixel
+    // gets a 64-bit atomicMin of its key (depth, triangle id)
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int rows = small ? r.box.w - r.box.z + 1 : 0;
+    int incl = rows;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;
+    int* start = s_start[wib];
+    SmallTri* st = s_tri + wib * 32;
+    start[lane] = incl - rows;
+    if (small) {
         SpanEq q;
         span_setup(r, q);
-        for (int py = r.box.z; py <= r.box.w; ++py) {
-            const float sy = s_ndc[W + py];
-            int x0, x1;
-            if (!row_span(r, q, sy, W, x0, x1)) continue;
-            for (int px = x0; px <= x1; ++px) {
-                float zw;
-                if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
-                    atomicMin(&kv[(size_t)py * W + px], depth_key(zw, t));
-            }
+        small_pack(st[lane], r, q, t, view);
+    }
+    __syncwarp();
+    for (int k = lane; k < total; k += 32) {
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+            if (start[j + step] <= k) j += step;
+        const SmallTri& S = st[j];
+        RTri rr;
+        rr.a = S.a; rr.b = S.b; rr.k = S.k; rr.z = S.z; rr.w = S.w; rr.box = S.box;
+        const float4 s0 = S.s0, s1 = S.s1;
+        const int code = __float_as_int(s1.z), tj = __float_as_int(s1.w);
+        SpanEq q;
+        q.al[0] = s0.x; q.be[0] = s0.y; q.al[1] = s0.z; q.be[1] = s0.w; q.al[2] = s1.x; q.be[2] = s1.y;
+        q.side[0] = (code & 3) - 1; q.side[1] = ((code >> 2) & 3) - 1; q.side[2] = ((code >> 4) & 3) - 1;
+        const int py = rr.box.z + (k - start[j]);
+        const float sy = s_ndc[W + py];
+        int x0, x1;
+        if (!row_span(rr, q, sy, W, x0, x1)) continue;
+        unsigned long long* kv = keys + (size_t)(code >> 8) * W * H + (size_t)py * W;
+        for (int px = x0; px <= x1; ++px) {
+            float zw;
+            if (pixel_test(rr.a, rr.b, rr.k, rr.z, rr.w, s_ndc[px], sy, zw)) atomicMin(&kv[px], depth_key(zw, tj));
         }
-        return;
     }
-    if (box_area(r.box) <= med_area) {
-        med_list[atomicAdd(med_count, 1)] = (int)gid;   // one warp rasterizes it (k_medium)
-        return;
-    }
-    int tx0 = r.box.x / tile, tx1 = r.box.y / tile, ty0 = r.box.z / tile, ty1 = r.box.w / tile;
-    int* cnt = count + (size_t)view * ntiles;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx)
-            if (tile_overlaps(r, tx, ty, tile, W, H)) atomicAdd(&cnt[ty * tiles_x + tx], 1);
 }
 
 // Exclusive scan of n ints by one CTA of 32 warps: warp w owns a contiguous
@@ -580,11 +644,10 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     long long work = (long long)views * nt;
     if (work > 0) {
         const size_t tab = sizeof(float) * (size_t)(W + H);
-        if (tab > 48 * 1024) {
-            cudaFuncSetAttribute(k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
-            cudaFuncSetAttribute(k_medium, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
-        }
-        k_setup<<<vcl_blocks(work, 256), 256, tab, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
+        const size_t stab = setup_smem(W, H);
+        if (stab > 48 * 1024) cudaFuncSetAttribute(k_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stab);
+        if (tab > 48 * 1024) cudaFuncSetAttribute(k_medium, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+        k_setup<<<vcl_blocks(work, SETUP_THREADS), SETUP_THREADS, stab, s>>>((const float4*)clip, nv, tri, nt, W, H, views, T, tiles_x,
                                                          (int)ntiles_view, w.setup, w.count, flags, w.keys, sa, ma,
                                                          w.med_list, w.count + ntiles);
         k_medium<<<ctx->sm_count * 8, 256, tab, s>>>(w.setup, nt, W, H, w.med_list, w.count + ntiles, w.keys);
