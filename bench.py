@@ -159,11 +159,21 @@ def fused_bytes(S, ncov):
     }
 
 
-# DRAM bytes per pixel of the lobe-gradient stage measured by an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum of one launch on 4 views of
-# 1024x1024 of this workload, divided by the pixels); the stage's traffic
+# DRAM bytes per pixel of the fused step's two largest kernels, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch on 4
+# views of 1024x1024 of this workload, divided by the pixels); their traffic
 # grows with the pixel count.
-SG_LOBES_DRAM_BYTES_PER_PIXEL = 215.8e6 / (4 * 1024 * 1024)
+DRAM_BYTES_PER_PIXEL = {
+    "bwd_pix": (290.7e6 + 46.6e6) / (4 * 1024 * 1024),
+    "sg_lobes": (179.5e6 + 5.0e6) / (4 * 1024 * 1024),
+}
+# What bounds each of them instead of HBM bandwidth (same capture).
+BOUND_NOTE = {
+    "bwd_pix": "k_bwd_pix is bound by the scatter of texel and vertex gradients through L2 (vector reductions; "
+               "L2 ~51% busy, warps waiting on loads and the LSU queue), not by HBM bandwidth",
+    "sg_lobes": "k_sg_lobes is FP32/MUFU-bound (per pixel and lobe: 2 rsqrt, 4 ex2, ~35 paired FP32 ops), "
+                "not HBM-bound",
+}
 
 
 # ------------------------------------------------------------------ vcl arm
@@ -511,12 +521,11 @@ def main():
         b = byts[top]
         achieved = b / (kms[top] * 1e-3) / 1e9
         N = S.W * S.H * S.views
-        traffic = SG_LOBES_DRAM_BYTES_PER_PIXEL * N if top == "sg_lobes" else None
+        traffic = DRAM_BYTES_PER_PIXEL[top] * N if top in DRAM_BYTES_PER_PIXEL else None
         line["roofline"] = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                             "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
                             "algorithmic_bytes": b, "avg_ms": kms[top],
-                            "note": ("k_sg_lobes is FP32/MUFU issue-bound (per pixel and lobe: 2 rsqrt, 4 ex2, "
-                                     "~80 FP32 ops), not HBM-bound" if top == "sg_lobes" else None)}
+                            "note": BOUND_NOTE.get(top)}
         line["fused_kernels_ms"] = {k: round(v, 4) for k, v in kms.items()}
         line["fused_kernels_frac_hbm"] = {k: round(byts[k] / (v * 1e-3) / 1e9 / hbm_peak, 3)
                                           for k, v in kms.items() if v > 0}
