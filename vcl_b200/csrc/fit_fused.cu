@@ -202,22 +202,40 @@ __global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4
 // grad ⊙ diffenv (material.cu:429 summed over the lobes), then texture
 // backward (texturemap.cu:229-284), interpolate backward to the
 // barycentrics (interpolate.cu:114-143) and raster backward
-// (rasterize.cu:84-141), scattered with vector reductions.  Held to 40
-// registers so that its blocks fit on the SMs beside the lobe-gradient
-// blocks it runs with.
-__global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
-                                                 const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
-                                                 const float* __restrict__ clip, float* __restrict__ g_clip,
-                                                 int want_tex, int want_geom) {
-    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.npix) return;
+// (rasterize.cu:84-141), scattered with vector reductions.
+// The clip-position gradient of one pixel's three vertices (x, y, w each;
+// z receives +0) and the triangle they belong to.
+struct VtxGrad {
+    float v[9];
+    uint32_t i[3];
+    int view;
+    bool ok;
+};
+
+// One covered pixel's texture sample: its two levels, the 2x2 cells (corner
+// u0, v0; the other corner is u0 or u0 + 1, v0 or v0 + 1) with their
+// fractions, and the gradient g = dL/dcolour * diffuse env it spreads over
+// the texels.
+struct PixSample {
+    float4 r, g;
+    float2 f0, f1;
+    float fl;
+    int l0, l1, u0, v0, u1, v1, s0, t0, s1, t1;
+    uint32_t i0, i1, i2;
+    int idx;
+    bool tri, ok;
+};
+
+DEV void pix_sample(const ShadeIn& a, const TexDesc& td, const float4* __restrict__ g_color,
+                    const float4* __restrict__ diffenv, long long p, PixSample& S) {
+    S.ok = false;
     const float4 r = a.rast[p];
     const int idx = rast_id(r.w);
     if (idx < 0 || idx >= a.nt) return;
     const uint32_t i0 = a.tri[3 * (size_t)idx], i1 = a.tri[3 * (size_t)idx + 1], i2 = a.tri[3 * (size_t)idx + 2];
     if (i0 >= (uint32_t)a.nv || i1 >= (uint32_t)a.nv || i2 >= (uint32_t)a.nv) return;
     const float4 gc = g_color[p], de = diffenv[p];
-    const float4 g = make_float4(gc.x * de.x, gc.y * de.y, gc.z * de.z, gc.w * de.w);
+    S.g = make_float4(gc.x * de.x, gc.y * de.y, gc.z * de.z, gc.w * de.w);
     // uv and its screen derivatives (interpolate.cu:20-49)
     const float4 d = a.db[p];
     const double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
@@ -231,43 +249,44 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
         dy[i] = addr(mulr(dadu, d.y), mulr(dadv, d.w));
     }
     const float2 uv = make_float2(u[0], u[1]);
-    int l0 = 0, l1 = 0;
-    float fl = 0.f;
+    S.l0 = 0; S.l1 = 0; S.fl = 0.f;
     const bool mip = td.L > 1;
-    if (mip) calc_level(td, make_float4(dx[0], dy[0], dx[1], dy[1]), l0, l1, fl, nullptr, 0);
-    int q0[4], q1[4];
-    float2 f0, f1 = make_float2(0.f, 0.f);
-    index_fetch(td, l0, uv, q0, f0);
-    const bool tri = mip && fl > 0;
-    if (tri) index_fetch(td, l1, uv, q1, f1);
-    const float wl0 = mip ? 1.f - fl : 1.f;
-    if (want_tex) {
-        float* G0 = g_pyr + td.off[l0];
-        float w00 = wl0 * (1.f - f0.x) * (1.f - f0.y), w01 = wl0 * f0.x * (1.f - f0.y);
-        float w10 = wl0 * (1.f - f0.x) * f0.y, w11 = wl0 * f0.x * f0.y;
-        red_add4(G0 + 4 * q0[0], w00 * g.x, w00 * g.y, w00 * g.z, w00 * g.w);
-        red_add4(G0 + 4 * q0[1], w01 * g.x, w01 * g.y, w01 * g.z, w01 * g.w);
-        red_add4(G0 + 4 * q0[2], w10 * g.x, w10 * g.y, w10 * g.z, w10 * g.w);
-        red_add4(G0 + 4 * q0[3], w11 * g.x, w11 * g.y, w11 * g.z, w11 * g.w);
-        if (tri) {
-            float* G1 = g_pyr + td.off[l1];
-            float v00 = fl * (1.f - f1.x) * (1.f - f1.y), v01 = fl * f1.x * (1.f - f1.y);
-            float v10 = fl * (1.f - f1.x) * f1.y, v11 = fl * f1.x * f1.y;
-            red_add4(G1 + 4 * q1[0], v00 * g.x, v00 * g.y, v00 * g.z, v00 * g.w);
-            red_add4(G1 + 4 * q1[1], v01 * g.x, v01 * g.y, v01 * g.z, v01 * g.w);
-            red_add4(G1 + 4 * q1[2], v10 * g.x, v10 * g.y, v10 * g.z, v10 * g.w);
-            red_add4(G1 + 4 * q1[3], v11 * g.x, v11 * g.y, v11 * g.z, v11 * g.w);
-        }
-    }
-    if (!want_geom) return;
-    const float* T0 = a.pyr + td.off[l0];
-    const float* T1 = a.pyr + td.off[l1];
-    const float s0x = (float)(td.tw >> l0), s0y = (float)(td.th >> l0);
-    const float s1x = (float)(td.tw >> l1), s1y = (float)(td.th >> l1);
-    const float4 a00 = ld4(T0, q0[0]), a01 = ld4(T0, q0[1]), a10 = ld4(T0, q0[2]), a11 = ld4(T0, q0[3]);
+    if (mip) calc_level(td, make_float4(dx[0], dy[0], dx[1], dy[1]), S.l0, S.l1, S.fl, nullptr, 0);
+    cell_fetch(td, S.l0, uv, S.u0, S.u1, S.v0, S.v1, S.f0);
+    S.tri = mip && S.fl > 0;
+    S.f1 = make_float2(0.f, 0.f);
+    S.s0 = S.s1 = S.t0 = S.t1 = 0;
+    if (S.tri) cell_fetch(td, S.l1, uv, S.s0, S.s1, S.t0, S.t1, S.f1);
+    if (!mip) S.fl = 0.f;
+    S.r = r;
+    S.i0 = i0; S.i1 = i1; S.i2 = i2;
+    S.idx = idx;
+    S.ok = true;
+}
+
+// One texel's share of a pixel's texture gradient (texturemap.cu:229-284).
+DEV void tex_add(const TexDesc& td, float* __restrict__ g_pyr, int level, int x, int y, float wt, float4 g) {
+    red_add4(g_pyr + td.off[level] + 4 * ((size_t)y * (td.tw >> level) + x), wt * g.x, wt * g.y, wt * g.z, wt * g.w);
+}
+
+// Geometry part: d colour / d uv from the texel values, back to the
+// barycentrics (interpolate.cu:114-143) and to the three clip-space vertices
+// (rasterize.cu:84-141).
+DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__ clip, const PixSample& S, int px,
+                  int py, int view, VtxGrad& o) {
+    const float* T0 = a.pyr + td.off[S.l0];
+    const float* T1 = a.pyr + td.off[S.l1];
+    const int sx0 = td.tw >> S.l0, sx1 = td.tw >> S.l1;
+    const float s0x = (float)sx0, s0y = (float)(td.th >> S.l0);
+    const float s1x = (float)sx1, s1y = (float)(td.th >> S.l1);
+    const float4 a00 = ld4(T0, S.v0 * sx0 + S.u0), a01 = ld4(T0, S.v0 * sx0 + S.u1);
+    const float4 a10 = ld4(T0, S.v1 * sx0 + S.u0), a11 = ld4(T0, S.v1 * sx0 + S.u1);
     float4 b00 = a00, b01 = a00, b10 = a00, b11 = a00;
-    if (tri) { b00 = ld4(T1, q1[0]); b01 = ld4(T1, q1[1]); b10 = ld4(T1, q1[2]); b11 = ld4(T1, q1[3]); }
-    const float ga[4] = {g.x, g.y, g.z, g.w};
+    if (S.tri) {
+        b00 = ld4(T1, S.t0 * sx1 + S.s0); b01 = ld4(T1, S.t0 * sx1 + S.s1);
+        b10 = ld4(T1, S.t1 * sx1 + S.s0); b11 = ld4(T1, S.t1 * sx1 + S.s1);
+    }
+    const float ga[4] = {S.g.x, S.g.y, S.g.z, S.g.w};
     const float A00[4] = {a00.x, a00.y, a00.z, a00.w}, A01[4] = {a01.x, a01.y, a01.z, a01.w};
     const float A10[4] = {a10.x, a10.y, a10.z, a10.w}, A11[4] = {a11.x, a11.y, a11.z, a11.w};
     const float B00[4] = {b00.x, b00.y, b00.z, b00.w}, B01[4] = {b01.x, b01.y, b01.z, b01.w};
@@ -275,11 +294,11 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
     float gu = 0.f, gv = 0.f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], f0.y) * s0x;
-        float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], f0.x) * s0y;
-        if (tri) {
-            du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], f1.y) * s1x, fl);
-            dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], f1.x) * s1y, fl);
+        float du = lerpf_(A01[i] - A00[i], A11[i] - A10[i], S.f0.y) * s0x;
+        float dv = lerpf_(A10[i] - A00[i], A11[i] - A01[i], S.f0.x) * s0y;
+        if (S.tri) {
+            du = lerpf_(du, lerpf_(B01[i] - B00[i], B11[i] - B10[i], S.f1.y) * s1x, S.fl);
+            dv = lerpf_(dv, lerpf_(B10[i] - B00[i], B11[i] - B01[i], S.f1.x) * s1y, S.fl);
         }
         gu += du * ga[i];
         gv += dv * ga[i];
@@ -288,35 +307,99 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
         float gi = i == 0 ? gu : gv;
-        float a2 = a.uvattr[2 * i2 + i];
-        gbu += gi * (a.uvattr[2 * i0 + i] - a2);
-        gbv += gi * (a.uvattr[2 * i1 + i] - a2);
+        float a2 = a.uvattr[2 * S.i2 + i];
+        gbu += gi * (a.uvattr[2 * S.i0 + i] - a2);
+        gbv += gi * (a.uvattr[2 * S.i1 + i] - a2);
     }
     if (((__float_as_uint(gbu) | __float_as_uint(gbv)) << 1) == 0u) return;
-    const long long hw = (long long)a.W * a.H;
-    const int view = (int)(p / hw);
-    const int rem = (int)(p - view * hw);
-    const int py = rem / a.W, px = rem - py * a.W;
     const float xs = 2.f / (float)a.W, ys = 2.f / (float)a.H;
     const float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
     const float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
     const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * a.nv;
-    const float4 c0 = cv[i0], c1 = cv[i1], c2 = cv[i2];
+    const float4 c0 = cv[S.i0], c1 = cv[S.i1], c2 = cv[S.i2];
     float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
     float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
     float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
     float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
     float ar = e0x * e1y - e0y * e1x;
     float ia = 1.f / (ar + (ar > 0 ? 1e-6f : -1e-6f));
-    float kuv = r.x * gbu + r.y * gbv;
+    float kuv = S.r.x * gbu + S.r.y * gbv;
     float gx0 = (gbv * p2y + kuv * e1y) * ia, gy0 = (-gbv * p2x - kuv * e1x) * ia;
     float gx1 = (-gbu * p2y - kuv * e0y) * ia, gy1 = (gbu * p2x + kuv * e0x) * ia;
     float gx2 = ((-gbv * p0y + gbu * p1y) - kuv * (-p0y + p1y)) * ia;
     float gy2 = ((gbv * p0x - gbu * p1x) - kuv * (p0x - p1x)) * ia;
+    o.v[0] = gx0; o.v[1] = gy0; o.v[2] = -gx0 * pxn - gy0 * pyn;
+    o.v[3] = gx1; o.v[4] = gy1; o.v[5] = -gx1 * pxn - gy1 * pyn;
+    o.v[6] = gx2; o.v[7] = gy2; o.v[8] = -gx2 * pxn - gy2 * pyn;
+    o.i[0] = S.i0; o.i[1] = S.i1; o.i[2] = S.i2;
+    o.view = view;
+    o.ok = true;
+}
+
+// One thread per pixel.  The vertex gradients are summed by the warp over
+// each run of consecutive lanes on the same triangle (a segmented scan by
+// shuffles, as many rounds as the longest run needs) and the last lane of a
+// run issues its three vector reductions: neighbouring pixels of one
+// triangle no longer collide on the same three addresses.  Held to 40
+// registers so that its blocks fit on the SMs beside the lobe-gradient
+// blocks it runs with.
+__global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+                                                 const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
+                                                 const float* __restrict__ clip, float* __restrict__ g_clip,
+                                                 int want_tex, int want_geom) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    PixSample S;
+    S.ok = false;
+    if (p < a.npix) pix_sample(a, td, g_color, diffenv, p, S);
+    if (want_tex && S.ok) {
+        const float wl0 = td.L > 1 ? 1.f - S.fl : 1.f;
+        const float2 f0 = S.f0;
+        tex_add(td, g_pyr, S.l0, S.u0, S.v0, wl0 * (1.f - f0.x) * (1.f - f0.y), S.g);
+        tex_add(td, g_pyr, S.l0, S.u1, S.v0, wl0 * f0.x * (1.f - f0.y), S.g);
+        tex_add(td, g_pyr, S.l0, S.u0, S.v1, wl0 * (1.f - f0.x) * f0.y, S.g);
+        tex_add(td, g_pyr, S.l0, S.u1, S.v1, wl0 * f0.x * f0.y, S.g);
+        if (S.tri) {
+            const float fl = S.fl;
+            const float2 f1 = S.f1;
+            tex_add(td, g_pyr, S.l1, S.s0, S.t0, fl * (1.f - f1.x) * (1.f - f1.y), S.g);
+            tex_add(td, g_pyr, S.l1, S.s1, S.t0, fl * f1.x * (1.f - f1.y), S.g);
+            tex_add(td, g_pyr, S.l1, S.s0, S.t1, fl * (1.f - f1.x) * f1.y, S.g);
+            tex_add(td, g_pyr, S.l1, S.s1, S.t1, fl * f1.x * f1.y, S.g);
+        }
+    }
+    if (!want_geom) return;
+    const long long hw = (long long)a.W * a.H;
+    const int view = (int)(p / hw), rem = (int)(p - view * hw);
+    const int py = rem / a.W, px = rem - py * a.W;
+    VtxGrad o;
+    o.ok = false;
+    if (S.ok) pix_geom(a, td, clip, S, px, py, view, o);
+    if (!o.ok) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o.v[k] = 0.f;
+    }
+    // runs: consecutive lanes on the same triangle of the same view; lanes
+    // without a vertex gradient form runs of their own
+    const int key = o.ok ? S.idx : -1 - lane, vw = o.ok ? view : -1;
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1), prev_vw = __shfl_up_sync(0xffffffffu, vw, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key || prev_vw != vw);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));   // this lane's run head
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    const int len = __reduce_max_sync(0xffffffffu, (unsigned)(lane - start + 1));
+    for (int d = 1; d < len; d <<= 1) {
+        const bool take = lane - d >= start;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float y = __shfl_up_sync(0xffffffffu, o.v[k], d);
+            if (take) o.v[k] += y;
+        }
+    }
+    if (!(tail && o.ok)) return;
     float* gcv = g_clip + (size_t)view * a.nv * 4;
-    red_add4(gcv + (size_t)i0 * 4, gx0, gy0, 0.f, -gx0 * pxn - gy0 * pyn);
-    red_add4(gcv + (size_t)i1 * 4, gx1, gy1, 0.f, -gx1 * pxn - gy1 * pyn);
-    red_add4(gcv + (size_t)i2 * 4, gx2, gy2, 0.f, -gx2 * pxn - gy2 * pyn);
+    red_add4(gcv + (size_t)o.i[0] * 4, o.v[0], o.v[1], 0.f, o.v[2]);
+    red_add4(gcv + (size_t)o.i[1] * 4, o.v[3], o.v[4], 0.f, o.v[5]);
+    red_add4(gcv + (size_t)o.i[2] * 4, o.v[6], o.v[7], 0.f, o.v[8]);
 }
 
 // Lobe gradients (material.cu:428-433), lobe-parallel: a warp stages 32

@@ -46,17 +46,26 @@ DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, fl
     }
 }
 
-// texturemap.cu:49-65
-DEV void index_fetch(const TexDesc& t, int level, float2 uv, int idx[4], float2& f) {
+// texturemap.cu:49-65: the 2x2 texel cell of `uv` at `level` as texel
+// coordinates (columns u0, u1, rows v0, v1; u1 is u0 or u0 + 1, likewise v1)
+// and the bilinear fractions.
+DEV void cell_fetch(const TexDesc& t, int level, float2 uv, int& u0, int& u1, int& v0, int& v1, float2& f) {
     int sx = t.tw >> level, sy = t.th >> level;
     float tx = uv.x * (float)sx, ty = uv.y * (float)sy;
-    int u0 = tx < 0 ? 0 : tx > (float)(sx - 1) ? sx - 1 : (int)tx;
-    int u1 = tx < 1 ? 0 : tx > (float)(sx - 2) ? sx - 1 : (int)tx + 1;
-    int v0 = ty < 0 ? 0 : ty > (float)(sy - 1) ? sy - 1 : (int)ty;
-    int v1 = ty < 1 ? 0 : ty > (float)(sy - 2) ? sy - 1 : (int)ty + 1;
-    idx[0] = v0 * sx + u0; idx[1] = v0 * sx + u1; idx[2] = v1 * sx + u0; idx[3] = v1 * sx + u1;
+    u0 = tx < 0 ? 0 : tx > (float)(sx - 1) ? sx - 1 : (int)tx;
+    u1 = tx < 1 ? 0 : tx > (float)(sx - 2) ? sx - 1 : (int)tx + 1;
+    v0 = ty < 0 ? 0 : ty > (float)(sy - 1) ? sy - 1 : (int)ty;
+    v1 = ty < 1 ? 0 : ty > (float)(sy - 2) ? sy - 1 : (int)ty + 1;
     f.x = tx < 0 ? 0.f : (float)sx < tx ? 1.f : tx - floorf(tx);
     f.y = ty < 0 ? 0.f : (float)sy < ty ? 1.f : ty - floorf(ty);
+}
+
+// The same cell as texel indices within the level.
+DEV void index_fetch(const TexDesc& t, int level, float2 uv, int idx[4], float2& f) {
+    int u0, u1, v0, v1;
+    cell_fetch(t, level, uv, u0, u1, v0, v1, f);
+    const int sx = t.tw >> level;
+    idx[0] = v0 * sx + u0; idx[1] = v0 * sx + u1; idx[2] = v1 * sx + u0; idx[3] = v1 * sx + u1;
 }
 
 DEV float4 ld4(const float* p, int i) { return reinterpret_cast<const float4*>(p)[i]; }
