@@ -909,7 +909,9 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));
     }
     if (d.learn_tex || d.learn_pos) TRY(stage_bwd_pix(f, a, td, s));
-    if (lobes) TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join"));
+    // the position gradient, the texture Adam and the mip rebuild do not
+    // depend on the lobe gradients (which read the shading records, not the
+    // texture): they run while the lobe branch finishes
     if (d.learn_pos) TRY(vcl_project_bwd(ctx, f->mvp, V, f->g_clip, d.nv, 4, f->g_pos, s));
     AdamArgs aa{d.beta1, d.beta2, d.lr_tex, d.eps, F->d_corr, 0.0};
     AdamArgs ap{d.beta1, d.beta2, d.lr_pos, d.eps, F->d_corr, d.lr_lobes};
@@ -933,6 +935,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
         }
         TRY(vcl_launch_check(ctx, "fused mips"));
     }
+    if (lobes) TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join"));
     long long np = d.learn_pos ? (long long)d.nv * 3 : 0;
     long long nl = lobes ? (long long)d.K * 8 : 0;
     if (np + nl > 0) {
