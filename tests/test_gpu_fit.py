@@ -75,6 +75,34 @@ def test_fit_steps_match_oracle(ctx, mode, strategy, K):
         assert_adam_close(got, want, S.lr, steps, name)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fused_odd_sizes_match_oracle(ctx, mode):
+    """Image sizes that are not multiples of the kernels' tiles and warps
+    (130 x 97: partial antialias tiles, warps spanning two pixel rows in the
+    per-pixel backward's run aggregation, partial record chunks), three
+    views and 16 lobes (two lobe groups per warp)."""
+    from vcl_b200 import capi
+    S = scenes.small(seed=5, W=130, H=97, views=3, subdiv=3, tex=128, K=16)
+    tgt = _target(S)
+    steps = 2
+    ref = chain.oracle_fit(S, mode, steps, tgt)
+    ctx.set_mode(mode)
+    fit = capi.Fit(ctx, S, strategy=capi.FIT_FUSED)
+    fit.set_target(tgt)
+    stream = torch.cuda.Stream()
+    losses = []
+    for _ in range(steps):
+        fit.step(stream.cuda_stream)
+        losses.append(fit.read_loss(stream.cuda_stream))
+    pos, tex, (ax, sh, am) = fit.read_params(stream.cuda_stream)
+    fit.close()
+    ctx.set_mode(0)
+    assert np.allclose(losses, ref["losses"], rtol=1e-5), (losses, ref["losses"])
+    for name, got, want in (("tex", tex, ref["tex"]), ("pos", pos, ref["pos"]), ("axis", ax, ref["axis"]),
+                            ("sharp", sh, ref["sharp"]), ("amp", am, ref["amp"])):
+        assert_adam_close(got, want, S.lr, steps, name)
+
+
 def test_fused_equals_plain(ctx):
     """One step from the same state agrees to rounding; over ten steps the
     two trajectories stay together (losses within 1e-3, parameters within
