@@ -404,24 +404,27 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
 
 // Lobe gradients (material.cu:428-433), lobe-parallel: a warp stages 32
 // shading records as 16 pixel pairs, then each lane walks the pairs for its
-// lobe(s) on paired FP32 instructions; sums stay in registers until the end.
-// The next chunk's records and dL/dout are loaded while the current one is
-// consumed (its pixel indices one chunk earlier still).  C = 4.
-template <int NL, bool EXACT>
-__global__ void __launch_bounds__(128, NL == 1 ? 4 : 1) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color, int Kp,
-                                                  float* __restrict__ g_axis, float* __restrict__ g_sharp,
-                                                  float* __restrict__ g_amp) {
-    extern __shared__ float sm[];
+// lobe on paired FP32 instructions; sums stay in registers until the end.
+// Block row blockIdx.y takes lobes [32 y, 32 y + 32) (fewer than 32 lobes:
+// the warp splits into 32 / Kp groups of Kp lanes that walk alternate
+// pairs).  The next chunk's records and dL/dout are loaded while the current
+// one is consumed (its pixel indices one chunk earlier still).  At most 112
+// registers: three blocks of this kernel and two of the per-pixel backward
+// fit on an SM together.  C = 4.
+template <bool EXACT>
+__global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
+                                                     float* __restrict__ g_axis, float* __restrict__ g_sharp,
+                                                     float* __restrict__ g_amp) {
+    __shared__ float s_acc[32 * 8];                                  // [lobe][axis xyz, sharpness, amplitude 4]
+    __shared__ SPair s_pix[4 * 16];
     const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int K = a.K;
-    float* s_acc = sm;                                               // [K][8]
-    SPair* s_pix = reinterpret_cast<SPair*>(sm + ((size_t)K * 8 + 3) / 4 * 4);
-    for (int i = threadIdx.x; i < K * 8; i += blockDim.x) s_acc[i] = 0.f;
+    const int base = 32 * blockIdx.y, Kg = min(32, a.K - base);
+    for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x) s_acc[i] = 0.f;
     __syncthreads();
+    const int Kp = sg_lobe_group_dev(Kg);
     const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
-    Lobe4x2 LL[NL];
-#pragma unroll
-    for (int sl = 0; sl < NL; ++sl) lobe4x2_load(LL[sl], li + sl * Kp, K, a.axis, a.sharp, a.amp);
+    Lobe4x2 L;
+    lobe4x2_load(L, li, Kg, a.axis + 3 * base, a.sharp + base, a.amp + 4 * base);
     SPair* st = s_pix + wid * 16;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n = *rec.count;
@@ -448,21 +451,16 @@ __global__ void __launch_bounds__(128, NL == 1 ? 4 : 1) k_sg_lobes(ShadeIn a, Sh
         }
         __syncwarp();
         const int npair = (m + 1) >> 1;
-        for (int j = g; j < npair; j += G) {
-            const SPair P = st[j];
-#pragma unroll
-            for (int sl = 0; sl < NL; ++sl)
-                if (LL[sl].valid) lobe4x2_accumulate<EXACT>(LL[sl], P);
-        }
+        if (L.valid)
+            for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j]);
         __syncwarp();
     }
-#pragma unroll
-    for (int sl = 0; sl < NL; ++sl) lobe4x2_flush(LL[sl], li + sl * Kp, Kp, s_acc);
+    lobe4x2_flush(L, li, Kp, s_acc);
     __syncthreads();
-    for (int j = threadIdx.x; j < K * 8; j += blockDim.x) {
+    for (int j = threadIdx.x; j < Kg * 8; j += blockDim.x) {
         const float v = s_acc[j];
         if (v == 0.f) continue;
-        const int i = j >> 3, q = j & 7;
+        const int i = base + (j >> 3), q = j & 7;
         if (q < 3) atomicAdd(&g_axis[3 * i + q], v);
         else if (q == 3) atomicAdd(&g_sharp[i], v);
         else atomicAdd(&g_amp[4 * i + (q - 4)], v);
@@ -592,9 +590,6 @@ __global__ void k_adam_small(float* __restrict__ p0, float* __restrict__ g0, flo
 #define TRY(x) do { vcl_status _s = (x); if (_s) return _s; } while (0)
 
 size_t shade_smem(int K) { return sg_lobes4_smem(K); }
-size_t lobes_smem(int K, int threads) {
-    return sizeof(float) * (((size_t)K * 8 + 3) / 4 * 4) + (size_t)(threads / 32) * 16 * sizeof(SPair);
-}
 
 vcl_status autotune_raster(vcl_fit* f);
 
@@ -848,28 +843,18 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
     const long long N = a.npix;
-    const int compat = ctx->mode == VCL_MODE_COMPAT;
-    const int Kp = sg_lobe_group(d.K);
-    const int NL = (d.K + 31) / 32;
-    const int lthreads = 128;
+    const int groups = (d.K + 31) / 32;
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
-    // three lobe blocks per SM leave registers for two blocks of the per-pixel
-    // backward that runs beside this kernel (the two overlap on each SM)
-    long long capg = (long long)ctx->sm_count * (NL == 1 ? 3 : 2);
-    int lgrid = (int)(want < capg ? (want < 1 ? 1 : want) : capg);
-    size_t lsm = lobes_smem(d.K, lthreads);
+    // three lobe blocks per SM (over all lobe groups) leave registers for two
+    // blocks of the per-pixel backward that runs beside this kernel (the two
+    // overlap on each SM)
+    long long capg = ((long long)ctx->sm_count * 3 + groups - 1) / groups;
+    const dim3 grid((unsigned)(want < capg ? (want < 1 ? 1 : want) : capg), (unsigned)groups);
     const float4* gc = (const float4*)f->g_color;
     const ShadeRec rec = shade_rec(f, true);
-    if (compat) {
-        if (NL <= 1) k_sg_lobes<1, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else if (NL <= 2) k_sg_lobes<2, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else k_sg_lobes<4, false><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-    } else {
-        if (NL <= 1) k_sg_lobes<1, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else if (NL <= 2) k_sg_lobes<2, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-        else k_sg_lobes<4, true><<<lgrid, lthreads, lsm, s>>>(a, rec, gc, Kp, f->g_axis, f->g_sharp, f->g_amp);
-    }
+    if (ctx->mode == VCL_MODE_COMPAT) k_sg_lobes<false><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp);
+    else k_sg_lobes<true><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp);
     return vcl_launch_check(ctx, "fused lobe gradients");
 }
 

@@ -550,6 +550,13 @@ inline int sg_lobe_group(int K) {
     while (kp < K && kp < 32) kp <<= 1;
     return kp;
 }
+// The same on the device: lanes per lobe group for K lobes (a power of two,
+// at most 32).
+DEV int sg_lobe_group_dev(int K) {
+    int kp = 1;
+    while (kp < K && kp < 32) kp <<= 1;
+    return kp;
+}
 
 // ---------------------------------------------------------------------------
 // C = 4 fast paths (the fit configurations' RGBA lighting).
