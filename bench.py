@@ -36,7 +36,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vcl", choices=["vcl", "reference"])
-    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--views", type=int, default=None, help="views per iteration (default: 16, config5: 4)")
     ap.add_argument("--config", default="config2", choices=["config1", "config2", "config5", "mix", "serve"])
     ap.add_argument("--scenes", type=int, default=64, help="mix: scenes per batched launch")
     ap.add_argument("--jobs", type=int, default=32, help="serve: fit jobs submitted")
@@ -56,8 +56,8 @@ def make_scene(args):
     if args.config == "config1":
         return scenes.config1()
     if args.config == "config5":
-        return scenes.config5()
-    return scenes.config2(views=args.views)
+        return scenes.config5(views=args.views or 4)
+    return scenes.config2(views=args.views or 16)
 
 
 def workload_name(S):

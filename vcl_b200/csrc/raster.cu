@@ -146,7 +146,7 @@ DEV void span_setup(const RTri& r, SpanEq& q) {
     for (int i = 0; i < 3; ++i) {
         const float a = sg * ea[i];
         const float m = 1e-5f * (fabsf(ea[i]) + fabsf(eb[i]) + fabsf(ek[i]));
-        const float ia = a != 0.f ? 1.f / a : 0.f;
+        const float ia = a != 0.f ? __frcp_rn(a) : 0.f;
         q.al[i] = -(sg * eb[i]) * ia;
         q.be[i] = (-(sg * ek[i]) - m) * ia;
         q.side[i] = a > 0.f ? 1 : a < 0.f ? -1 : 0;
@@ -195,11 +195,18 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
     bool o2 = y0 > w0 && y1 > w1 && y2 > w2, o3 = y0 < -w0 && y1 < -w1 && y2 < -w2;
     bool o4 = c0.z > w0 && c1.z > w1 && c2.z > w2, o5 = c0.z < -w0 && c1.z < -w1 && c2.z < -w2;
     if (o0 || o1 || o2 || o3 || o4 || o5) valid = false;
-    // conservative pixel box (the CPU restatement's raster_bbox)
+    // conservative pixel box: the pixel centres within half a pixel of the
+    // projected vertices' extent.  A centre the exact test accepts lies
+    // inside the projected triangle up to the rounding of the edge functions
+    // (~1e-4 px), and the extent below is off by a few ulps of x/w, so the
+    // half-pixel margin keeps every accepted pixel in the box (the CPU
+    // restatement's raster_bbox keeps one pixel each way; both boxes hold the
+    // same accepted pixels).
     int bx0 = 0, bx1 = W - 1, by0 = 0, by1 = H - 1;
     if (w0 > 0.f && w1 > 0.f && w2 > 0.f) {
-        float X0 = dvd(x0, w0), X1 = dvd(x1, w1), X2 = dvd(x2, w2);
-        float Y0 = dvd(y0, w0), Y1 = dvd(y1, w1), Y2 = dvd(y2, w2);
+        const float iw0 = __frcp_rn(w0), iw1 = __frcp_rn(w1), iw2 = __frcp_rn(w2);
+        float X0 = x0 * iw0, X1 = x1 * iw1, X2 = x2 * iw2;
+        float Y0 = y0 * iw0, Y1 = y1 * iw1, Y2 = y2 * iw2;
         float xmn = fminf(fminf(X0, X1), X2), xmx = fmaxf(fmaxf(X0, X1), X2);
         float ymn = fminf(fminf(Y0, Y1), Y2), ymx = fmaxf(fmaxf(Y0, Y1), Y2);
         float hw = mul(0.5f, (float)W), hh = mul(0.5f, (float)H);
@@ -208,8 +215,8 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
         fx0 = fmaxf(fminf(fx0, (float)W), -2.f); fx1 = fmaxf(fminf(fx1, (float)W), -2.f);
         fy0 = fmaxf(fminf(fy0, (float)H), -2.f); fy1 = fmaxf(fminf(fy1, (float)H), -2.f);
         if (fx0 == fx0 && fx1 == fx1 && fy0 == fy0 && fy1 == fy1) {
-            bx0 = max((int)floorf(fx0) - 1, 0); bx1 = min((int)ceilf(fx1) + 1, W - 1);
-            by0 = max((int)floorf(fy0) - 1, 0); by1 = min((int)ceilf(fy1) + 1, H - 1);
+            bx0 = max((int)ceilf(fx0 - 0.5f), 0); bx1 = min((int)floorf(fx1 + 0.5f), W - 1);
+            by0 = max((int)ceilf(fy0 - 0.5f), 0); by1 = min((int)floorf(fy1 + 0.5f), H - 1);
         }
     }
     if (!valid) { bx0 = 1; bx1 = 0; }

@@ -343,10 +343,10 @@ def config3(seed=0, n=64):
     return [config3_scene(seed, i) for i in range(n)]
 
 
-def config5(seed=0):
+def config5(seed=0, views=4):
     """Dense stress: icosphere s8 (1.31M tris) displaced N(0,0.005), 4 views at
     2048^2, 4096^2 texture (13 levels), 64 lobes."""
-    return make_scene("ico8-2048x4-tex4096-K64", mesh=("ico", 8), W=2048, H=2048, views=4, tex=4096,
+    return make_scene(f"ico8-2048x{views}-tex4096-K64", mesh=("ico", 8), W=2048, H=2048, views=views, tex=4096,
                       K=64, dist=(2.5, 4.0), disp=0.005, seed=seed, iters=100, lr_pos=LR_POS)
 
 
