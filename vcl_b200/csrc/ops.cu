@@ -324,10 +324,10 @@ struct AATri { float2 v[3]; float2 ndc[3]; float iw[3]; uint32_t id[3]; };
 // k_aa_screen -- [2v] = ((x/w + 1) s.x, (y/w + 1) s.y, 1/w, -), [2v+1] =
 // (x/w, y/w, -, -) -- with the same rounded operations as computed here.
 DEV bool aa_fetch(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv,
-                  const uint32_t* __restrict__ tri, int nt, const float4* __restrict__ rast, long long pidx, float2 s,
+                  const uint32_t* __restrict__ tri, int nt, float id_w, float2 s,
                   float2 f, AATri& t, int* flags, bool need_ndc) {
     uint32_t i[3];
-    if (!tri_ok(rast_id(rast[pidx].w), nt, tri, nv, i[0], i[1], i[2], flags)) return false;
+    if (!tri_ok(rast_id(id_w), nt, tri, nv, i[0], i[1], i[2], flags)) return false;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         t.id[k] = i[k];
@@ -403,7 +403,7 @@ DEV bool aa_pair(const float4* __restrict__ proj, const float4* __restrict__ scr
     else { f = make_float2((float)qx + .5f, (float)qy + (pp > op ? .5f : -.5f)); P.o = make_float2(0.f, pp > op ? -1.f : 1.f); }
     P.pp = pp;
     P.op = op;
-    return aa_fetch(proj, scr, nv, tri, nt, rast, pp, s, f, P.t, flags, need_ndc);
+    return aa_fetch(proj, scr, nv, tri, nt, pp == q ? tr.w : to.w, s, f, P.t, flags, need_ndc);
 }
 
 // Forward antialias as a gather: each pixel evaluates the (up to four)
