@@ -76,6 +76,29 @@ def test_operators_match_oracle(ctx, si, mode):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("si", [0, 1, 2])
+def test_sg_bwd_diffuse_and_lobes_only(ctx, si, mode):
+    """SphericalGaussian::backward asked only for the diffuse and lobe
+    gradients (the fit's call; C = 4) takes the split pixel-parallel /
+    lobe-parallel kernels: it must give the oracle's values like the full
+    call does."""
+    G = _gpu_chain()
+    S = SCENES[si]
+    assert S.C == 4
+    o = chain.run_chain(O.orc(), S, mode, pyr=chain.build_pyramid(S, S.tex_target))
+    ctx.set_mode(mode)
+    N, C, K = S.W * S.H * S.views, S.C, S.K
+    d = lambda k: G.dev(o[k])
+    g_diffuse, g_axis, g_sharp, g_amp = G.zeros(N, C), G.zeros(K, 3), G.zeros(K), G.zeros(K, C)
+    ctx.sg_bwd(d("rast"), S.W, S.H, S.views, C, K, G.dev(S.lobe_axis_init), G.dev(S.lobe_sharp_init),
+               G.dev(S.lobe_amp_init), d("normal"), d("diffuse"), d("spec_axis"), d("spec_sharp"), d("spec_amp"),
+               d("g_color"), g_diffuse, g_axis, g_sharp, g_amp, None, None, None, None)
+    ctx.set_mode(0)
+    for k, v in (("g_diffuse", g_diffuse), ("g_axis", g_axis), ("g_sharp", g_sharp), ("g_amp", g_amp)):
+        assert rel_err(G.host(v), o[k]) <= REL_TOL, (k, rel_err(G.host(v), o[k]))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
 def test_chained_pipeline_matches_oracle(ctx, mode):
     S = SCENES[2]
     pyr = chain.build_pyramid(S, S.tex_target)

@@ -291,6 +291,90 @@ __global__ void __launch_bounds__(128) k_sg_bwd_lp(int C, int K, int Kp, int nac
     sg_flush_block(s_acc, K, C, nacc, gaxis, gsharp, gamp, exact ? nullptr : gssh);
 }
 
+// SphericalGaussian::backward for C = 4 when only the diffuse and lobe
+// gradients are asked for (material.cu:369-438 without the specular-lobe
+// outputs).  The diffuse gradient is grad_out * sum_k dg_k amp_k, i.e.
+// grad_out times the forward's diffuse environment sum (sg_env4, two lobes
+// per paired instruction, with its guarded fallback); a term that is not
+// finite is dropped as the reference's guarded add drops it.
+__global__ void __launch_bounds__(256) k_sg_bwd_diffuse4(int K, const float* __restrict__ axis,
+                                                         const float* __restrict__ sharp, const float* __restrict__ amp,
+                                                         const float4* __restrict__ rast, long long npix,
+                                                         const float* __restrict__ normal, const float* __restrict__ sax,
+                                                         const float* __restrict__ ssh, const float* __restrict__ sam,
+                                                         const float4* __restrict__ gout, float4* __restrict__ gdiff) {
+    extern __shared__ float4 sm4[];
+    sg_stage_lobes4(sm4, K, axis, sharp, amp);
+    __syncthreads();
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix || rast_id(rast[p].w) < 0) return;
+    float4 de, se;
+    sg_env4(sm4, K, ld3(normal, p), ld3(sax, p), ssh[p], sam[p], de, se);
+    const float4 g = gout[p];
+    float4 d = gdiff[p];
+    add_nan_check(d.x, g.x * de.x); add_nan_check(d.y, g.y * de.y);
+    add_nan_check(d.z, g.z * de.z); add_nan_check(d.w, g.w * de.w);
+    gdiff[p] = d;
+}
+
+// Lobe gradients of SphericalGaussian::backward for C = 4 from the operator's
+// per-pixel inputs: the fused step's lobe-gradient kernel (lobe per lane, two
+// pixels per paired instruction, 32 lobes per block row) with each warp
+// compacting the covered pixels of its 32-pixel chunk itself.
+template <bool EXACT>
+__global__ void __launch_bounds__(128, 4) k_sg_lobes_op(int K, const float* __restrict__ axis,
+                                                        const float* __restrict__ sharp, const float* __restrict__ amp,
+                                                        const float4* __restrict__ rast, long long npix,
+                                                        const float* __restrict__ normal,
+                                                        const float4* __restrict__ diffuse,
+                                                        const float* __restrict__ sax, const float* __restrict__ ssh,
+                                                        const float* __restrict__ sam, const float4* __restrict__ gout,
+                                                        float* __restrict__ g_axis, float* __restrict__ g_sharp,
+                                                        float* __restrict__ g_amp) {
+    __shared__ float s_acc[32 * 8];
+    __shared__ SPair s_pix[4 * 16];
+    const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int base = 32 * blockIdx.y, Kg = min(32, K - base);
+    for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x) s_acc[i] = 0.f;
+    __syncthreads();
+    const int Kp = sg_lobe_group_dev(Kg);
+    const int G = 32 / Kp, g = lane / Kp, li = lane % Kp;
+    Lobe4x2 L;
+    lobe4x2_load(L, li, Kg, axis + 3 * base, sharp + base, amp + 4 * base);
+    SPair* st = s_pix + wid * 16;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const long long nchunks = (npix + 31) / 32;
+    for (long long c = (long long)blockIdx.x * nwarps + wid; c < nchunks; c += (long long)gridDim.x * nwarps) {
+        const long long p = c * 32 + lane;
+        const bool live = p < npix && rast_id(rast[p].w) >= 0;
+        const unsigned ball = __ballot_sync(0xffffffffu, live);
+        const int m = __popc(ball);
+        if (m == 0) continue;
+        if (live) {
+            const int k = __popc(ball & ((1u << lane) - 1u));
+            const float3 n = ld3(normal, p), pa = ld3(sax, p);
+            spair_put(st + (k >> 1), k & 1, make_float4(n.x, n.y, n.z, ssh[p]), make_float4(pa.x, pa.y, pa.z, sam[p]),
+                      diffuse[p], gout[p]);
+        }
+        if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
+        __syncwarp();
+        const int npair = (m + 1) >> 1;
+        if (L.valid)
+            for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j]);
+        __syncwarp();
+    }
+    lobe4x2_flush(L, li, Kp, s_acc);
+    __syncthreads();
+    for (int j = threadIdx.x; j < Kg * 8; j += blockDim.x) {
+        const float v = s_acc[j];
+        if (v == 0.f) continue;
+        const int i = base + (j >> 3), q = j & 7;
+        if (q < 3) { if (g_axis) atomicAdd(&g_axis[3 * i + q], v); }
+        else if (q == 3) { if (g_sharp) atomicAdd(&g_sharp[i], v); }
+        else if (g_amp) atomicAdd(&g_amp[4 * i + (q - 4)], v);
+    }
+}
+
 size_t sg_bwd_lp_smem(int K, int C, int nacc, int threads) {
     return sizeof(float) * ((size_t)K * nacc + (size_t)K * (4 + C)) +
            (size_t)(threads / 32) * 32 * (sizeof(SPix) + sizeof(SPixOut));
@@ -391,6 +475,34 @@ VCL_API vcl_status vcl_sg_bwd(vcl_ctx* ctx, const float* rast, int W, int H, int
     VCL_REQUIRE(smem <= 200 * 1024, "too many lobes for the shared-memory reduction (K=%d)", K);
     VCL_REQUIRE(C == 4 || C <= CMAX, "channel count");
     const bool pix_out = grad_diffuse || grad_spec_axis || grad_spec_sharpness || grad_spec_amplitude;
+    const bool spec_out = grad_spec_axis || grad_spec_sharpness || grad_spec_amplitude;
+    const bool lobe_out = grad_axis || grad_sharpness || grad_amplitude;
+    auto al16 = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    if (C == 4 && K > 0 && !spec_out && al16(diffuse) && al16(grad_out) && al16(rast) &&
+        (!grad_diffuse || al16(grad_diffuse))) {
+        // diffuse gradient pixel-parallel, lobe gradients lobe-parallel: no
+        // cross-lane sums per pixel and no per-lobe block sums per chunk
+        cudaStream_t st = (cudaStream_t)stream;
+        if (grad_diffuse) {
+            const size_t dsm = sg_lobes4_smem(K);
+            if (dsm > 48 * 1024) cudaFuncSetAttribute(k_sg_bwd_diffuse4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+            k_sg_bwd_diffuse4<<<vcl_blocks(npix, 256), 256, dsm, st>>>(K, axis, sharpness, amplitude, (const float4*)rast,
+                                                                      npix, normal, spec_axis, spec_sharpness,
+                                                                      spec_amplitude, (const float4*)grad_out,
+                                                                      (float4*)grad_diffuse);
+        }
+        if (lobe_out) {
+            const int groups = (K + 31) / 32;
+            long long want = ((npix + 31) / 32 + 3) / 4;
+            long long cap = ((long long)ctx->sm_count * 4 + groups - 1) / groups;
+            const dim3 grid((unsigned)(want < cap ? (want < 1 ? 1 : want) : cap), (unsigned)groups);
+            auto lk = exact ? k_sg_lobes_op<true> : k_sg_lobes_op<false>;
+            lk<<<grid, 128, 0, st>>>(K, axis, sharpness, amplitude, (const float4*)rast, npix, normal,
+                                     (const float4*)diffuse, spec_axis, spec_sharpness, spec_amplitude,
+                                     (const float4*)grad_out, grad_axis, grad_sharpness, grad_amplitude);
+        }
+        return vcl_launch_check(ctx, "sg_bwd");
+    }
     if (K <= 128 && !pix_out) {
         const int Kp = sg_lobe_group(K > 0 ? K : 1);
         const int NL = (K + 31) / 32;
