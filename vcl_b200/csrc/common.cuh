@@ -72,6 +72,30 @@ DEV float lerpf_(float a, float b, float t) { return a + t * (b - a); }
 DEV void red_add4(float* p, float a, float b, float c, float d) {
     atomicAdd(reinterpret_cast<float4*>(p), make_float4(a, b, c, d));
 }
+// Sums v[0..N) over each run of consecutive lanes of the warp that carry the
+// same (key, view): a segmented scan by shuffles, as many rounds as the
+// longest run needs.  Returns true on the last lane of a run, which then holds
+// the run's sums.  All 32 lanes must call it; lanes with nothing to add pass
+// zeros and a key no other lane uses (e.g. -1 - lane).  Neighbouring pixels of
+// one triangle then issue one scatter instead of one each.
+template <int N>
+DEV bool warp_run_sum(float (&v)[N], int key, int view) {
+    const int lane = threadIdx.x & 31;
+    const int pk = __shfl_up_sync(0xffffffffu, key, 1), pv = __shfl_up_sync(0xffffffffu, view, 1);
+    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || pk != key || pv != view);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    const int len = (int)__reduce_max_sync(0xffffffffu, (unsigned)(lane - start + 1));
+    for (int d = 1; d < len; d <<= 1) {
+        const bool take = lane - d >= start;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const float y = __shfl_up_sync(0xffffffffu, v[k], d);
+            if (take) v[k] += y;
+        }
+    }
+    return tail;
+}
 DEV void red_add2(float* p, float a, float b) {
     atomicAdd(reinterpret_cast<float2*>(p), make_float2(a, b));
 }

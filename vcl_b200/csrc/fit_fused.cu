@@ -381,20 +381,7 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
     }
     // runs: consecutive lanes on the same triangle of the same view; lanes
     // without a vertex gradient form runs of their own
-    const int key = o.ok ? S.idx : -1 - lane, vw = o.ok ? view : -1;
-    const int prev = __shfl_up_sync(0xffffffffu, key, 1), prev_vw = __shfl_up_sync(0xffffffffu, vw, 1);
-    const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key || prev_vw != vw);
-    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));   // this lane's run head
-    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
-    const int len = __reduce_max_sync(0xffffffffu, (unsigned)(lane - start + 1));
-    for (int d = 1; d < len; d <<= 1) {
-        const bool take = lane - d >= start;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float y = __shfl_up_sync(0xffffffffu, o.v[k], d);
-            if (take) o.v[k] += y;
-        }
-    }
+    const bool tail = warp_run_sum(o.v, o.ok ? S.idx : -1 - lane, o.ok ? view : -1);
     if (!(tail && o.ok)) return;
     float* gcv = g_clip + (size_t)view * a.nv * 4;
     red_add4(gcv + (size_t)o.i[0] * 4, o.v[0], o.v[1], 0.f, o.v[2]);

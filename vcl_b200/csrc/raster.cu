@@ -529,48 +529,60 @@ __global__ void k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, 
 }
 
 // rasterize.cu:84-141: dL/d(x, y, w) of the three clip-space vertices from
-// dL/d(u, v); one vector atomic per vertex (z receives +0).
+// dL/d(u, v) (z receives +0).  One thread per pixel; the vertex gradients of
+// neighbouring pixels on the same triangle are summed by the warp, then one
+// vector reduction per vertex and run.
 __global__ void k_raster_bwd(const float* __restrict__ clip, int nv, const uint32_t* __restrict__ tri, int nt, int W,
                              int H, long long npix, const float4* __restrict__ rast, const float2* __restrict__ gb,
                              float* __restrict__ gclip) {
-    long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pidx >= npix) return;
-    float4 r = rast[pidx];
-    int idx = rast_id(r.w);
-    if (idx < 0 || idx >= nt) return;
-    float2 g = gb[pidx];
-    if (((__float_as_uint(g.x) | __float_as_uint(g.y)) << 1) == 0u) return;
-    long long hw = (long long)W * H;
-    int view = (int)(pidx / hw);
-    int rem = (int)(pidx - view * hw);
-    int py = rem / W, px = rem - py * W;
-    const float xs = 2.f / (float)W, ys = 2.f / (float)H;
-    float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
-    float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
-    uint32_t i0 = tri[3 * (size_t)idx], i1 = tri[3 * (size_t)idx + 1], i2 = tri[3 * (size_t)idx + 2];
-    if (i0 >= (uint32_t)nv || i1 >= (uint32_t)nv || i2 >= (uint32_t)nv) return;
-    const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * nv;
-    float4 c0 = cv[i0], c1 = cv[i1], c2 = cv[i2];
-    float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
-    float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
-    float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
-    float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
-    float a = e0x * e1y - e0y * e1x;
-    float ia = 1.f / (a + (a > 0 ? 1e-6f : -1e-6f));
-    float kuv = r.x * g.x + r.y * g.y;
-    float gx0 = (g.y * p2y + kuv * e1y) * ia;
-    float gy0 = (-g.y * p2x - kuv * e1x) * ia;
-    float gw0 = -gx0 * pxn - gy0 * pyn;
-    float gx1 = (-g.x * p2y - kuv * e0y) * ia;
-    float gy1 = (g.x * p2x + kuv * e0x) * ia;
-    float gw1 = -gx1 * pxn - gy1 * pyn;
-    float gx2 = ((-g.y * p0y + g.x * p1y) - kuv * (-p0y + p1y)) * ia;
-    float gy2 = ((g.y * p0x - g.x * p1x) - kuv * (p0x - p1x)) * ia;
-    float gw2 = -gx2 * pxn - gy2 * pyn;
+    const long long pidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    float v[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    uint32_t i0 = 0, i1 = 0, i2 = 0;
+    int idx = -1, view = -1;
+    bool ok = false;
+    if (pidx < npix) {
+        const float4 r = rast[pidx];
+        idx = rast_id(r.w);
+        const float2 g = gb[pidx];
+        if (idx >= 0 && idx < nt && ((__float_as_uint(g.x) | __float_as_uint(g.y)) << 1) != 0u) {
+            i0 = tri[3 * (size_t)idx]; i1 = tri[3 * (size_t)idx + 1]; i2 = tri[3 * (size_t)idx + 2];
+            if (i0 < (uint32_t)nv && i1 < (uint32_t)nv && i2 < (uint32_t)nv) {
+                const long long hw = (long long)W * H;
+                view = (int)(pidx / hw);
+                const int rem = (int)(pidx - view * hw);
+                const int py = rem / W, px = rem - py * W;
+                const float xs = 2.f / (float)W, ys = 2.f / (float)H;
+                const float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
+                const float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
+                const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * nv;
+                const float4 c0 = cv[i0], c1 = cv[i1], c2 = cv[i2];
+                float p0x = c0.w * pxn - c0.x, p0y = c0.w * pyn - c0.y;
+                float p1x = c1.w * pxn - c1.x, p1y = c1.w * pyn - c1.y;
+                float p2x = c2.w * pxn - c2.x, p2y = c2.w * pyn - c2.y;
+                float e0x = p0x - p2x, e0y = p0y - p2y, e1x = p1x - p2x, e1y = p1y - p2y;
+                float a = e0x * e1y - e0y * e1x;
+                float ia = 1.f / (a + (a > 0 ? 1e-6f : -1e-6f));
+                float kuv = r.x * g.x + r.y * g.y;
+                float gx0 = (g.y * p2y + kuv * e1y) * ia;
+                float gy0 = (-g.y * p2x - kuv * e1x) * ia;
+                float gx1 = (-g.x * p2y - kuv * e0y) * ia;
+                float gy1 = (g.x * p2x + kuv * e0x) * ia;
+                float gx2 = ((-g.y * p0y + g.x * p1y) - kuv * (-p0y + p1y)) * ia;
+                float gy2 = ((g.y * p0x - g.x * p1x) - kuv * (p0x - p1x)) * ia;
+                v[0] = gx0; v[1] = gy0; v[2] = -gx0 * pxn - gy0 * pyn;
+                v[3] = gx1; v[4] = gy1; v[5] = -gx1 * pxn - gy1 * pyn;
+                v[6] = gx2; v[7] = gy2; v[8] = -gx2 * pxn - gy2 * pyn;
+                ok = true;
+            }
+        }
+    }
+    const bool tail = warp_run_sum(v, ok ? idx : -1 - lane, ok ? view : -1);
+    if (!(tail && ok)) return;
     float* gv = gclip + (size_t)view * nv * 4;
-    red_add4(gv + (size_t)i0 * 4, gx0, gy0, 0.f, gw0);
-    red_add4(gv + (size_t)i1 * 4, gx1, gy1, 0.f, gw1);
-    red_add4(gv + (size_t)i2 * 4, gx2, gy2, 0.f, gw2);
+    red_add4(gv + (size_t)i0 * 4, v[0], v[1], 0.f, v[2]);
+    red_add4(gv + (size_t)i1 * 4, v[3], v[4], 0.f, v[5]);
+    red_add4(gv + (size_t)i2 * 4, v[6], v[7], 0.f, v[8]);
 }
 
 struct RasterWS {
