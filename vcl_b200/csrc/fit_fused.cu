@@ -605,6 +605,7 @@ vcl_status fused_init(vcl_fit* f) {
         if (F->d_step) cudaFreeAsync(F->d_step, as);
         if (F->d_corr) cudaFreeAsync(F->d_corr, as);
         if (F->flags) cudaFreeAsync(F->flags, as);
+        if (F->scr) cudaFreeAsync(F->scr, as);
         delete F;
         return vcl_fail(ctx, VCL_ERR_NOMEM, "fused fit state: %s", cudaGetErrorString(e));
     }
@@ -1112,7 +1113,7 @@ vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* m
 }
 
 size_t fit_fused_footprint(const vcl_fit_desc& d) {
-    size_t ws = 0;
+    size_t ws = sizeof(float) * 8 * (size_t)d.views * d.nv;   // antialias screen terms
     for (int t : {8, 16, 32}) {
         long long cap = raster_auto_capacity(d.views, d.nt, d.W, d.H, t);
         size_t b = raster_ws_size(d.W, d.H, d.views, d.nt, t, cap);
