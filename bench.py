@@ -164,13 +164,13 @@ def fused_bytes(S, ncov):
 # views of 1024x1024 of this workload, divided by the pixels); their traffic
 # grows with the pixel count.
 DRAM_BYTES_PER_PIXEL = {
-    "bwd_pix": (290.7e6 + 46.6e6) / (4 * 1024 * 1024),
-    "sg_lobes": (179.5e6 + 5.0e6) / (4 * 1024 * 1024),
+    "bwd_pix": (319.0e6 + 64.1e6) / (4 * 1024 * 1024),
+    "sg_lobes": (182.5e6 + 4.1e6) / (4 * 1024 * 1024),
 }
 # What bounds each of them instead of HBM bandwidth (same capture).
 BOUND_NOTE = {
-    "bwd_pix": "k_bwd_pix is bound by the scatter of texel and vertex gradients through L2 (vector reductions; "
-               "L2 ~51% busy, warps waiting on loads and the LSU queue), not by HBM bandwidth",
+    "bwd_pix": "k_bwd_pix is bound by the scatter of texel gradients through L2 (vector reductions; "
+               "L2 ~50% busy, warps waiting on loads and the LSU queue), not by HBM bandwidth",
     "sg_lobes": "k_sg_lobes is FP32/MUFU-bound (per pixel and lobe: 2 rsqrt, 4 ex2, ~35 paired FP32 ops), "
                 "not HBM-bound",
 }
