@@ -67,7 +67,11 @@ def workload_name(S):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples during the timed region (clock, throttle reasons)."""
+    """nvidia-smi samples during the timed region (clock, throttle reasons).
+    Started before the warm-up (so that nvidia-smi is running when timing
+    begins), sampling every 20 ms; window(t0, t1) keeps the samples whose host
+    arrival time falls inside the timed region (the first later sample when a
+    short region caught none)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -76,11 +80,15 @@ class ClockSampler:
         self.device = device
         self.rows = []
         self.proc = None
+        self.win = None
+
+    def window(self, t0, t1):
+        self.win = (t0, t1)
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -89,7 +97,7 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
 
     def stop(self):
         if not self.proc:
@@ -100,6 +108,13 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.t.join(timeout=2)
+        rows = [r for _, r in self.rows]
+        if self.win is not None:
+            t0, t1 = self.win
+            inside = [r for t, r in self.rows if t0 <= t <= t1]
+            later = [r for t, r in self.rows if t > t1][:1]
+            rows = inside or later
+        self.rows = rows
         sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -208,17 +223,20 @@ def run_vcl(args, rank, world):
         f.set_target(target, sh, is_device=True)
         return f
 
-    def timed(fit, steps, warmup):
+    def timed(fit, steps, warmup, sampler=None):
         for _ in range(warmup):
             fit.step(sh)
         stream.synchronize()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
         e0.record(stream)
         for _ in range(steps):
             fit.step(sh)
         e1.record(stream)
         stream.synchronize()
+        if sampler is not None:
+            sampler.window(t0, time.perf_counter())
         barrier()
         return e0.elapsed_time(e1)
 
@@ -241,7 +259,7 @@ def run_vcl(args, rank, world):
         fit = make_fit(strat)
         if name == strategies[-1][0]:
             clocks.start()
-        ms = maxr(timed(fit, args.steps, args.warmup))
+        ms = maxr(timed(fit, args.steps, args.warmup, clocks if name == strategies[-1][0] else None))
         if name == strategies[-1][0]:
             clk = clocks.stop()
         results[name] = ms
