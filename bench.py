@@ -291,6 +291,8 @@ def run_vcl(args, rank, world):
     copy_stream = torch.cuda.Stream()
     cs = copy_stream.cuda_stream
 
+    host_losses = torch.zeros(max(args.steps, args.warmup, 1), dtype=torch.float32).pin_memory()
+
     def e2e_run(n, e0=None, e1=None):
         if e0 is not None:
             e0.record(copy_stream)
@@ -300,7 +302,9 @@ def run_vcl(args, rank, world):
             fit.step(sh)
             if i + 1 < n:
                 fit.stage_target(host_target, cs)
-            fit.read_loss(sh)   # device->host read of the step's loss (synchronizes)
+            # device->host read of every step's loss into pinned memory, queued
+            # behind the step (the host runs ahead; all reads land before e1)
+            fit.read_loss_async(host_losses.data_ptr() + 4 * i, sh)
         if e1 is not None:
             e1.record(stream)
 
@@ -313,6 +317,9 @@ def run_vcl(args, rank, world):
     copy_stream.synchronize()
     barrier()
     e2e_ms = maxr(e0.elapsed_time(e1)) / args.steps
+    e2e_losses = host_losses[:args.steps].numpy().copy()
+    if not np.all(np.isfinite(e2e_losses)) or not np.all(e2e_losses > 0):
+        raise RuntimeError(f"end-to-end loop read back invalid losses: {e2e_losses[:4]} ...")
     fit.close()
 
     out.update(results=results, launches=launches, losses=losses, value=value, ms_per_step=ms_per_step,

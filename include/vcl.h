@@ -329,6 +329,12 @@ VCL_API vcl_status vcl_fit_render(vcl_fit* fit, float* out, void* stream);
 VCL_API const float* vcl_fit_loss_device(const vcl_fit* fit);
 /* Copies the last step's loss to *loss_host; synchronizes `stream`. */
 VCL_API vcl_status vcl_fit_read_loss(vcl_fit* fit, float* loss_host, void* stream);
+/* The same copy, stream-ordered without waiting: *loss_host (pinned host
+ * memory) holds the loss once `stream` has passed this point, so a caller can
+ * read every step's loss while the next steps are already queued.  No
+ * reference counterpart (Loss::loss reads back synchronously every
+ * iteration, preset_primitives.cpp:222). */
+VCL_API vcl_status vcl_fit_read_loss_async(vcl_fit* fit, float* loss_host, void* stream);
 /* Copies the current parameters to host memory (any pointer may be NULL);
  * synchronizes `stream`. */
 VCL_API vcl_status vcl_fit_read_params(vcl_fit* fit, float* pos, float* tex_level0, float* lobe_axis,

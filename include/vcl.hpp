@@ -139,6 +139,10 @@ public:
         chk(vcl_fit_read_loss(h_.get(), &l, stream), "vcl_fit_read_loss");
         return l;
     }
+    // Queues the loss copy into pinned host memory without waiting.
+    void read_loss_async(float* pinned_dst, void* stream = nullptr) {
+        chk(vcl_fit_read_loss_async(h_.get(), pinned_dst, stream), "vcl_fit_read_loss_async");
+    }
     void read_params(float* pos, float* tex_level0, float* lobe_axis, float* lobe_sharp, float* lobe_amp,
                      void* stream = nullptr) {
         chk(vcl_fit_read_params(h_.get(), pos, tex_level0, lobe_axis, lobe_sharp, lobe_amp, stream),

@@ -70,6 +70,7 @@ SIGNATURES = {
     "vcl_fit_render": (c_int, [P, P, P]),
     "vcl_fit_loss_device": (c_void_p, [P]),
     "vcl_fit_read_loss": (c_int, [P, P, P]),
+    "vcl_fit_read_loss_async": (c_int, [P, P, P]),
     "vcl_fit_read_params": (c_int, [P, P, P, P, P, P, P]),
     "vcl_fit_footprint": (c_size, [P]),
     "vcl_fit_raster_tuning": (c_int, [P, P, P]),
@@ -311,6 +312,12 @@ class Fit:
         out = ctypes.c_float()
         self._c(self.ctx.lib.vcl_fit_read_loss(self.h, ctypes.byref(out), stream), "vcl_fit_read_loss")
         return out.value
+
+    def read_loss_async(self, host_address, stream=None):
+        """Queue the copy of the last step's loss to `host_address` (pinned
+        host memory, e.g. a pinned torch tensor's data_ptr()) without waiting."""
+        self._c(self.ctx.lib.vcl_fit_read_loss_async(self.h, ctypes.c_void_p(host_address), stream),
+                "vcl_fit_read_loss_async")
 
     def loss_address(self):
         return self.ctx.lib.vcl_fit_loss_device(self.h)

@@ -254,6 +254,14 @@ VCL_API vcl_status vcl_fit_read_loss(vcl_fit* f, float* loss_host, void* stream)
     return vcl_cuda_check(ctx, cudaStreamSynchronize(s), "loss readback sync");
 }
 
+VCL_API vcl_status vcl_fit_read_loss_async(vcl_fit* f, float* loss_host, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    VCL_REQUIRE(loss_host, "null loss output");
+    return vcl_cuda_check(ctx, cudaMemcpyAsync(loss_host, f->loss, sizeof(float), cudaMemcpyDeviceToHost,
+                                               (cudaStream_t)stream), "loss readback");
+}
+
 VCL_API vcl_status vcl_fit_read_params(vcl_fit* f, float* pos, float* tex0, float* axis, float* sharp, float* amp,
                                        void* stream) {
     if (!f) return VCL_ERR_ARG;
