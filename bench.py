@@ -554,6 +554,20 @@ def main():
         line["fused_kernels_ms"] = {k: round(v, 4) for k, v in kms.items()}
         line["fused_kernels_frac_hbm"] = {k: round(byts[k] / (v * 1e-3) / 1e9 / hbm_peak, 3)
                                           for k, v in kms.items() if v > 0}
+        # the SG kernels' own bound, the MUFU pipe: 2 rsqrt + 4 ex2 per covered
+        # pixel and lobe in each, against 16 MUFU operations per clock per SM
+        # at the SM clock sampled in the timed region (a nominal peak: no
+        # measured figure exists for this unit)
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        mhz = (r["clocks"] or {}).get("sm_mhz") or 1965.0
+        sfu_peak = 16.0 * sms * mhz * 1e6
+        ops = 6.0 * ncov * S.K
+        line["sfu_roofline"] = {
+            k: {"mufu_ops": ops, "achieved_gops": ops / (kms[k] * 1e-3) / 1e9, "peak_gops": sfu_peak / 1e9,
+                "frac": ops / (kms[k] * 1e-3) / sfu_peak, "covered_pixels": ncov,
+                "peak_source": f"nominal: 16 MUFU ops/clock/SM x {sms} SMs x {mhz:.0f} MHz"}
+            for k in ("shade_fwd", "sg_lobes") if kms.get(k, 0) > 0}
     if "stages" in r:
         st = r["stages"]
         byts = stage_bytes(S, st["ncov"])
