@@ -339,6 +339,16 @@ VCL_API vcl_status vcl_fit_read_loss_async(vcl_fit* fit, float* loss_host, void*
  * synchronizes `stream`. */
 VCL_API vcl_status vcl_fit_read_params(vcl_fit* fit, float* pos, float* tex_level0, float* lobe_axis,
                                        float* lobe_sharp, float* lobe_amp, void* stream);
+/* Checkpoint / resume of a job (no reference counterpart; the reference
+ * keeps no state across runs): vcl_fit_save_state writes, into host memory
+ * of vcl_fit_state_bytes() bytes, a header (shapes, Adam step) and the
+ * positions, texture pyramid, lobes and the Adam moments of every group;
+ * vcl_fit_load_state restores them into a job of the same shapes, which
+ * then continues as the saved one would.  Both synchronize `stream`; no step
+ * of the job may be in flight elsewhere. */
+VCL_API size_t vcl_fit_state_bytes(const vcl_fit* fit);
+VCL_API vcl_status vcl_fit_save_state(vcl_fit* fit, void* host_dst, size_t bytes, void* stream);
+VCL_API vcl_status vcl_fit_load_state(vcl_fit* fit, const void* host_src, size_t bytes, void* stream);
 /* The raster tile size the fused strategy's autotuner picked for this job
  * (tuned on first use by timing tiles 8, 16 and 32 on the job's geometry)
  * and the measured milliseconds per raster call for each (ms_per_tile[3],

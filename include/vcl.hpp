@@ -149,6 +149,15 @@ public:
             "vcl_fit_read_params");
     }
     int launches_per_step() const { return vcl_fit_launches_per_step(h_.get()); }
+    // Checkpoint / resume: parameters, Adam moments and step as bytes.
+    std::vector<unsigned char> save_state(void* stream = nullptr) {
+        std::vector<unsigned char> buf(vcl_fit_state_bytes(h_.get()));
+        chk(vcl_fit_save_state(h_.get(), buf.data(), buf.size(), stream), "vcl_fit_save_state");
+        return buf;
+    }
+    void load_state(const std::vector<unsigned char>& buf, void* stream = nullptr) {
+        chk(vcl_fit_load_state(h_.get(), buf.data(), buf.size(), stream), "vcl_fit_load_state");
+    }
 
 private:
     void chk(vcl_status st, const char* what) const { ctx_->check(st, what); }

@@ -103,6 +103,48 @@ def test_fused_odd_sizes_match_oracle(ctx, mode):
         assert_adam_close(got, want, S.lr, steps, name)
 
 
+@pytest.mark.parametrize("strategy", [0, 1])
+def test_state_save_load_resumes(ctx, strategy):
+    """A job saved after 3 steps and loaded into a fresh job of the same
+    shapes continues as the original does (losses and parameters of the next
+    2 steps); a state of other shapes, or not a state at all, is refused."""
+    from vcl_b200 import capi
+    S = _scene()
+    tgt = _target(S)
+    st = torch.cuda.Stream()
+    a = capi.Fit(ctx, S, strategy=strategy)
+    a.set_target(tgt)
+    for _ in range(3):
+        a.step(st.cuda_stream)
+    state = a.save_state(st.cuda_stream)
+    la = []
+    for _ in range(2):
+        a.step(st.cuda_stream)
+        la.append(a.read_loss(st.cuda_stream))
+    pa = a.read_params(st.cuda_stream)
+    a.close()
+    b = capi.Fit(ctx, S, strategy=strategy)
+    b.set_target(tgt)
+    b.load_state(state, st.cuda_stream)
+    lb = []
+    for _ in range(2):
+        b.step(st.cuda_stream)
+        lb.append(b.read_loss(st.cuda_stream))
+    pb = b.read_params(st.cuda_stream)
+    b.close()
+    assert np.allclose(la, lb, rtol=1e-5), (la, lb)
+    assert_adam_close(pb[0], pa[0], S.lr, 2, "pos")
+    assert_adam_close(pb[1], pa[1], S.lr, 2, "tex")
+    for x, y in zip(pb[2], pa[2]):
+        assert_adam_close(x, y, S.lr, 2, "lobes")
+    other = capi.Fit(ctx, scenes.small(seed=3, W=32, H=24, views=1, subdiv=1, tex=32, K=4), strategy=strategy)
+    with pytest.raises(capi.VclError, match="another job shape"):
+        other.load_state(state, st.cuda_stream)
+    with pytest.raises(capi.VclError, match="bad magic"):
+        other.load_state(b"x" * len(state), st.cuda_stream)
+    other.close()
+
+
 def test_fused_equals_plain(ctx):
     """One step from the same state agrees to rounding; over ten steps the
     two trajectories stay together (losses within 1e-3, parameters within

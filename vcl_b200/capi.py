@@ -71,6 +71,9 @@ SIGNATURES = {
     "vcl_fit_loss_device": (c_void_p, [P]),
     "vcl_fit_read_loss": (c_int, [P, P, P]),
     "vcl_fit_read_loss_async": (c_int, [P, P, P]),
+    "vcl_fit_state_bytes": (ctypes.c_size_t, [P]),
+    "vcl_fit_save_state": (c_int, [P, P, ctypes.c_size_t, P]),
+    "vcl_fit_load_state": (c_int, [P, P, ctypes.c_size_t, P]),
     "vcl_fit_read_params": (c_int, [P, P, P, P, P, P, P]),
     "vcl_fit_footprint": (c_size, [P]),
     "vcl_fit_raster_tuning": (c_int, [P, P, P]),
@@ -318,6 +321,17 @@ class Fit:
         host memory, e.g. a pinned torch tensor's data_ptr()) without waiting."""
         self._c(self.ctx.lib.vcl_fit_read_loss_async(self.h, ctypes.c_void_p(host_address), stream),
                 "vcl_fit_read_loss_async")
+
+    def save_state(self, stream=None):
+        """The job's resumable state (parameters, Adam moments and step) as bytes."""
+        n = self.ctx.lib.vcl_fit_state_bytes(self.h)
+        buf = ctypes.create_string_buffer(n)
+        self._c(self.ctx.lib.vcl_fit_save_state(self.h, buf, n, stream), "vcl_fit_save_state")
+        return buf.raw
+
+    def load_state(self, state, stream=None):
+        buf = ctypes.create_string_buffer(bytes(state), len(state))
+        self._c(self.ctx.lib.vcl_fit_load_state(self.h, buf, len(state), stream), "vcl_fit_load_state")
 
     def loss_address(self):
         return self.ctx.lib.vcl_fit_loss_device(self.h)

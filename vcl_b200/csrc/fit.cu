@@ -282,6 +282,107 @@ VCL_API vcl_status vcl_fit_read_params(vcl_fit* f, float* pos, float* tex0, floa
     return st;
 }
 
+// ---------------------------------------------------------------- job state
+// A job's resumable state in one host buffer: a header (magic, version, the
+// shapes it belongs to, the Adam step) followed by the parameters (positions,
+// the whole texture pyramid, the lobe block) and the Adam moments of the three
+// groups, each as the device holds it.
+namespace {
+
+struct StateHeader {
+    char magic[8];
+    int32_t version, nv, tex_w, tex_h, C, levels, K, step;
+    int64_t npyr;
+};
+constexpr char kStateMagic[8] = {'V', 'C', 'L', 'F', 'I', 'T', '0', '1'};
+
+struct StatePart {
+    float* dev;
+    size_t bytes;
+};
+
+void state_parts(const vcl_fit* f, StatePart (&p)[6]) {
+    const vcl_fit_desc& d = f->d;
+    const size_t F = sizeof(float);
+    const size_t npyr = vcl_tex_level_offset(d.tex_w, d.tex_h, d.C, d.levels);
+    const size_t n0 = (size_t)d.tex_w * d.tex_h * d.C, nl = (size_t)d.K * (4 + d.C);
+    p[0] = {f->pos, F * d.nv * 3};
+    p[1] = {f->pyr, F * npyr};
+    p[2] = {f->lobe, F * nl};
+    p[3] = {f->mv_tex, F * n0 * 2};
+    p[4] = {f->mv_pos, F * d.nv * 3 * 2};
+    p[5] = {f->mv_lobe, F * nl * 2};
+}
+
+}  // namespace
+
+VCL_API size_t vcl_fit_state_bytes(const vcl_fit* f) {
+    if (!f) return 0;
+    StatePart p[6];
+    state_parts(f, p);
+    size_t n = sizeof(StateHeader);
+    for (const StatePart& q : p) n += q.bytes;
+    return n;
+}
+
+VCL_API vcl_status vcl_fit_save_state(vcl_fit* f, void* host_dst, size_t bytes, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    const size_t need = vcl_fit_state_bytes(f);
+    VCL_REQUIRE(host_dst && bytes >= need, "state buffer of %zu bytes, %zu needed", bytes, need);
+    const vcl_fit_desc& d = f->d;
+    StateHeader h;
+    std::memcpy(h.magic, kStateMagic, 8);
+    h.version = 1; h.nv = d.nv; h.tex_w = d.tex_w; h.tex_h = d.tex_h; h.C = d.C; h.levels = d.levels; h.K = d.K;
+    h.step = f->step_count;
+    h.npyr = (int64_t)vcl_tex_level_offset(d.tex_w, d.tex_h, d.C, d.levels);
+    char* out = (char*)host_dst;
+    std::memcpy(out, &h, sizeof(h));
+    size_t off = sizeof(h);
+    StatePart p[6];
+    state_parts(f, p);
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = VCL_OK;
+    for (const StatePart& q : p) {
+        if (q.bytes && st == VCL_OK)
+            st = vcl_cuda_check(ctx, cudaMemcpyAsync(out + off, q.dev, q.bytes, cudaMemcpyDeviceToHost, s), "state save");
+        off += q.bytes;
+    }
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "state save sync");
+    return st;
+}
+
+VCL_API vcl_status vcl_fit_load_state(vcl_fit* f, const void* host_src, size_t bytes, void* stream) {
+    if (!f) return VCL_ERR_ARG;
+    vcl_ctx* ctx = f->ctx;
+    const size_t need = vcl_fit_state_bytes(f);
+    VCL_REQUIRE(host_src && bytes >= need, "state of %zu bytes, %zu needed", bytes, need);
+    StateHeader h;
+    std::memcpy(&h, host_src, sizeof(h));
+    const vcl_fit_desc& d = f->d;
+    VCL_REQUIRE(std::memcmp(h.magic, kStateMagic, 8) == 0 && h.version == 1,
+                "not a fit job state (bad magic or version)");
+    VCL_REQUIRE(h.nv == d.nv && h.tex_w == d.tex_w && h.tex_h == d.tex_h && h.C == d.C && h.levels == d.levels &&
+                    h.K == d.K && h.step >= 0,
+                "state of another job shape (nv %d, texture %dx%dx%d/%d levels, K %d)", h.nv, h.tex_w, h.tex_h, h.C,
+                h.levels, h.K);
+    const char* in = (const char*)host_src;
+    size_t off = sizeof(h);
+    StatePart p[6];
+    state_parts(f, p);
+    cudaStream_t s = (cudaStream_t)stream;
+    vcl_status st = VCL_OK;
+    for (const StatePart& q : p) {
+        if (q.bytes && st == VCL_OK)
+            st = vcl_cuda_check(ctx, cudaMemcpyAsync(q.dev, in + off, q.bytes, cudaMemcpyHostToDevice, s), "state load");
+        off += q.bytes;
+    }
+    if (st == VCL_OK) st = vcl_cuda_check(ctx, cudaStreamSynchronize(s), "state load sync");
+    if (st) return st;
+    f->step_count = h.step;
+    return fit_fused_sync_counter(f, true);
+}
+
 VCL_API int vcl_fit_launches_per_step(const vcl_fit* f) {
     if (!f) return 0;
     return f->strategy == VCL_FIT_FUSED ? fit_fused_launches(f) : fit_plain_launches(f);
