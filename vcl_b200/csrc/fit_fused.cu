@@ -157,8 +157,9 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
 // Forward shading of every pixel; writes the color and the diffuse
 // environment sum (kept for the backward's diffuse gradient) and, when
 // rec.count is set, the shading record of each covered pixel (one slot
-// claim per block).  C = 4; 256 threads.
-__global__ void __launch_bounds__(256) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
+// claim per block).  C = 4; 256 threads, held to 40 registers for six blocks
+// per SM (more warps to cover the texture and attribute loads).
+__global__ void __launch_bounds__(256, 6) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
                                                    float4* __restrict__ diffenv, ShadeRec rec) {
     extern __shared__ float4 sm4[];
     __shared__ int s_off[8], s_base;
