@@ -496,8 +496,9 @@ __global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, 
     }
 }
 
-// Winning key -> (u, v, z/w, id+1) and DB per pixel.
-__global__ void k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, long long npix,
+// Winning key -> (u, v, z/w, id+1) and DB per pixel; held to 32 registers
+// for eight blocks per SM (the record and vertex gathers need the warps).
+__global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, long long npix,
                           const unsigned long long* __restrict__ keys, const float4* __restrict__ clip, int nv,
                           const uint32_t* __restrict__ tri, float4* __restrict__ rast, float4* __restrict__ db) {
     const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
