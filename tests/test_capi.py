@@ -55,3 +55,21 @@ def test_host_helpers_without_gpu():
     if not torch.cuda.is_available():
         h = ctypes.c_void_p()
         assert L.vcl_create(0, ctypes.byref(h)) != 0
+
+
+def test_fit_footprint_without_gpu():
+    """vcl_fit_footprint is host arithmetic (admission control needs it before
+    any device work): it grows with the views, the triangles and the texture,
+    and covers at least the per-pixel buffers of both strategies."""
+    from vcl_b200 import capi, scenes
+    if not os.path.exists(capi.LIB_PATH):
+        pytest.skip("libvcl.so not built")
+    f4, f16 = capi.footprint(scenes.config2(views=4)), capi.footprint(scenes.config2(views=16))
+    assert f16 > 3 * f4
+    px16 = 16 * 1024 * 1024
+    assert f16 >= 248 * px16          # per-pixel intermediates, gradients, targets and raster keys
+    small = scenes.small(seed=1)
+    dense = scenes.small(seed=1, subdiv=3)
+    assert capi.footprint(dense) > capi.footprint(small)
+    bigtex = scenes.small(seed=1, tex=256)
+    assert capi.footprint(bigtex) > capi.footprint(small) + 256 * 256 * 4 * 4 * 3   # texture, grads, Adam m and v
