@@ -119,14 +119,19 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
  * not allocate device memory or synchronize the device on their per-frame
  * path.  No counterpart in the reference (its rasterizer has no workspace).
  * Same arguments and results as vcl_rasterize_fwd.  Requests whose depth
- * keys (8 B per pixel and view), triangle records (84 B per view and
- * triangle) and tile counters exceed the limit return VCL_ERR_ARG.  No part
- * of the scratch needs to start at zero.  One scratch per device: calls
- * whose work overlaps on the device race, so serialize them.  The first call
- * per device (or vcl_raster_scratch_init) resolves the scratch address with
- * the context's device current; make it during set-up, before any stream
- * capture. */
+ * keys (8 B per pixel and view), triangle records and medium-list entries
+ * (VCL_RASTER_BYTES_PER_VIEW_TRIANGLE = 96 + 4 B per view and triangle) and
+ * tile counters (12 B per tile and view), each rounded up to 256 B, exceed
+ * the limit return VCL_ERR_ARG; what is left holds the tile bin lists (4 B
+ * per entry).  No part of the scratch needs to start at zero.  One scratch
+ * per device: calls whose work overlaps on the device race, so serialize
+ * them.  The first call per device (or vcl_raster_scratch_init) resolves the
+ * scratch address with the context's device current; make it during set-up,
+ * before any stream capture.  cudaDeviceReset unloads the module and with it
+ * the scratch: after a reset, call vcl_raster_scratch_init again (it always
+ * resolves the address anew) before the next static call. */
 #define VCL_RASTER_SCRATCH_BYTES (32u << 20)
+#define VCL_RASTER_BYTES_PER_VIEW_TRIANGLE 100
 VCL_API size_t vcl_raster_scratch_bytes(void);
 VCL_API vcl_status vcl_raster_scratch_init(vcl_ctx* ctx);
 VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
@@ -137,6 +142,19 @@ VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int
 VCL_API vcl_status vcl_rasterize_bwd(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W,
                                      int H, int views, const float* rast, const float* grad_bary, float* grad_clip,
                                      void* stream);
+/* GL tie census of a finished raster `rast` (the output of vcl_rasterize_fwd
+ * for the same clip/tri).  No counterpart in the reference: these are the
+ * pixels where GL leaves the result implementation-defined, so where a real
+ * GL driver (rasterize.cpp:252-254) may legally give another triangle id
+ * than these rules.  flags [views*H*W] (device, written whole): bit 1 = the
+ * pixel centre lies exactly on an edge of a triangle whose closed interior
+ * holds it (the top-left rule decided coverage); bit 2 = a triangle other
+ * than the winner covers the pixel at exactly the winning depth (the lower
+ * id decided).  counts [2] (device, written): pixels with bit 1, bit 2.
+ * A diagnostic, not part of the fit path. */
+VCL_API vcl_status vcl_raster_ties(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W, int H,
+                                   int views, const float* rast, uint32_t* flags, unsigned long long* counts,
+                                   void* stream);
 
 /* ----------------------------------------------------------- interpolate */
 /* Interpolate::forward (interpolate.cu:51-60, kernel :20-49): out[p] =

@@ -20,6 +20,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout the recipes read (present only where the oracle's
+# reference build is made; the GPU tests never need it)
+REF_DIR = os.environ.get("VCL_REF_DIR", "/root/reference")
 ORC_PATH = os.path.join(HERE, "liborc.so")
 REF_PATH = os.path.join(HERE, "_ref", "libvclref.so")
 
@@ -35,6 +38,7 @@ SIGS = {
     "project_fwd": "ippip",
     "project_bwd": "ippip",
     "rasterize_fwd": "iiipipiipp",
+    "raster_ties": "iiipipippp",
     "rasterize_bwd": "iiipipppp",
     "interpolate_fwd": "iiiiipppppp",
     "interpolate_bwd": "iiiiipppppp",

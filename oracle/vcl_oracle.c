@@ -272,6 +272,71 @@ void orc_rasterize_fwd(int W, int H, int views, const float* clip, int nv,
     free(setup); free(depth); free(best); free(sxs); free(sys);
 }
 
+/* Tie census: the pixels at which a GL implementation may legally differ
+ * from the restated rules above.  GL fixes neither the fill rule for a
+ * centre exactly on an edge nor (with a 24-bit buffer) equal-depth order, so
+ * these are the pixels where a triangle-id mismatch against real GL would be
+ * admissible; everywhere else the rules are the same.  Walks every triangle
+ * over its raster_bbox() with the same arithmetic as orc_rasterize_fwd. */
+void orc_raster_ties(int W, int H, int views, const float* clip, int nv,
+                     const uint32_t* tri, int nt, const float* rast,
+                     uint32_t* flags, long long* counts) {
+    const float xs = 2.f / (float)W, ys = 2.f / (float)H;
+    const size_t npix = (size_t)W * H;
+    float* sxs = (float*)malloc(sizeof(float) * (size_t)W);
+    float* sys = (float*)malloc(sizeof(float) * (size_t)H);
+    for (int px = 0; px < W; ++px) sxs[px] = (float)(2 * px + 1 - W) / (float)W;
+    for (int py = 0; py < H; ++py) sys[py] = (float)(2 * py + 1 - H) / (float)H;
+    memset(flags, 0, sizeof(uint32_t) * npix * (size_t)views);
+    (void)nv;
+    for (int vw = 0; vw < views; ++vw) {
+        const float* cv = clip + (size_t)vw * nv * 4;
+        const float* rv = rast + (size_t)vw * npix * 4;
+        uint32_t* fv = flags + (size_t)vw * npix;
+        for (int t = 0; t < nt; ++t) {
+            const float* c0 = cv + (size_t)tri[3 * t] * 4;
+            const float* c1 = cv + (size_t)tri[3 * t + 1] * 4;
+            const float* c2 = cv + (size_t)tri[3 * t + 2] * 4;
+            rtri T;
+            raster_setup(c0, c1, c2, xs, ys, 0, &T);
+            if (raster_outside(c0, c1, c2)) T.valid = 0;
+            int bx0, bx1, by0, by1;
+            if (!T.valid || !raster_bbox(c0, c1, c2, W, H, &bx0, &bx1, &by0, &by1)) continue;
+            for (int py = by0; py <= by1; ++py) {
+                float sy = sys[py];
+                for (int px = bx0; px <= bx1; ++px) {
+                    float sx = sxs[px];
+                    float A[3];
+                    int closed = 1, on_edge = 0, in = 1;
+                    for (int i = 0; i < 3; ++i) {
+                        A[i] = (T.a[i] * sx + T.b[i] * sy) + T.k[i];
+                        closed &= T.sigma * A[i] >= 0.f;
+                        on_edge |= A[i] == 0.f;
+                        in &= edge_in(A[i], T.a[i], T.b[i], T.sigma);
+                    }
+                    if (!closed) continue;
+                    float D = (A[0] + A[1]) + A[2];
+                    if (!(T.sigma * D > 0.f)) continue;
+                    float zn = (A[0] * T.z[0] + A[1] * T.z[1]) + A[2] * T.z[2];
+                    float wn = (A[0] * T.w[0] + A[1] * T.w[1]) + A[2] * T.w[2];
+                    float zw = zn / wn;
+                    if (!(zw >= -1.f && zw < 1.f)) continue;
+                    size_t pi = (size_t)py * W + px;
+                    if (on_edge) fv[pi] |= 1u;
+                    if (in && rv[pi * 4 + 3] != (float)(t + 1) && rv[pi * 4 + 3] > 0.f && zw == rv[pi * 4 + 2])
+                        fv[pi] |= 2u;
+                }
+            }
+        }
+    }
+    counts[0] = counts[1] = 0;
+    for (size_t i = 0; i < npix * (size_t)views; ++i) {
+        counts[0] += (flags[i] & 1u) != 0;
+        counts[1] += (flags[i] & 2u) != 0;
+    }
+    free(sxs); free(sys);
+}
+
 /* rasterize.cu:84-141 */
 void orc_rasterize_bwd(int W, int H, int views, const float* clip, int nv,
                        const uint32_t* tri, const float* rast, const float* gb, float* gclip) {

@@ -35,6 +35,16 @@ void orc_project_bwd(int nv, const float* mat16, const float* grad_out, int dim,
 void orc_rasterize_fwd(int W, int H, int views, const float* clip, int nv,
                        const uint32_t* tri, int nt, int enable_db,
                        float* rast, float* db);
+/* ---- GL tie census of a finished raster (no reference counterpart: GL
+ *      leaves these pixels implementation-defined, rasterize.cpp:252-254).
+ *      flags[pixel] |= 1: the centre lies exactly on an edge of a triangle
+ *      whose closed interior holds it (the top-left rule decides);
+ *      flags[pixel] |= 2: a triangle other than the winner covers the pixel
+ *      at exactly the winning depth (the lower id decides).
+ *      counts[0], counts[1] = pixels with bit 1, bit 2. ------------------- */
+void orc_raster_ties(int W, int H, int views, const float* clip, int nv,
+                     const uint32_t* tri, int nt, const float* rast,
+                     uint32_t* flags, long long* counts);
 /* ---- rasterize backward: rasterize.cu:84-141 ---------------------------- */
 void orc_rasterize_bwd(int W, int H, int views, const float* clip, int nv,
                        const uint32_t* tri, const float* rast,

@@ -34,7 +34,8 @@ def project(lib, scene, pos):
 def run_chain(lib, scene, mode=0, target=None, rast=None, db=None, pos=None, pyr=None,
               lobes=None, raster_lib=None, adam_step=1):
     """Forward + backward of the predicted render, then one Adam step on a
-    copy of the texture level 0.  Returns a dict of every intermediate."""
+    copy of the texture level 0 (none when adam_step is 0).  Returns a dict
+    of every intermediate."""
     S = scene
     W, H, V, C, K = S.W, S.H, S.views, S.C, S.K
     N = W * H * V
@@ -98,10 +99,11 @@ def run_chain(lib, scene, mode=0, target=None, rast=None, db=None, pos=None, pyr
     for v in range(V):
         lib.project_bwd(S.nv, S.mvp[v].copy(), np.ascontiguousarray(g_clip[v]), 4, g_pos)
     r["g_pos"] = g_pos
-    n0 = S.tex_w * S.tex_h * C
-    p = pyr[:n0].copy(); m = f32((n0,)); vv = f32((n0,))
-    lib.adam(mode, n0, p, np.ascontiguousarray(g_pyr[:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, adam_step)
-    r["adam_p"], r["adam_m"], r["adam_v"] = p, m, vv
+    if adam_step:
+        n0 = S.tex_w * S.tex_h * C
+        p = pyr[:n0].copy(); m = f32((n0,)); vv = f32((n0,))
+        lib.adam(mode, n0, p, np.ascontiguousarray(g_pyr[:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, adam_step)
+        r["adam_p"], r["adam_m"], r["adam_v"] = p, m, vv
     return r
 
 
@@ -112,6 +114,7 @@ def oracle_fit(S, mode, steps, target, lr=None):
     (axis | sharpness | amplitude), all with persistent moments."""
     lib = O.orc()
     lr = S.lr if lr is None else lr
+    lr_pos = getattr(S, "lr_pos", 0.0) or lr     # positions have their own Adam step (0: the common one)
     pos = S.pos.copy()
     pyr = build_pyramid(S, S.tex_init)
     lobes = np.concatenate([S.lobe_axis_init.reshape(-1), S.lobe_sharp_init.reshape(-1),
@@ -137,7 +140,7 @@ def oracle_fit(S, mode, steps, target, lr=None):
         pyr = pyr.copy(); pyr[:n0] = p0
         lib.mip_build(S.tex_w, S.tex_h, C, S.levels, pyr)
         pp = np.ascontiguousarray(pos.reshape(-1))
-        lib.adam(mode, pp.size, pp, np.ascontiguousarray(r["g_pos"].reshape(-1)), mp, vp, lr, 0.9, 0.999, 1e-8, t)
+        lib.adam(mode, pp.size, pp, np.ascontiguousarray(r["g_pos"].reshape(-1)), mp, vp, lr_pos, 0.9, 0.999, 1e-8, t)
         pos = pp.reshape(-1, 3)
         gl = np.concatenate([r["g_axis"].reshape(-1), r["g_sharp"].reshape(-1), r["g_amp"].reshape(-1)]).astype(np.float32)
         lib.adam(mode, lobes.size, lobes, gl, ml, vl, lr, 0.9, 0.999, 1e-8, t)

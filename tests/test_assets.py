@@ -9,6 +9,7 @@ import struct
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from vcl_b200 import capi
 
 
@@ -113,7 +114,7 @@ def test_sg_lobe_list(tmp_path):
         capi.load_sg(_write(tmp_path / "short.txt", text + "1 2 3\n"))
 
 
-ENVMAP = "/root/reference/data/envmap2.txt"
+ENVMAP = os.path.join(O.REF_DIR, "data", "envmap2.txt")
 
 
 @pytest.mark.skipif(not os.path.exists(ENVMAP), reason="the reference's lobe file is not on this machine")

@@ -193,3 +193,32 @@ def test_mse_compat_reduction_drops_tail():
     n2 = 64
     pred = np.ones(n2, np.float32); tgt = np.zeros(n2, np.float32); g = np.zeros(n2, np.float32)
     assert O.orc().mse(0, n2, pred, tgt, g) == O.orc().mse(1, n2, pred, tgt, g) == 32.0
+
+
+def test_tie_census_known_answers():
+    """orc_raster_ties on scenes with known ties: the diagonal of a
+    full-screen quad runs through the 8 pixel centres of an 8x8 view (8 edge
+    ties, no depth ties); the same triangle drawn twice makes every covered
+    pixel a depth tie won by the lower id; a generic scene has none."""
+    quad = np.array([[-1, -1, 0.5, 1], [1, -1, 0.5, 1], [1, 1, 0.5, 1], [-1, 1, 0.5, 1]], np.float32)
+    tri = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    r = np.zeros((64, 4), np.float32); d = r.copy()
+    O.orc().rasterize_fwd(8, 8, 1, quad, 4, tri, 2, 1, r, d)
+    f = np.zeros(64, np.uint32); c = np.zeros(2, np.int64)
+    O.orc().raster_ties(8, 8, 1, quad, 4, tri, 2, r, f, c)
+    assert tuple(c) == (8, 0)
+    assert np.array_equal(np.nonzero(f.reshape(8, 8))[0], np.arange(8))
+    dup = np.array([[-0.9, -0.8, 0.1, 1], [0.7, -0.6, 0.1, 1], [0.1, 0.9, 0.1, 1]] * 2, np.float32)
+    tri = np.array([[0, 1, 2], [3, 4, 5]], np.uint32)
+    r = np.zeros((16 * 12, 4), np.float32); d = r.copy()
+    O.orc().rasterize_fwd(16, 12, 1, dup, 6, tri, 2, 1, r, d)
+    f = np.zeros(16 * 12, np.uint32)
+    O.orc().raster_ties(16, 12, 1, dup, 6, tri, 2, r, f, c)
+    assert c[1] == (r[:, 3] == 1).sum() > 0
+    S = scenes.config1()
+    clip = chain.project(O.orc(), S, S.pos)
+    r = np.zeros((S.W * S.H, 4), np.float32); d = r.copy()
+    O.orc().rasterize_fwd(S.W, S.H, 1, clip, S.nv, S.tri, S.nt, 1, r, d)
+    f = np.zeros(S.W * S.H, np.uint32)
+    O.orc().raster_ties(S.W, S.H, 1, clip, S.nv, S.tri, S.nt, r, f, c)
+    assert tuple(c) == (0, 0)

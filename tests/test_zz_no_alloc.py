@@ -97,3 +97,37 @@ def test_static_scratch_rejects_oversize_request(ctx):
     # the context stays usable
     S = _scenes()[2]
     assert np.array_equal(_raster(ctx, S, "rasterize_fwd_static")[0], _raster(ctx, S, "rasterize_fwd")[0])
+
+
+def test_static_scratch_bin_list_cut_to_room(ctx):
+    """A request whose depth keys nearly fill the scratch: the bin list gets
+    only the room that is left, less than the automatic capacity asks for.
+    The documented sizes (8 B per pixel, 100 B per view and triangle, 12 B
+    per tile, each part rounded up to 256 B) say how much room that is; the
+    result stays bit-identical to the workspace path, with every triangle
+    through the bins and with the default direct paths."""
+    S = scenes.make_scene("noalloc-big", mesh=("ico", 4), W=2000, H=2000, views=1, tex=16, K=1, dist=(2.0, 3.5),
+                          disp=0.05, seed=4)
+    a256 = lambda x: (x + 255) // 256 * 256
+    npix, vt = S.W * S.H * S.views, S.nt * S.views
+    tile = 16
+    ntiles = -(-S.W // tile) * -(-S.H // tile) * S.views
+    fixed = a256(8 * npix) + a256(96 * vt) + a256(4 * vt) + 3 * a256(4 * (ntiles + 1))
+    limit = capi.lib().vcl_raster_scratch_bytes()
+    assert fixed < limit
+    room = ((limit - fixed) // 4) & ~63
+    want = vt * 6 + ntiles * 4 + (1 << 20)        # the automatic bin capacity
+    assert room < want
+    ctx.set_raster_config(tile, 0)
+    try:
+        for areas in ((0, 0), (-1, -1)):
+            ctx.set_raster_areas(*areas)
+            wr, wd = _raster(ctx, S, "rasterize_fwd")
+            gr, gd = _raster(ctx, S, "rasterize_fwd_static")
+            assert ctx.raster_overflow_count() == 0
+            assert (wr[:, 3] > 0).sum() > 100000
+            assert np.array_equal(gr, wr), areas
+            assert np.array_equal(gd, wd), areas
+    finally:
+        ctx.set_raster_config(16, 0)
+        ctx.set_raster_areas(-1, -1)

@@ -43,6 +43,7 @@ SIGNATURES = {
     "vcl_raster_scratch_init": (c_int, [P]),
     "vcl_rasterize_fwd_static": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
     "vcl_rasterize_bwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
+    "vcl_raster_ties": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
     "vcl_interpolate_fwd": (c_int, [P, P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P]),
     "vcl_interpolate_bwd": (c_int, [P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P, P]),
     "vcl_texture_fwd": (c_int, [P, P, P, P, c_int, c_int, c_int, P, c_int, c_int, c_int, c_int, P, P]),

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <mutex>
 #include <cstdio>
 #include <cstdarg>
 #include "../../include/vcl.h"
@@ -11,7 +12,11 @@ struct vcl_ctx {
     int device = 0;
     int mode = VCL_MODE_COMPAT;
     int sm_count = 148;
+    // last error message; written and read under err_mu, since a context's
+    // jobs can report errors from more than one host thread (the serving
+    // loop's tick thread and its set-up worker)
     std::string err;
+    mutable std::mutex err_mu;
     // raster binning schedule
     int tile = 16;
     long long bin_capacity = 0;   // 0 = automatic

@@ -9,6 +9,7 @@ vcl_status vcl_fail(vcl_ctx* ctx, vcl_status code, const char* fmt, ...) {
         va_start(ap, fmt);
         vsnprintf(buf, sizeof buf, fmt, ap);
         va_end(ap);
+        std::lock_guard<std::mutex> lock(ctx->err_mu);
         ctx->err = buf;
     }
     return code;
@@ -91,7 +92,16 @@ VCL_API void vcl_destroy(vcl_ctx* ctx) {
     delete ctx;
 }
 
-VCL_API const char* vcl_last_error(const vcl_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+// The message is copied for the calling thread under the context's lock:
+// the pointer stays valid until this thread's next vcl_last_error call,
+// whatever other threads report meanwhile.
+VCL_API const char* vcl_last_error(const vcl_ctx* ctx) {
+    if (!ctx) return "null context";
+    thread_local std::string copy;
+    std::lock_guard<std::mutex> lock(ctx->err_mu);
+    copy = ctx->err;
+    return copy.c_str();
+}
 
 VCL_API vcl_status vcl_set_mode(vcl_ctx* ctx, int mode) {
     VCL_CTX_CHECK();

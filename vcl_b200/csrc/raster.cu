@@ -46,6 +46,9 @@ struct __align__(16) RTri {
     float4 w;   // w0 w1 w2 -
     int4 box;   // x0 x1 y0 y1 ; empty when x0 > x1
 };
+// the workspace's per-(view, triangle) cost that vcl.h states: this record
+// plus one medium-list entry
+static_assert(sizeof(RTri) + sizeof(int) == VCL_RASTER_BYTES_PER_VIEW_TRIANGLE, "raster record size changed");
 
 constexpr int CHUNK = 128;
 // default box areas (pixels): up to SMALL_AREA a triangle is rasterized by its
@@ -586,6 +589,80 @@ __global__ void k_raster_bwd(const float* __restrict__ clip, int nv, const uint3
     red_add4(gv + (size_t)i2 * 4, v[6], v[7], 0.f, v[8]);
 }
 
+// GL tie census of a finished raster (vcl_raster_ties): one warp per (view,
+// triangle), a lane per pixel row of the triangle's box, walking the row's
+// conservative span with the rasterizer's own arithmetic.  Bit 1 marks a
+// centre exactly on an edge of a triangle whose closed interior holds it
+// (the top-left rule decided), bit 2 a pixel that a triangle other than the
+// winner covers at exactly the winning depth (the lower id decided).
+__global__ void __launch_bounds__(256) k_ties(const float4* __restrict__ clip, int nv, const uint32_t* __restrict__ tri,
+                                              int nt, int W, int H, int views, const float4* __restrict__ rast,
+                                              unsigned* __restrict__ flags) {
+    extern __shared__ float s_ndc[];   // [W] column centres, [H] row centres
+    stage_ndc(s_ndc, W, H);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long work = (long long)views * nt;
+    for (long long g = warp; g < work; g += nwarps) {
+        const int view = (int)(g / nt), t = (int)(g - (long long)view * nt);
+        const uint32_t i0 = tri[3 * (size_t)t], i1 = tri[3 * (size_t)t + 1], i2 = tri[3 * (size_t)t + 2];
+        if (i0 >= (uint32_t)nv || i1 >= (uint32_t)nv || i2 >= (uint32_t)nv) continue;
+        const float4* cv = clip + (size_t)view * nv;
+        RTri r;
+        bool valid = false;
+        setup_tri(cv[i0], cv[i1], cv[i2], W, H, r, valid);
+        if (r.box.x > r.box.y || r.box.z > r.box.w) continue;
+        SpanEq q;
+        span_setup(r, q);
+        const size_t vbase = (size_t)view * W * H;
+        const float sg = r.a.w;
+        for (int py = r.box.z + lane; py <= r.box.w; py += 32) {
+            const float sy = s_ndc[W + py];
+            int x0, x1;
+            if (!row_span(r, q, sy, W, x0, x1)) continue;
+            for (int px = x0; px <= x1; ++px) {
+                const float sx = s_ndc[px];
+                const float A0 = edge(r.a.x, r.b.x, r.k.x, sx, sy);
+                const float A1 = edge(r.a.y, r.b.y, r.k.y, sx, sy);
+                const float A2 = edge(r.a.z, r.b.z, r.k.z, sx, sy);
+                if (!(mul(sg, A0) >= 0.f && mul(sg, A1) >= 0.f && mul(sg, A2) >= 0.f)) continue;
+                const float D = add(add(A0, A1), A2);
+                if (!(mul(sg, D) > 0.f)) continue;
+                const float zn = add(add(mul(A0, r.z.x), mul(A1, r.z.y)), mul(A2, r.z.z));
+                const float wn = add(add(mul(A0, r.w.x), mul(A1, r.w.y)), mul(A2, r.w.z));
+                const float zw = dvd(zn, wn);
+                if (!(zw >= -1.f && zw < 1.f)) continue;
+                const size_t pi = vbase + (size_t)py * W + px;
+                unsigned f = (A0 == 0.f || A1 == 0.f || A2 == 0.f) ? 1u : 0u;
+                if (edge_in(A0, r.a.x, r.b.x, sg) && edge_in(A1, r.a.y, r.b.y, sg) && edge_in(A2, r.a.z, r.b.z, sg)) {
+                    const float4 rp = rast[pi];
+                    if (rp.w > 0.f && rp.w != (float)(t + 1) && zw == rp.z) f |= 2u;
+                }
+                if (f) atomicOr(&flags[pi], f);
+            }
+        }
+    }
+}
+
+__global__ void k_tie_count(const unsigned* __restrict__ flags, long long n, unsigned long long* __restrict__ counts) {
+    unsigned long long e = 0, d = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned f = flags[i];
+        e += f & 1u;
+        d += (f >> 1) & 1u;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, o);
+        d += __shfl_xor_sync(0xffffffffu, d, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (e | d)) {
+        atomicAdd(&counts[0], e);
+        atomicAdd(&counts[1], d);
+    }
+}
+
 struct RasterWS {
     unsigned long long* keys;
     RTri* setup;
@@ -762,6 +839,30 @@ VCL_API vcl_status vcl_rasterize_bwd(vcl_ctx* ctx, const float* clip, int nv, co
     k_raster_bwd<<<vcl_blocks(npix, 256), 256, 0, (cudaStream_t)stream>>>(
         clip, nv, tri, nt, W, H, npix, (const float4*)rast, (const float2*)grad_bary, grad_clip);
     return vcl_launch_check(ctx, "rasterize_bwd");
+}
+
+VCL_API vcl_status vcl_raster_ties(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt, int W, int H,
+                                   int views, const float* rast, uint32_t* flags, unsigned long long* counts,
+                                   void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(W > 0 && H > 0 && views > 0 && nv >= 0 && nt >= 0, "bad raster sizes");
+    VCL_REQUIRE(rast && flags && counts, "null buffer");
+    VCL_REQUIRE(nt == 0 || (clip && tri), "clip/tri is null");
+    VCL_REQUIRE(((uintptr_t)clip & 15) == 0 && ((uintptr_t)rast & 15) == 0 && ((uintptr_t)flags & 3) == 0 &&
+                    ((uintptr_t)counts & 7) == 0, "misaligned buffer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long npix = (long long)W * H * views;
+    vcl_status st = vcl_cuda_check(ctx, cudaMemsetAsync(flags, 0, sizeof(uint32_t) * (size_t)npix, s), "ties memset");
+    if (!st) st = vcl_cuda_check(ctx, cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s), "ties memset");
+    if (st) return st;
+    if ((long long)views * nt > 0) {
+        const size_t tab = sizeof(float) * (size_t)(W + H);
+        if (tab > 48 * 1024) cudaFuncSetAttribute(k_ties, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab);
+        k_ties<<<ctx->sm_count * 8, 256, tab, s>>>((const float4*)clip, nv, tri, nt, W, H, views,
+                                                   (const float4*)rast, flags);
+    }
+    k_tie_count<<<ctx->sm_count * 4, 256, 0, s>>>(flags, npix, counts);
+    return vcl_launch_check(ctx, "raster_ties");
 }
 
 }  // extern "C"

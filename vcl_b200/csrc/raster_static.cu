@@ -14,9 +14,11 @@
 // Limits and rules:
 //   * RASTER_SCRATCH_BYTES (VCL_RASTER_SCRATCH_BYTES, 32 MiB) bounds the
 //     request: the per-pixel depth keys (8 B x W x H x views), the triangle
-//     records (80 B x views x nt) and the per-tile counters must fit, and the
-//     remainder holds the tile bin lists.  Larger requests are rejected with
-//     VCL_ERR_ARG and a message that gives the bytes needed.  A bin list that
+//     records with their medium-list entries (96 + 4 = 100 B x views x nt,
+//     VCL_RASTER_BYTES_PER_VIEW_TRIANGLE) and the per-tile counters (12 B x
+//     tiles x views) must fit, and the remainder holds the tile bin lists.
+//     Larger requests are rejected with VCL_ERR_ARG and a message that gives
+//     the bytes needed.  A bin list that
 //     does not fit the remainder falls back to testing every large triangle
 //     for the overflowing tiles: same result, slower.
 //   * Nothing in the scratch has to start at zero: every call initializes
@@ -31,7 +33,10 @@
 //     vcl_raster_scratch_init or lazily by the first call on that device,
 //     with that device current.  That first call may load the module that
 //     holds the scratch, so make it during set-up, before any stream capture
-//     begins.
+//     begins.  cudaDeviceReset by the host application unloads the module:
+//     the cached address is stale after it, so vcl_raster_scratch_init
+//     always resolves the address anew, and a caller that resets the device
+//     calls it again before the next static call.
 #include <mutex>
 
 #include "common.cuh"
@@ -47,7 +52,7 @@ static __device__ __align__(256) unsigned char g_raster_scratch[RASTER_SCRATCH_B
 std::mutex g_scratch_mu;
 void* g_scratch_addr[MAX_DEVICES] = {};
 
-vcl_status scratch_address(vcl_ctx* ctx, void** out) {
+vcl_status scratch_address(vcl_ctx* ctx, void** out, bool refresh) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "raster scratch: cudaGetDevice");
@@ -57,7 +62,7 @@ vcl_status scratch_address(vcl_ctx* ctx, void** out) {
     if (dev < 0 || dev >= MAX_DEVICES)
         return vcl_fail(ctx, VCL_ERR_STATE, "raster scratch: device ordinal %d above %d", dev, MAX_DEVICES - 1);
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (refresh || !g_scratch_addr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_raster_scratch);
         if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "raster scratch: cudaGetSymbolAddress");
@@ -78,7 +83,7 @@ VCL_API size_t vcl_raster_scratch_bytes(void) { return RASTER_SCRATCH_BYTES; }
 VCL_API vcl_status vcl_raster_scratch_init(vcl_ctx* ctx) {
     VCL_CTX_CHECK();
     void* p = nullptr;
-    return scratch_address(ctx, &p);
+    return scratch_address(ctx, &p, true);
 }
 
 VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,
@@ -97,14 +102,14 @@ VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int
     const size_t fixed = raster_ws_size(W, H, views, nt, T, 0);
     VCL_REQUIRE(fixed <= RASTER_SCRATCH_BYTES,
                 "rasterize_fwd_static: W=%d H=%d views=%d nt=%d needs %zu bytes of scratch "
-                "(8 B per pixel + 84 B per view and triangle + tile counters), the static limit is %zu; "
+                "(8 B per pixel + %d B per view and triangle + 12 B per tile), the static limit is %zu; "
                 "use vcl_rasterize_fwd",
-                W, H, views, nt, fixed, RASTER_SCRATCH_BYTES);
+                W, H, views, nt, fixed, VCL_RASTER_BYTES_PER_VIEW_TRIANGLE, RASTER_SCRATCH_BYTES);
     const long long want = ctx->bin_capacity ? ctx->bin_capacity : raster_auto_capacity(views, nt, W, H, T);
     const long long room = (long long)((RASTER_SCRATCH_BYTES - fixed) / sizeof(int)) & ~63ll;
     const long long cap = want < room ? want : room;
     void* scratch = nullptr;
-    vcl_status st = scratch_address(ctx, &scratch);
+    vcl_status st = scratch_address(ctx, &scratch, false);
     if (st) return st;
     return raster_fwd_ws(ctx, scratch, ctx_sched(ctx, T, cap), ctx->dev_flags, clip, nv, tri, nt, W, H, views, rast,
                          db, (cudaStream_t)stream);
