@@ -42,6 +42,11 @@ def parse():
     ap.add_argument("--jobs", type=int, default=32, help="serve: fit jobs submitted")
     ap.add_argument("--lams", default="10,30,100,300,1000", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mix", action="store_true", help="default run: skip the batched-vs-plain mix measurement")
+    ap.add_argument("--no-serve", action="store_true", help="default run: skip the serving measurement")
+    ap.add_argument("--serve-lam", type=float, default=100.0, help="default run: serving arrival rate (jobs/s)")
+    ap.add_argument("--serve-jobs", type=int, default=24, help="default run: serving jobs per repeat")
+    ap.add_argument("--serve-repeats", type=int, default=3, help="default run: serving repeats")
     ap.add_argument("--no-stages", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--strategy", default="both", choices=["both", "plain", "fused"])
@@ -58,6 +63,14 @@ def make_scene(args):
     if args.config == "config5":
         return scenes.config5(views=args.views or 4)
     return scenes.config2(views=args.views or 16)
+
+
+def bench_config(S, world):
+    """The `config` object of both arms' JSON lines (same workload, same keys)."""
+    return {"workload": workload_name(S), "global_batch": S.views * world, "seq_len": 0,
+            "parallelism": f"replicas x{world}",
+            "adam": {"lr": S.lr, "lr_pos": S.lr_pos or S.lr, "betas": [0.9, 0.999], "eps": 1e-8},
+            "l2": "per-step working set > 2 GB (larger than the 126 MB L2); no flush"}
 
 
 def workload_name(S):
@@ -131,7 +144,11 @@ class ClockSampler:
 # ------------------------------------------------------------ algorithmic bytes
 def stage_bytes(S, ncov):
     """Compulsory FP32 traffic per fit iteration by stage (caches ignored,
-    each buffer counted once), the per-stage model of the design notes."""
+    each buffer counted once).  Every per-pixel kernel reads the raster word
+    of all N pixels; the other per-pixel inputs are read only at the ncov
+    covered pixels (background pixels return early), and outputs are
+    written at all N pixels where the kernel clears the background, at the
+    covered ones where it does not."""
     N = S.W * S.H * S.views
     C = S.C
     ntex = S.tex_w * S.tex_h
@@ -139,19 +156,19 @@ def stage_bytes(S, ncov):
     texel_fwd = min(npyr_bytes, ncov * 8 * C * 4)
     return {
         "raster_fwd": S.nv * 16 * S.views + S.nt * 12 + N * 32,
-        "interp_fwd": N * (16 + 16) + N * (8 + 16),
-        "texture_fwd": N * (4 + 8 + 16) + N * C * 4 + texel_fwd,
+        "interp_fwd": N * 16 + ncov * 16 + N * (8 + 16),                 # rast; db; uv + DA written everywhere
+        "texture_fwd": N * 16 + ncov * (8 + 16) + N * C * 4 + texel_fwd,  # rast; uv, DA; colour everywhere
         "normal_axis": N * 16 + N * 12,
         "view_axis": N * 12,
-        "sg_specular_fwd": N * (16 + 12 + 12 + 4) + N * 20,
-        "sg_fwd": N * (16 + 12 + C * 4 + 12 + 8) + N * C * 4 + S.K * (4 + C) * 4,
+        "sg_specular_fwd": N * 16 + ncov * (12 + 12 + 4) + N * 20,        # rast; n, view, roughness; 3 outputs
+        "sg_fwd": N * 16 + ncov * (12 + C * 4 + 12 + 8) + N * C * 4 + S.K * (4 + C) * 4,
         "antialias_fwd": N * (16 + C * 4) + N * C * 4,
         "mse": N * C * 4 * 2 + N * C * 4,
         "antialias_bwd": N * (C * 8 + 16) + N * C * 4,
-        "sg_bwd": N * (C * 4 * 2 + 16 + 12 + 12 + 8) + N * C * 4,
-        "texture_bwd": N * (C * 4 + 4 + 8 + 16) + N * 8 + texel_fwd,
-        "interp_bwd": N * (16 + 8) + N * 8,
-        "raster_bwd": N * (16 + 8),
+        "sg_bwd": N * 16 + ncov * (C * 4 * 2 + 12 + 12 + 8) + ncov * C * 4,
+        "texture_bwd": N * 16 + ncov * (C * 4 + 8 + 16) + ncov * 8 + texel_fwd,
+        "interp_bwd": N * 16 + ncov * 8 + ncov * 8,
+        "raster_bwd": N * 16 + ncov * 8,
         "project": S.nv * 12 * 2,
         "optimizer": 28 * (ntex * C + S.nv * 3 + S.K * (4 + C)) + ntex * C * 4 * (1 / 3 + 2 / 3 + 1 + 4 / 3),
     }
@@ -159,17 +176,20 @@ def stage_bytes(S, ncov):
 
 def fused_bytes(S, ncov):
     """Compulsory FP32 traffic of each fused-step stage (one launch; caches
-    ignored, each buffer counted once).  N = views*W*H pixels, C = 4."""
+    ignored, each buffer counted once).  N = views*W*H pixels, ncov of them
+    covered, C = 4; inputs other than the raster word are read at covered
+    pixels only."""
     N = S.W * S.H * S.views
     ntex = S.tex_w * S.tex_h
     texels = min(ntex * 16 * 4 / 3, ncov * 8 * 16)      # trilinear reads, at most the pyramid once
     verts = S.views * S.nv * 16
     return {
         "raster": verts + S.nt * 12 + N * 32,                       # clip, indices -> rast + db
-        "shade_fwd": N * 32 + S.nv * 20 + texels + N * 32 + ncov * 52,  # ... -> colour, diffuse env, shading records
+        # rast (all), db (covered) -> colour, diffuse env (all), shading records (covered)
+        "shade_fwd": N * 16 + ncov * 16 + S.nv * 20 + texels + N * 32 + ncov * 52,
         "aa_fwd_mse": N * 64 + verts,                               # rast, colour, target -> image gradient, loss
         "aa_bwd": N * 64 + verts * 2,                               # rast, colour, grad -> colour grad, clip grad
-        "bwd_pix": N * 64 + texels + verts * 2,                     # rast, db, colour grad, diffuse env -> texel, clip grads
+        "bwd_pix": N * 16 + ncov * 48 + texels + verts * 2,         # rast; db, colour grad, diffuse env -> texel, clip grads
         "sg_lobes": ncov * (52 + 16) + S.K * 32,                    # shading records, colour grad -> lobe grads
     }
 
@@ -189,6 +209,45 @@ BOUND_NOTE = {
     "sg_lobes": "k_sg_lobes is FP32/MUFU-bound (per pixel and lobe: 2 rsqrt, 4 ex2, ~35 paired FP32 ops), "
                 "not HBM-bound",
 }
+
+
+# ------------------------------------------------------------ measured peaks
+def measure_unit_peaks(ctx, stream, reps=3):
+    """Peak rates of the L2 vector reductions and of the MUFU pipe on this
+    GPU, from the library's throughput probes (best of `reps`, CUDA events on
+    the launching stream): red.global.add.v4.f32 per second over a 32 MB
+    buffer (inside L2), and ex2/rsqrt operations per second."""
+    import ctypes
+    import torch
+    from vcl_b200 import capi
+    L = capi.lib()
+    sh = stream.cuda_stream
+    buf = torch.zeros(8 << 20, dtype=torch.float32, device="cuda")
+    out = torch.zeros(L.vcl_probe_mufu_threads(ctx.h), dtype=torch.float32, device="cuda")
+    n = ctypes.c_longlong()
+
+    def best(fn):
+        fn()
+        t = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            stream.synchronize()
+            t.append(e0.elapsed_time(e1) * 1e-3)
+        return min(t)
+
+    t_red = best(lambda: ctx._check(L.vcl_probe_red_throughput(ctx.h, buf.data_ptr(), buf.numel(), 20,
+                                                               ctypes.byref(n), sh), "probe"))
+    reds = n.value
+    t_mufu = best(lambda: ctx._check(L.vcl_probe_mufu_throughput(ctx.h, out.data_ptr(), 4096, ctypes.byref(n), sh),
+                                     "probe"))
+    mufu = n.value
+    return {"l2_red_v4_per_s": reds / t_red, "mufu_ops_per_s": mufu / t_mufu,
+            "how": "vcl_probe_red_throughput (coalesced red.global.add.v4.f32 over 32 MB, 20 passes) and "
+                   "vcl_probe_mufu_throughput (8 independent ex2.approx/rsqrt.approx chains per thread, "
+                   "8 blocks of 256 per SM); best of 3, CUDA events"}
 
 
 # ------------------------------------------------------------------ vcl arm
@@ -326,6 +385,8 @@ def run_vcl(args, rank, world):
                e2e_ms=e2e_ms, clocks=clk, scene=S, best=best)
     if rank == 0 and not args.no_stages:
         out["stages"] = stage_times(ctx, S, target, stream)
+    if rank == 0:
+        out["unit_peaks"] = measure_unit_peaks(ctx, stream)
     ctx.close()
     return out
 
@@ -392,68 +453,140 @@ def stage_times(ctx, S, target, stream, reps=5):
             e1.record(stream)
             stream.synchronize()
             res[name] = e0.elapsed_time(e1) / reps
-    return {"ms": res, "ncov": ncov}
+        # GL tie census of this raster: pixels where a GL driver may legally
+        # pick another triangle (centre exactly on an edge; equal depth)
+        ctx.rasterize_fwd(clip, S.nv, tri, S.nt, W, H, V, rast, db, sh)
+        flags = torch.zeros(N, dtype=torch.int32, device="cuda")
+        counts = torch.zeros(2, dtype=torch.int64, device="cuda")
+        ctx.raster_ties(clip, S.nv, tri, S.nt, W, H, V, rast, flags, counts, sh)
+        stream.synchronize()
+        c = counts.cpu().tolist()
+    ties = {"edge_tie_pixels": c[0], "depth_tie_pixels": c[1], "covered_pixels": ncov, "pixels": N,
+            "geometry": "the workload's starting positions"}
+    return {"ms": res, "ncov": ncov, "ties": ties}
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_reference_iteration(S, threads, views_sample=1):
-    """Time the reference's own kernels (oracle/_ref, compiled for the host)
-    on `views_sample` views of one fit iteration plus the parameter update,
-    with `threads` host threads; the raster stage is the CPU restatement of
-    the reference's GL rasterizer.  Returns (seconds for a full iteration
-    extrapolated to all views, kind, sample description)."""
-    from oracle import oracle as O
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import chain
-    lib = O.ref()
-    kind = "reference"
-    if lib is None:
-        lib, kind = O.orc(), "port"
-    else:
-        lib.set_threads(threads)
-    import types
-    sub = types.SimpleNamespace(**{k: getattr(S, k) for k in S.__dataclass_fields__})
-    sub.views = views_sample
-    sub.mvp = S.mvp[:views_sample].copy()
-    sub.pvinv = S.pvinv[:views_sample].copy()
-    sub.nv, sub.nt = S.nv, S.nt
-    pyr = chain.build_pyramid(sub, S.tex_init)
-    t0 = time.perf_counter()
-    chain.run_chain(lib, sub, 0, pyr=pyr, raster_lib=O.orc())
-    per_views = time.perf_counter() - t0
-    # the chain already includes one Adam step on the texture; add the mip
-    # rebuild and the remaining parameter groups
-    t1 = time.perf_counter()
-    O.orc().mip_build(S.tex_w, S.tex_h, S.C, S.levels, pyr)
-    par = time.perf_counter() - t1
-    total = per_views * (S.views / views_sample) + par
-    if lib is not O.orc():
-        lib.set_threads(1)
-    return total, kind, (f"{views_sample} of {S.views} views of one fit iteration (all per-pixel operators "
-                         f"fwd+bwd, Adam on the texture) + mip rebuild, extrapolated to {S.views} views; raster "
-                         f"stage = CPU restatement of the GL rasterizer")
+class RefStepper:
+    """The reference's own CPU implementation of the path (oracle/_ref: its
+    kernel sources compiled for the host, run with `threads` host threads;
+    the raster stage is the CPU restatement of its GL rasterizer), stepped
+    in bounded samples of one fit iteration: step s processes view s mod V
+    -- project, raster, interpolate, texture, the four shading operators,
+    antialias, MSE and every backward pass -- plus 1/V of the iteration's
+    parameter work (Adam on a 1/V slice of texture level 0; on the last
+    view also the mip gradient push-down, Adam on positions and lobes and
+    the mip rebuild).  V consecutive steps are exactly one fit iteration of
+    the workload, so iterations/s = steps / V / seconds."""
+
+    def __init__(self, S, threads):
+        from oracle import oracle as O
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import chain
+        import types
+        self.O, self.chain, self.S = O, chain, S
+        lib = O.ref()
+        self.kind = "reference"
+        if lib is None:
+            lib, self.kind = O.orc(), "port"
+            self.threads = 1
+        else:
+            lib.set_threads(threads)
+            self.threads = threads
+        self.lib = lib
+        self.views = []
+        for v in range(S.views):
+            sub = types.SimpleNamespace(**{k: getattr(S, k) for k in S.__dataclass_fields__})
+            sub.views = 1
+            sub.mvp = S.mvp[v:v + 1].copy()
+            sub.pvinv = S.pvinv[v:v + 1].copy()
+            sub.nv, sub.nt = S.nv, S.nt
+            self.views.append(sub)
+        rng = np.random.default_rng(S.seed + 11)
+        self.targets = [rng.random((S.W * S.H, S.C), dtype=np.float32) for _ in range(S.views)]
+        self.pyr = chain.build_pyramid(S, S.tex_init)
+        self.pos = S.pos.copy()
+        self.lobes = np.concatenate([S.lobe_axis_init.reshape(-1), S.lobe_sharp_init.reshape(-1),
+                                     S.lobe_amp_init.reshape(-1)]).astype(np.float32)
+        n0 = S.tex_w * S.tex_h * S.C
+        z = lambda n: np.zeros(n, np.float32)
+        self.n0 = n0
+        self.mt, self.vt = z(n0), z(n0)
+        self.mp, self.vp = z(self.pos.size), z(self.pos.size)
+        self.ml, self.vl = z(self.lobes.size), z(self.lobes.size)
+        self.s = 0
+
+    def step(self):
+        S, O, lib = self.S, self.O, self.lib
+        V, K, C = S.views, S.K, S.C
+        j = self.s % V
+        t = self.s // V + 1
+        ax = np.ascontiguousarray(self.lobes[:3 * K].reshape(K, 3))
+        sh = np.ascontiguousarray(self.lobes[3 * K:4 * K])
+        am = np.ascontiguousarray(self.lobes[4 * K:].reshape(K, C))
+        r = self.chain.run_chain(lib, self.views[j], 0, target=self.targets[j], pos=self.pos, pyr=self.pyr,
+                                 lobes=(ax, sh, am), raster_lib=O.orc(), adam_step=0)
+        g = r["g_pyr"]
+        if j == V - 1:
+            lib_m = O.orc()
+            lib_m.mip_pushdown(0, S.tex_w, S.tex_h, C, S.levels, g)
+        a, b = self.n0 * j // V, self.n0 * (j + 1) // V
+        p0 = self.pyr[a:b]
+        lib.adam(0, b - a, p0, np.ascontiguousarray(g[a:b]), self.mt[a:b], self.vt[a:b], S.lr, 0.9, 0.999, 1e-8, t)
+        if j == V - 1:
+            O.orc().clamp(self.n0, self.pyr, 0.0, 1.0)
+            O.orc().mip_build(S.tex_w, S.tex_h, C, S.levels, self.pyr)
+            pp = self.pos.reshape(-1)
+            lib.adam(0, pp.size, pp, np.ascontiguousarray(r["g_pos"].reshape(-1)), self.mp, self.vp,
+                     S.lr_pos or S.lr, 0.9, 0.999, 1e-8, t)
+            gl = np.concatenate([r["g_axis"].reshape(-1), r["g_sharp"].reshape(-1),
+                                 r["g_amp"].reshape(-1)]).astype(np.float32)
+            lib.adam(0, self.lobes.size, self.lobes, gl, self.ml, self.vl, S.lr, 0.9, 0.999, 1e-8, t)
+        self.s += 1
+
+    def close(self):
+        if self.kind == "reference":
+            self.lib.set_threads(1)
+
+    def sample(self, steps):
+        V = self.S.views
+        return (f"{steps} steps of one view each ({steps / V:g} fit iterations of {V} views): every per-pixel "
+                f"operator fwd+bwd through the reference's kernels for the host, raster by the CPU restatement "
+                f"of its GL rasterizer, 1/{V} of texture Adam per step; mip push-down/rebuild and Adam on "
+                f"positions and lobes once per {V} steps")
+
+
+def time_reference(S, threads, steps, warmup):
+    """(seconds per full fit iteration, kind, cores, sample) of the reference's
+    CPU implementation over `steps` view-steps after `warmup` view-steps."""
+    rs = RefStepper(S, threads)
+    try:
+        for _ in range(warmup):
+            rs.step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            rs.step()
+        dt = time.perf_counter() - t0
+    finally:
+        rs.close()
+    return dt * S.views / steps, dt / steps, rs.kind, rs.threads, rs.sample(steps)
 
 
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU implementation of the path,
-    all host threads, bounded per-step samples of the same workload."""
+    all host threads, on the same workload, `--warmup` + `--steps` steps of
+    one view (and 1/V of the parameter work) each."""
     S = make_scene(args)
     threads = os.cpu_count() or 1
-    steps, warm = args.steps, args.warmup
-    for _ in range(min(warm, 1)):
-        cpu_reference_iteration(S, threads)
-    times = []
-    for _ in range(max(1, min(steps, 3))):
-        t, kind, sample = cpu_reference_iteration(S, threads)
-        times.append(t)
-    per_iter = statistics.median(times)
+    per_iter, per_step, kind, cores, sample = time_reference(S, threads, args.steps, args.warmup)
     v = 1.0 / per_iter
-    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": args.gpus,
-            "steps": len(times), "warmup": min(warm, 1), "ms_per_step": per_iter * 1000, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(S), "global_batch": S.views, "seq_len": 0,
-                       "parallelism": "replicas"},
-            "cpu_baseline": {"value": v, "unit": "iters/s", "cores": threads, "kind": kind, "sample": sample},
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1000, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
+            "config": bench_config(S, world),
+            "step": f"one view of the {S.views}-view fit iteration + 1/{S.views} of its parameter work; "
+                    f"{S.views} steps = one iteration",
+            "cpu_baseline": {"value": v, "unit": "iters/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -489,10 +622,75 @@ def run_mixed(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(n):
+    """`--gpus N` outside torchrun: start the N ranks through
+    torch.distributed.run on this node and return its exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def mix_summary(args):
+    """Batched vs plain on the uneven 64-scene mix: one batched graph launch
+    per iteration of every scene against the same scenes stepped one at a
+    time through the plain pipeline (scene fit-iterations/s)."""
+    import torch
+    from vcl_b200 import capi, mixbench
+    ctx = capi.Context(int(os.environ.get("LOCAL_RANK", 0)))
+    try:
+        r = mixbench.run_mix(ctx, args.scenes, args.steps, args.warmup)
+    finally:
+        ctx.close()
+    torch.cuda.empty_cache()
+    return {"unit": "scene-iters/s", "batched": r["value"], "plain_one_at_a_time": r["plain_seq_scene_iters_per_s"],
+            "fused_one_at_a_time": r["fused_seq_scene_iters_per_s"], "ratio_vs_plain": r["speedup_vs_plain"],
+            "ratio_vs_fused_one_at_a_time": r["speedup_vs_fused_seq"], "ms_per_batched_step": r["ms_per_step"],
+            "steps": args.steps, "warmup": args.warmup, "launches_per_batched_step": r["launches_per_batched_step"],
+            "one_at_a_time_by_resolution": r["one_at_a_time_by_resolution"],
+            "first_step_ms_incl_autotune_capture": r["first_step_ms_incl_autotune_capture"],
+            "workload": r["config"]["workload"], "resident_bytes": r["config"]["resident_bytes"]}
+
+
+def serve_summary(args):
+    """The serving loop at one arrival rate, repeated: median and range of
+    p50/p99 job latency and iterations/s, beside the same jobs one at a time
+    through the plain pipeline."""
+    import torch
+    from vcl_b200 import capi, mixbench
+    ctx = capi.Context(int(os.environ.get("LOCAL_RANK", 0)))
+    try:
+        r = mixbench.run_serve(ctx, args.serve_jobs, [args.serve_lam], repeats=args.serve_repeats)
+    finally:
+        ctx.close()
+    torch.cuda.empty_cache()
+    sw = r["sweep"]
+
+    def stat(key, src=None):
+        xs = [(x[src] if src else x)[key] for x in sw]
+        xs = [x for x in xs if x is not None]
+        return {"median": statistics.median(xs), "min": min(xs), "max": max(xs)} if xs else None
+
+    return {"lambda_per_s": args.serve_lam, "jobs": r["jobs"], "repeats": len(sw),
+            "iterations_per_repeat": r["iterations_total"], "budget_gb": r["budget_gb"],
+            "p50_ms": stat("p50_ms"), "p99_ms": stat("p99_ms"), "iters_per_s": stat("iters_per_s"),
+            "completed": [x["completed"] for x in sw],
+            "plain_one_at_a_time": {"p50_ms": stat("p50_ms", "plain_one_at_a_time"),
+                                    "p99_ms": stat("p99_ms", "plain_one_at_a_time"),
+                                    "iters_per_s": stat("iters_per_s", "plain_one_at_a_time")},
+            "workload": f"{r['jobs']} fit jobs from the uneven scene mix, U[50,500] iterations each, Poisson "
+                        f"arrivals at {args.serve_lam:g} jobs/s, {r['budget_gb']:g} GB admission budget"}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl != "reference":
+        sys.exit(spawn_ranks(args.gpus))
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args, rank, world)), flush=True)
@@ -520,10 +718,8 @@ def main():
         "metric": METRIC, "value": r["value"], "unit": "iters/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": workload_name(S), "strategy": r["best"], "global_batch": S.views * world,
-                   "seq_len": 0, "parallelism": f"replicas x{world}",
-                   "adam": {"lr": S.lr, "lr_pos": S.lr_pos or S.lr, "betas": [0.9, 0.999], "eps": 1e-8},
-                   "l2": "per-step working set > 2 GB (larger than the 126 MB L2); no flush"},
+        "config": bench_config(S, world),
+        "strategy": r["best"],
         "strategies_ms_per_step": {k: v / args.steps for k, v in r["results"].items()},
         "gpu_launches": r["launches"][r["best"]] * args.steps,
         "clocks": r["clocks"],
@@ -555,19 +751,33 @@ def main():
         line["fused_kernels_frac_hbm"] = {k: round(byts[k] / (v * 1e-3) / 1e9 / hbm_peak, 3)
                                           for k, v in kms.items() if v > 0}
         # the SG kernels' own bound, the MUFU pipe: 2 rsqrt + 4 ex2 per covered
-        # pixel and lobe in each, against 16 MUFU operations per clock per SM
-        # at the SM clock sampled in the timed region (a nominal peak: no
-        # measured figure exists for this unit)
+        # pixel and lobe in each, against the MUFU rate measured by the probe
+        # on this GPU (the nominal 16 operations per clock per SM beside it)
         import torch
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
         mhz = (r["clocks"] or {}).get("sm_mhz") or 1965.0
-        sfu_peak = 16.0 * sms * mhz * 1e6
+        nominal = 16.0 * sms * mhz * 1e6
+        up = r.get("unit_peaks") or {}
+        sfu_peak = up.get("mufu_ops_per_s") or nominal
         ops = 6.0 * ncov * S.K
         line["sfu_roofline"] = {
             k: {"mufu_ops": ops, "achieved_gops": ops / (kms[k] * 1e-3) / 1e9, "peak_gops": sfu_peak / 1e9,
                 "frac": ops / (kms[k] * 1e-3) / sfu_peak, "covered_pixels": ncov,
-                "peak_source": f"nominal: 16 MUFU ops/clock/SM x {sms} SMs x {mhz:.0f} MHz"}
+                "peak_source": "measured (vcl_probe_mufu_throughput)" if "mufu_ops_per_s" in up else "nominal",
+                "nominal_gops": nominal / 1e9}
             for k in ("shade_fwd", "sg_lobes") if kms.get(k, 0) > 0}
+        if "l2_red_v4_per_s" in up and kms.get("bwd_pix", 0) > 0:
+            # the per-pixel backward's texel scatter: 4 vector reductions per
+            # covered pixel and level it samples (8 with trilinear sampling),
+            # the reference's atomics per pixel (texturemap.cu:246-279), against
+            # the measured L2 vector-reduction rate
+            reds = 8.0 * ncov
+            line["atomic_roofline"] = {
+                "bwd_pix": {"texel_reductions": reds, "achieved_per_s": reds / (kms["bwd_pix"] * 1e-3),
+                            "peak_per_s": up["l2_red_v4_per_s"],
+                            "frac": reds / (kms["bwd_pix"] * 1e-3) / up["l2_red_v4_per_s"],
+                            "peak_source": "measured (vcl_probe_red_throughput, coalesced)"}}
+        line["unit_peaks"] = up
     if "stages" in r:
         st = r["stages"]
         byts = stage_bytes(S, st["ncov"])
@@ -580,12 +790,19 @@ def main():
                                 "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
                                 "peak_source": peak_src, "algorithmic_bytes": b, "avg_ms": ms[top]}
         line["stages_ms"] = {k: round(v, 4) for k, v in ms.items()}
+        line["raster_ties"] = st.get("ties")
         line["stages_frac_hbm"] = {k: round(byts.get(k, 0) / (v * 1e-3) / 1e9 / hbm_peak, 3) for k, v in ms.items()
                                    if v > 0}
     if not args.no_cpu_baseline:
-        t, kind, sample = cpu_reference_iteration(S, os.cpu_count() or 1)
-        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "iters/s", "cores": os.cpu_count() or 1, "kind": kind,
+        # one full fit iteration of the workload (V view-steps) after one
+        # warm-up step, on every host core
+        per_iter, _, kind, cores, sample = time_reference(S, os.cpu_count() or 1, S.views, 1)
+        line["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": "iters/s", "cores": cores, "kind": kind,
                                 "sample": sample}
+    if not args.no_mix:
+        line["mix"] = mix_summary(args)
+    if not args.no_serve:
+        line["serve"] = serve_summary(args)
     print(json.dumps(line), flush=True)
 
 

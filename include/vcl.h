@@ -505,6 +505,24 @@ VCL_API vcl_status vcl_server_job_result(const vcl_server* server, long long job
 VCL_API vcl_status vcl_server_stats(const vcl_server* server, double* p50_ms, double* p99_ms, long long* iterations,
                                     int* completed, long long* ticks, size_t* resident_bytes);
 
+/* ------------------------------------------------------ throughput probes */
+/* Measurement utilities with no counterpart in the reference: they measure
+ * the peak rates of the two units other than HBM that bound the path's
+ * kernels, so that those kernels can be reported against measured peaks.
+ * Time the launch with CUDA events on `stream` and divide the count.
+ *
+ * L2 reductions: every thread adds (1,1,1,1) with red.global.add.v4.f32 to
+ * consecutive 16-byte slots of `buf` (n_floats floats, 16-byte aligned,
+ * device), `iters` passes; *reductions = the number of vector reductions
+ * issued.  Keep buf well inside L2 (e.g. 32 MB) to measure the L2 units. */
+VCL_API vcl_status vcl_probe_red_throughput(vcl_ctx* ctx, float* buf, long long n_floats, int iters,
+                                            long long* reductions, void* stream);
+/* MUFU: independent ex2.approx / rsqrt.approx chains on every SM; `out`
+ * (device) holds vcl_probe_mufu_threads(ctx) floats; *ops = the number of
+ * MUFU operations issued. */
+VCL_API long long vcl_probe_mufu_threads(const vcl_ctx* ctx);
+VCL_API vcl_status vcl_probe_mufu_throughput(vcl_ctx* ctx, float* out, int iters, long long* ops, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

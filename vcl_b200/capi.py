@@ -10,7 +10,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libvcl.so")
+# the in-tree build; VCL_LIB names another build of the same library
+LIB_PATH = os.environ.get("VCL_LIB") or os.path.join(HERE, "libvcl.so")
 
 c_int, c_ll, c_size, c_float, c_double, c_void_p, c_char_p = (
     ctypes.c_int, ctypes.c_longlong, ctypes.c_size_t, ctypes.c_float, ctypes.c_double, ctypes.c_void_p, ctypes.c_char_p)
@@ -44,6 +45,9 @@ SIGNATURES = {
     "vcl_rasterize_fwd_static": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P]),
     "vcl_rasterize_bwd": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
     "vcl_raster_ties": (c_int, [P, P, c_int, P, c_int, c_int, c_int, c_int, P, P, P, P]),
+    "vcl_probe_red_throughput": (c_int, [P, P, c_ll, c_int, ctypes.POINTER(c_ll), P]),
+    "vcl_probe_mufu_threads": (c_ll, [P]),
+    "vcl_probe_mufu_throughput": (c_int, [P, P, c_int, ctypes.POINTER(c_ll), P]),
     "vcl_interpolate_fwd": (c_int, [P, P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P]),
     "vcl_interpolate_bwd": (c_int, [P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P, P]),
     "vcl_texture_fwd": (c_int, [P, P, P, P, c_int, c_int, c_int, P, c_int, c_int, c_int, c_int, P, P]),

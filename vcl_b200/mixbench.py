@@ -99,8 +99,21 @@ def run_mix(ctx, n_scenes, steps, warmup, seed=0):
     for f in fits:
         batch.remove(f)
     batch.close()
-    fused_seq_ms, _ = seq(capi.FIT_FUSED)
+    fused_seq_ms, fused_per = seq(capi.FIT_FUSED)
     plain_seq_ms, plain_per = seq(capi.FIT_PLAIN)
+    # where the time goes: scenes grouped by resolution, one at a time
+    buckets = {}
+    for S, pm, fm in zip(S_list, plain_per, fused_per):
+        b = buckets.setdefault(f"{S.W}x{S.H}", {"scenes": 0, "pixels": 0, "triangles": 0, "plain_ms": 0.0,
+                                                 "fused_ms": 0.0})
+        b["scenes"] += 1
+        b["pixels"] += S.W * S.H * S.views
+        b["triangles"] += S.nt
+        b["plain_ms"] += pm
+        b["fused_ms"] += fm
+    for b in buckets.values():
+        b["plain_ms"] = round(b["plain_ms"], 3)
+        b["fused_ms"] = round(b["fused_ms"], 3)
     sched = {}
     for f in fits:
         f.set_strategy(capi.FIT_FUSED)
@@ -119,13 +132,14 @@ def run_mix(ctx, n_scenes, steps, warmup, seed=0):
         "gpu_launches": launches * steps, "launches_per_batched_step": launches,
         "first_step_ms_incl_autotune_capture": round(first_ms, 1),
         "raster_schedules_tile_direct_area": sched,
+        "one_at_a_time_by_resolution": dict(sorted(buckets.items(), key=lambda kv: int(kv[0].split("x")[0]))),
         "config": {"workload": f"{n} uneven scenes (icosphere 1k-200k tris, 128^2-1024^2 x 1-16 views, "
                                f"256^2-2048^2 RGBA textures, 8-32 lobes), {px / 1e6:.1f} M pixels per iteration",
                    "scenes": n, "pixels": px, "resident_bytes": resident, "seed": seed},
     }
 
 
-def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_range=(50, 500)):
+def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_range=(50, 500), repeats=1):
     import torch
     from vcl_b200 import capi, scenes
     rng = np.random.default_rng(seed + 7)
@@ -148,7 +162,7 @@ def run_serve(ctx, n_jobs, lams, budget_gb=150.0, seed=0, max_live=64, iters_ran
         f.close()
     out = {"jobs": n_jobs, "iterations_total": int(sum(iters)), "budget_gb": budget_gb, "max_live": max_live,
            "sweep": []}
-    for lam in lams:
+    for lam in [l for l in lams for _ in range(repeats)]:
         arr = np.cumsum(rng.exponential(1000.0 / lam, size=n_jobs))   # ms after start
         srv = capi.Server(ctx, int(budget_gb * 1e9), max_live=max_live)
         base = srv.now_ms()
