@@ -650,7 +650,7 @@ def mix_summary(args):
             "fused_one_at_a_time": r["fused_seq_scene_iters_per_s"], "ratio_vs_plain": r["speedup_vs_plain"],
             "ratio_vs_fused_one_at_a_time": r["speedup_vs_fused_seq"], "ms_per_batched_step": r["ms_per_step"],
             "steps": args.steps, "warmup": args.warmup, "launches_per_batched_step": r["launches_per_batched_step"],
-            "one_at_a_time_by_resolution": r["one_at_a_time_by_resolution"],
+            "one_at_a_time_by_resolution": r["one_at_a_time_by_resolution"], "subsets": r["subsets"],
             "first_step_ms_incl_autotune_capture": r["first_step_ms_incl_autotune_capture"],
             "workload": r["config"]["workload"], "resident_bytes": r["config"]["resident_bytes"]}
 

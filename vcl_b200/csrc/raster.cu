@@ -312,27 +312,55 @@ __global__ void __launch_bounds__(SETUP_THREADS, 4) k_setup(const float4* __rest
         small_pack(st[lane], r, q, t, view);
     }
     __syncwarp();
-    for (int k = lane; k < total; k += 32) {
-        int j = 0;
+    // 32 rows at a time: each lane finds its row's conservative span, then
+    // the warp walks the concatenated spans pixel by pixel (lane m takes
+    // pixels m, m + 32, ... of the concatenation), so lanes stay busy however
+    // unequal the spans are
+    for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        int j = 0, py = 0, x0 = 0, x1 = -1;
+        if (k < total) {
 #pragma unroll
-        for (int step = 16; step > 0; step >>= 1)
-            if (start[j + step] <= k) j += step;
-        const SmallTri& S = st[j];
-        RTri rr;
-        rr.a = S.a; rr.b = S.b; rr.k = S.k; rr.z = S.z; rr.w = S.w; rr.box = S.box;
-        const float4 s0 = S.s0, s1 = S.s1;
-        const int code = __float_as_int(s1.z), tj = __float_as_int(s1.w);
-        SpanEq q;
-        q.al[0] = s0.x; q.be[0] = s0.y; q.al[1] = s0.z; q.be[1] = s0.w; q.al[2] = s1.x; q.be[2] = s1.y;
-        q.side[0] = (code & 3) - 1; q.side[1] = ((code >> 2) & 3) - 1; q.side[2] = ((code >> 4) & 3) - 1;
-        const int py = rr.box.z + (k - start[j]);
-        const float sy = s_ndc[W + py];
-        int x0, x1;
-        if (!row_span(rr, q, sy, W, x0, x1)) continue;
-        unsigned long long* kv = keys + (size_t)(code >> 8) * W * H + (size_t)py * W;
-        for (int px = x0; px <= x1; ++px) {
+            for (int step = 16; step > 0; step >>= 1)
+                if (start[j + step] <= k) j += step;
+            const SmallTri& S = st[j];
+            RTri rr;
+            rr.a = S.a; rr.b = S.b; rr.k = S.k; rr.z = S.z; rr.w = S.w; rr.box = S.box;
+            const float4 s0 = S.s0, s1 = S.s1;
+            const int code = __float_as_int(s1.z);
+            SpanEq q;
+            q.al[0] = s0.x; q.be[0] = s0.y; q.al[1] = s0.z; q.be[1] = s0.w; q.al[2] = s1.x; q.be[2] = s1.y;
+            q.side[0] = (code & 3) - 1; q.side[1] = ((code >> 2) & 3) - 1; q.side[2] = ((code >> 4) & 3) - 1;
+            py = rr.box.z + (k - start[j]);
+            if (!row_span(rr, q, s_ndc[W + py], W, x0, x1)) x1 = x0 - 1;
+        }
+        const int len = x1 >= x0 ? x1 - x0 + 1 : 0;
+        int end = len;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, end, o);
+            if (lane >= o) end += y;
+        }
+        const int beg = end - len;
+        const int npx = __shfl_sync(0xffffffffu, end, 31);
+        for (int m0 = 0; m0 < npx; m0 += 32) {
+            const int m = m0 + lane;
+            // the row lane owning pixel m: the last lane whose span starts at or before m
+            int r = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int b = __shfl_sync(0xffffffffu, beg, r + step);
+                if (b <= m) r += step;
+            }
+            const int rb = __shfl_sync(0xffffffffu, beg, r), rx = __shfl_sync(0xffffffffu, x0, r);
+            const int ry = __shfl_sync(0xffffffffu, py, r), rj = __shfl_sync(0xffffffffu, j, r);
+            if (m >= npx) continue;
+            const SmallTri& S = st[rj];
+            const int px = rx + (m - rb);
+            const float4 s1 = S.s1;
+            const int code = __float_as_int(s1.z), tj = __float_as_int(s1.w);
             float zw;
-            if (pixel_test(rr.a, rr.b, rr.k, rr.z, rr.w, s_ndc[px], sy, zw)) atomicMin(&kv[px], depth_key(zw, tj));
+            if (pixel_test(S.a, S.b, S.k, S.z, S.w, s_ndc[px], s_ndc[W + ry], zw))
+                atomicMin(&keys[(size_t)(code >> 8) * W * H + (size_t)ry * W + px], depth_key(zw, tj));
         }
     }
 }
@@ -485,15 +513,34 @@ __global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, 
         unsigned long long* kv = keys + (size_t)view * W * H;
         SpanEq q;
         span_setup(r, q);
-        // lane per row; each lane walks only its row's conservative span
-        for (int py = r.box.z + lane; py <= r.box.w; py += 32) {
-            const float sy = s_ndc[W + py];
-            int x0, x1;
-            if (!row_span(r, q, sy, W, x0, x1)) continue;
-            for (int px = x0; px <= x1; ++px) {
+        // 32 rows at a time: a lane finds its row's conservative span, then
+        // the warp walks the concatenated spans pixel by pixel
+        for (int y0 = r.box.z; y0 <= r.box.w; y0 += 32) {
+            const int py = y0 + lane;
+            int x0 = 0, x1 = -1;
+            if (py <= r.box.w && !row_span(r, q, s_ndc[W + py], W, x0, x1)) x1 = x0 - 1;
+            const int len = x1 >= x0 ? x1 - x0 + 1 : 0;
+            int end = len;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, end, o);
+                if (lane >= o) end += y;
+            }
+            const int beg = end - len;
+            const int npx = __shfl_sync(0xffffffffu, end, 31);
+            for (int m0 = 0; m0 < npx; m0 += 32) {
+                const int m = m0 + lane;
+                int rl = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int b = __shfl_sync(0xffffffffu, beg, rl + step);
+                    if (b <= m) rl += step;
+                }
+                const int rb = __shfl_sync(0xffffffffu, beg, rl), rx = __shfl_sync(0xffffffffu, x0, rl);
+                if (m >= npx) continue;
+                const int px = rx + (m - rb), ry = y0 + rl;
                 float zw;
-                if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], sy, zw))
-                    atomicMin(&kv[(size_t)py * W + px], depth_key(zw, t));
+                if (pixel_test(r.a, r.b, r.k, r.z, r.w, s_ndc[px], s_ndc[W + ry], zw))
+                    atomicMin(&kv[(size_t)ry * W + px], depth_key(zw, t));
             }
         }
     }

@@ -99,6 +99,36 @@ def run_mix(ctx, n_scenes, steps, warmup, seed=0):
     for f in fits:
         batch.remove(f)
     batch.close()
+
+    # the same batched launch on the small scenes alone and on the large ones
+    # alone: where batching pays (many small launches) and where it cannot
+    # (kernels that already fill the GPU)
+    def batched_subset(sel):
+        sub = [f for f, S in zip(fits, S_list) if sel(S)]
+        if not sub:
+            return None, 0
+        b = capi.Batch(ctx)
+        for f in sub:
+            b.add(f)
+        for _ in range(max(1, warmup)):
+            b.step(sh)
+        stream.synchronize()
+        a, z = _events(torch)
+        a.record(stream)
+        for _ in range(steps):
+            b.step(sh)
+        z.record(stream)
+        stream.synchronize()
+        for f in sub:
+            b.remove(f)
+        b.close()
+        return a.elapsed_time(z) / steps, len(sub)
+
+    small = lambda S: S.W * S.H <= 256 * 256
+    subsets = {}
+    for name, sel in (("small_256_or_less", small), ("large_512_or_more", lambda S: not small(S))):
+        ms, n_sub = batched_subset(sel)
+        subsets[name] = {"scenes": n_sub, "batched_ms": ms}
     fused_seq_ms, fused_per = seq(capi.FIT_FUSED)
     plain_seq_ms, plain_per = seq(capi.FIT_PLAIN)
     # where the time goes: scenes grouped by resolution, one at a time
@@ -114,6 +144,13 @@ def run_mix(ctx, n_scenes, steps, warmup, seed=0):
     for b in buckets.values():
         b["plain_ms"] = round(b["plain_ms"], 3)
         b["fused_ms"] = round(b["fused_ms"], 3)
+    for name, sel in (("small_256_or_less", small), ("large_512_or_more", lambda S: not small(S))):
+        d = subsets[name]
+        d["plain_one_at_a_time_ms"] = sum(pm for S, pm in zip(S_list, plain_per) if sel(S))
+        d["fused_one_at_a_time_ms"] = sum(fm for S, fm in zip(S_list, fused_per) if sel(S))
+        d["pixels"] = sum(S.W * S.H * S.views for S in S_list if sel(S))
+        if d["batched_ms"]:
+            d["ratio_vs_plain"] = d["plain_one_at_a_time_ms"] / d["batched_ms"]
     sched = {}
     for f in fits:
         f.set_strategy(capi.FIT_FUSED)
@@ -132,6 +169,7 @@ def run_mix(ctx, n_scenes, steps, warmup, seed=0):
         "gpu_launches": launches * steps, "launches_per_batched_step": launches,
         "first_step_ms_incl_autotune_capture": round(first_ms, 1),
         "raster_schedules_tile_direct_area": sched,
+        "subsets": subsets,
         "one_at_a_time_by_resolution": dict(sorted(buckets.items(), key=lambda kv: int(kv[0].split("x")[0]))),
         "config": {"workload": f"{n} uneven scenes (icosphere 1k-200k tris, 128^2-1024^2 x 1-16 views, "
                                f"256^2-2048^2 RGBA textures, 8-32 lobes), {px / 1e6:.1f} M pixels per iteration",
