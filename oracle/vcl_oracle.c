@@ -60,6 +60,16 @@ static inline void add_nan_check3(float* a, f3 b) {
         if (isfinite(v.x) && isfinite(v.y) && isfinite(v.z)) { a[0] = v.x; a[1] = v.y; a[2] = v.z; }
     }
 }
+/* The same NaN/Inf-guarded adds on double accumulators (sums over pixels). */
+static inline void add_nan_check_d(double* a, double b) {
+    if (!isfinite(*a)) *a = 0.0;
+    else { double v = *a + b; if (isfinite(v)) *a = v; }
+}
+static inline void add_nan_check3_d(double* a, f3 b) {
+    if (!(isfinite(a[0]) && isfinite(a[1]) && isfinite(a[2]))) { a[0] = a[1] = a[2] = 0.0; return; }
+    double x = a[0] + b.x, y = a[1] + b.y, z = a[2] + b.z;
+    if (isfinite(x) && isfinite(y) && isfinite(z)) { a[0] = x; a[1] = y; a[2] = z; }
+}
 
 /* ------------------------------------------------------------------------ */
 /* project.cu:69-77 */
@@ -351,9 +361,7 @@ void orc_rasterize_bwd(int W, int H, int views, const float* clip, int nv,
                 int idx = f2i(r[3]) - 1;
                 if (idx < 0) continue;
                 f2 g = F2(gb[pidx * 2], gb[pidx * 2 + 1]);
-                uint32_t bits, by;
-                memcpy(&bits, &g.x, 4); memcpy(&by, &g.y, 4);
-                if (((bits | by) << 1) == 0) continue;
+                if (g.x == 0.f && g.y == 0.f) continue;   /* both zero (either sign) */
                 f2 pix = F2((float)(((double)px + 0.5) * (double)xs - 1.0), (float)(((double)py + 0.5) * (double)ys - 1.0));
                 uint32_t i0 = tri[idx * 3], i1 = tri[idx * 3 + 1], i2 = tri[idx * 3 + 2];
                 f2 p0 = F2(proj[i0 * 4], proj[i0 * 4 + 1]);
@@ -1011,6 +1019,17 @@ void orc_sg_bwd(int mode, int W, int H, int views, int C, const float* rast, int
                 float* g_axis, float* g_sharp, float* g_amp,
                 float* g_spec_axis, float* g_spec_sharp, float* g_spec_amp) {
     size_t N = (size_t)W * H * views;
+    /* The lobe gradients (and, in compat, the lobe-indexed specular sharpness
+     * gradient) are sums over every covered pixel: accumulated in double and
+     * added to the outputs once, so that the checker's value is the sum of the
+     * per-pixel terms to far below FP32 rounding however many pixels there
+     * are (a serial FP32 sum over a megapixel drifts by ~1e-5 relative).  The
+     * per-pixel terms themselves are FP32, as in the reference. */
+    double* acc = (double*)calloc((size_t)K * (C + 5), sizeof(double));
+    double* acc_amp = acc;
+    double* acc_axis = acc + (size_t)K * C;
+    double* acc_sharp = acc_axis + (size_t)K * 3;
+    double* acc_ss = acc_sharp + K;
     for (size_t pidx = 0; pidx < N; ++pidx) {
         int idx = f2i(rast[pidx * 4 + 3]) - 1;
         if (idx < 0) continue;
@@ -1052,7 +1071,7 @@ void orc_sg_bwd(int mode, int W, int H, int views, int C, const float* rast, int
                 float a = amp[i * C + k];
                 sum += g * a;
                 sumd += g * a * diffuse[pidx * C + k];
-                if (g_amp) add_nan_check(&g_amp[i * C + k], g * (dg * diffuse[pidx * C + k] + sgv));
+                if (g_amp) add_nan_check_d(&acc_amp[i * C + k], g * (dg * diffuse[pidx * C + k] + sgv));
                 if (g_diffuse) add_nan_check(&g_diffuse[pidx * C + k], g * dg * a);
                 if (g_spec_amp) {
                     if (mode == 0) add_nan_check(&g_spec_amp[pidx * C + k], g * sgv * a);
@@ -1062,13 +1081,24 @@ void orc_sg_bwd(int mode, int W, int H, int views, int C, const float* rast, int
             if (g_spec_amp && mode != 0) add_nan_check(&g_spec_amp[pidx], sum_exact_sa);
             if (g_axis) {
                 f3 t = add3(mul3s(mul3s(ddg, sumd), DIFF_AMP), mul3s(mul3s(dsg, sum), sa));
-                add_nan_check3(&g_axis[i * 3], mul3s(t, gs));
+                add_nan_check3_d(&acc_axis[i * 3], mul3s(t, gs));
             }
-            if (g_sharp) add_nan_check(&g_sharp[i], sumd * ddgs * DIFF_AMP + sum * dsgs * sa);
+            if (g_sharp) add_nan_check_d(&acc_sharp[i], sumd * ddgs * DIFF_AMP + sum * dsgs * sa);
             if (g_spec_axis) add_nan_check3(&g_spec_axis[pidx * 3], mul3s(mul3s(mul3s(dsg, sum), sa), ss));
-            if (g_spec_sharp) add_nan_check(&g_spec_sharp[mode == 0 ? (size_t)i : pidx], sum * dsgss * sa);
+            if (g_spec_sharp) {
+                if (mode == 0) add_nan_check_d(&acc_ss[i], sum * dsgss * sa);
+                else add_nan_check(&g_spec_sharp[pidx], sum * dsgss * sa);
+            }
         }
     }
+    for (int i = 0; i < K; ++i) {
+        for (int k = 0; k < C; ++k)
+            if (g_amp) add_nan_check(&g_amp[i * C + k], (float)acc_amp[i * C + k]);
+        if (g_axis) add_nan_check3(&g_axis[i * 3], F3((float)acc_axis[i * 3], (float)acc_axis[i * 3 + 1], (float)acc_axis[i * 3 + 2]));
+        if (g_sharp) add_nan_check(&g_sharp[i], (float)acc_sharp[i]);
+        if (g_spec_sharp && mode == 0) add_nan_check(&g_spec_sharp[i], (float)acc_ss[i]);
+    }
+    free(acc);
 }
 
 /* ------------------------------------------------------------------------ */

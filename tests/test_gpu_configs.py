@@ -116,7 +116,8 @@ def test_config_chain_matches_oracle(ctx, name, mode):
     assert np.array_equal(g["rast"][:, 3], o["rast"][:, 3]), "triangle ids differ"
     assert np.array_equal(g["rast"], o["rast"]), "barycentrics/depth differ"
     assert np.array_equal(g["db"], o["db"]), "DB differs"
-    res, bad = parity.check_keys(g, o, KEYS, f"{name}:mode{mode}")
+    exact = chain.run_isolated64(S, o, mode)
+    res, bad = parity.check_keys(g, o, exact, KEYS, f"{name}:mode{mode}")
     assert not bad, bad
     n = S.W * S.H * S.views * S.C
     exact_loss = O.orc().mse(1, n, o["aa"], o["target"], np.zeros(n, np.float32))
@@ -167,7 +168,22 @@ def test_config_fit_matches_oracle(ctx, name, mode, strategy, steps):
     parity.report(f"{name}:fit:mode{mode}:strategy{strategy}", {"loss": (float(rel.max()), float(rel.max()), -1)})
     assert rel.max() <= 1e-5, (losses, ref["losses"])
     lr_pos = S.lr_pos or S.lr
-    for pname, got, want, lr in (("tex", tex, ref["tex"], S.lr), ("pos", pos, ref["pos"], lr_pos),
+    # texels whose gradient is at the rounding-noise level of its sum (a
+    # 4096^2 texture seen at 512^2: almost every texel's gradient comes from
+    # the mip push-down of coarse-level sums) take Adam steps of +-lr in
+    # whichever direction their noise points, so the texture is compared
+    # where its gradient was resolved in every step: above 1e-4 of that
+    # step's largest magnitude (every texel still within the step budget)
+    resolved = ref["g_tex_resolved"] > 1e-4
+    dt = np.abs(np.asarray(tex, np.float64) - ref["tex"]).reshape(-1)
+    assert dt.max() <= 2.0 * S.lr * steps, dt.max()
+    parity.report(f"{name}:fit:mode{mode}:strategy{strategy}:tex",
+                  {"texels_differing": (float(np.mean(dt > 1e-5)), 0.0, -1),
+                   "resolved_texels": (float(resolved.mean()), 0.0, -1),
+                   "resolved_differing": (float(np.mean(dt[resolved.reshape(-1)] > 1e-5)), 0.0, -1)})
+    _adam_close(np.asarray(tex).reshape(-1)[resolved.reshape(-1)], ref["tex"].reshape(-1)[resolved.reshape(-1)],
+                S.lr, steps, "tex")
+    for pname, got, want, lr in (("pos", pos, ref["pos"], lr_pos),
                                  ("axis", ax, ref["axis"], S.lr), ("sharp", sh, ref["sharp"], S.lr),
                                  ("amp", am, ref["amp"], S.lr)):
         _adam_close(got, want, lr, steps, pname)

@@ -266,47 +266,9 @@ DEV void pix_sample(const ShadeIn& a, const TexDesc& td, const float4* __restric
     S.ok = true;
 }
 
-// One row of a pixel's bilinear texel cell at one level (texturemap.cu:
-// 246-279: the cell's four texels each take weight x gradient), combined
-// across the warp before the vector reductions.  The 32 lanes are 32
-// consecutive pixels of an image row, so their cells overlap: lanes of a run
-// with the same (level, texel row, left column) sum their left and right
-// texel values (warp_run_sum), and a run whose right texel is the next run's
-// left texel hands it over, so each texel of the row gets at most one
-// reduction per warp.  All 32 lanes call it; `ok` false adds nothing.
-DEV void tex_row_add(const TexDesc& td, float* __restrict__ g_pyr, bool ok, int level, int v, int u0, int u1,
-                     float wrow, float fx, float4 g) {
-    const int lane = threadIdx.x & 31;
-    const float wl = ok ? wrow * (1.f - fx) : 0.f, wr = ok ? wrow * fx : 0.f;
-    float x[8] = {wl * g.x, wl * g.y, wl * g.z, wl * g.w, wr * g.x, wr * g.y, wr * g.z, wr * g.w};
-    if (!ok) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) x[k] = 0.f;
-        u0 = u1 = v = level = 0;
-    } else if (u1 == u0) {           // a clamped cell: both columns are one texel
-#pragma unroll
-        for (int k = 0; k < 4; ++k) { x[k] += x[k + 4]; x[k + 4] = 0.f; }
-    }
-    const int key = ok ? u0 : -1 - lane;
-    const int row = ok ? (level << 16) | v : -1;
-    const bool live = warp_run_sum(x, key, row) && ok;
-    const unsigned tails = __ballot_sync(0xffffffffu, live);
-    const unsigned below = tails & ((1u << lane) - 1u);
-    const int prev = below ? 31 - __clz(below) : lane;
-    const float r0 = __shfl_sync(0xffffffffu, x[4], prev), r1 = __shfl_sync(0xffffffffu, x[5], prev);
-    const float r2 = __shfl_sync(0xffffffffu, x[6], prev), r3 = __shfl_sync(0xffffffffu, x[7], prev);
-    const int pu0 = __shfl_sync(0xffffffffu, u0, prev), pu1 = __shfl_sync(0xffffffffu, u1, prev);
-    const int prow = __shfl_sync(0xffffffffu, row, prev);
-    // the previous run's right texel is this run's left one
-    const bool take = live && below != 0u && prow == row && pu1 == u0 && pu1 != pu0;
-    const unsigned takers = __ballot_sync(0xffffffffu, take);
-    const unsigned above = tails & ~((2u << lane) - 1u);
-    const bool given = above != 0u && ((takers >> (__ffs(above) - 1)) & 1u);
-    if (!live) return;
-    if (take) { x[0] += r0; x[1] += r1; x[2] += r2; x[3] += r3; }
-    float* rowp = g_pyr + td.off[level] + 4 * ((size_t)v * (td.tw >> level));
-    red_add4(rowp + 4 * (size_t)u0, x[0], x[1], x[2], x[3]);
-    if (!given && u1 != u0) red_add4(rowp + 4 * (size_t)u1, x[4], x[5], x[6], x[7]);
+// One texel's share of a pixel's texture gradient (texturemap.cu:229-284).
+DEV void tex_add(const TexDesc& td, float* __restrict__ g_pyr, int level, int x, int y, float wt, float4 g) {
+    red_add4(g_pyr + td.off[level] + 4 * ((size_t)y * (td.tw >> level) + x), wt * g.x, wt * g.y, wt * g.z, wt * g.w);
 }
 
 // Geometry part: d colour / d uv from the texel values, back to the
@@ -383,7 +345,7 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // triangle no longer collide on the same three addresses.  Held to 40
 // registers so that its blocks fit on the SMs beside the lobe-gradient
 // blocks it runs with.
-__global__ void __launch_bounds__(256, 4) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+__global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
                                                  int want_tex, int want_geom) {
@@ -392,13 +354,21 @@ __global__ void __launch_bounds__(256, 4) k_bwd_pix(ShadeIn a, TexDesc td, const
     PixSample S;
     S.ok = false;
     if (p < a.npix) pix_sample(a, td, g_color, diffenv, p, S);
-    if (want_tex) {     // uniform: every lane of the warp takes part in the combining
+    if (want_tex && S.ok) {
         const float wl0 = td.L > 1 ? 1.f - S.fl : 1.f;
-        tex_row_add(td, g_pyr, S.ok, S.l0, S.v0, S.u0, S.u1, wl0 * (1.f - S.f0.y), S.f0.x, S.g);
-        tex_row_add(td, g_pyr, S.ok, S.l0, S.v1, S.u0, S.u1, wl0 * S.f0.y, S.f0.x, S.g);
-        const bool tri = S.ok && S.tri;
-        tex_row_add(td, g_pyr, tri, S.l1, S.t0, S.s0, S.s1, S.fl * (1.f - S.f1.y), S.f1.x, S.g);
-        tex_row_add(td, g_pyr, tri, S.l1, S.t1, S.s0, S.s1, S.fl * S.f1.y, S.f1.x, S.g);
+        const float2 f0 = S.f0;
+        tex_add(td, g_pyr, S.l0, S.u0, S.v0, wl0 * (1.f - f0.x) * (1.f - f0.y), S.g);
+        tex_add(td, g_pyr, S.l0, S.u1, S.v0, wl0 * f0.x * (1.f - f0.y), S.g);
+        tex_add(td, g_pyr, S.l0, S.u0, S.v1, wl0 * (1.f - f0.x) * f0.y, S.g);
+        tex_add(td, g_pyr, S.l0, S.u1, S.v1, wl0 * f0.x * f0.y, S.g);
+        if (S.tri) {
+            const float fl = S.fl;
+            const float2 f1 = S.f1;
+            tex_add(td, g_pyr, S.l1, S.s0, S.t0, fl * (1.f - f1.x) * (1.f - f1.y), S.g);
+            tex_add(td, g_pyr, S.l1, S.s1, S.t0, fl * f1.x * (1.f - f1.y), S.g);
+            tex_add(td, g_pyr, S.l1, S.s0, S.t1, fl * (1.f - f1.x) * f1.y, S.g);
+            tex_add(td, g_pyr, S.l1, S.s1, S.t1, fl * f1.x * f1.y, S.g);
+        }
     }
     if (!want_geom) return;
     const long long hw = (long long)a.W * a.H;

@@ -389,29 +389,21 @@ struct AAPair {
     AATri t;
 };
 
-// tr, to: (z/w, id + 1) of pixel q and of its pair partner (q - 1 or q - W).
-DEV bool aa_pair_zw(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv,
-                    const uint32_t* __restrict__ tri, int nt, float2 tr, float2 to, long long q, int qx, int qy, int W,
-                    int dir, bool typo, float2 s, AAPair& P, int* flags, bool need_ndc) {
+DEV bool aa_pair(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv, const uint32_t* __restrict__ tri, int nt,
+                 const float4* __restrict__ rast, long long q, int qx, int qy, int W, int dir, bool typo, float2 s,
+                 AAPair& P, int* flags, bool need_ndc) {
     const long long oidx = dir == 0 ? q - 1 : q - W;
-    if (to.y == tr.y) return false;
-    long long pp = (int)tr.y ? q : oidx;
-    long long op = (int)((dir == 0 && typo) ? tr.y : to.y) ? q : oidx;
-    if (pp == op) { if (tr.x > to.x) op = oidx; else pp = oidx; }
+    const float4 tr = rast[q], to = rast[oidx];
+    if (to.w == tr.w) return false;
+    long long pp = (int)tr.w ? q : oidx;
+    long long op = (int)((dir == 0 && typo) ? tr.w : to.w) ? q : oidx;
+    if (pp == op) { if (tr.z > to.z) op = oidx; else pp = oidx; }
     float2 f;
     if (dir == 0) { f = make_float2((float)qx + (pp > op ? .5f : -.5f), (float)qy + .5f); P.o = make_float2(pp > op ? -1.f : 1.f, 0.f); }
     else { f = make_float2((float)qx + .5f, (float)qy + (pp > op ? .5f : -.5f)); P.o = make_float2(0.f, pp > op ? -1.f : 1.f); }
     P.pp = pp;
     P.op = op;
-    return aa_fetch(proj, scr, nv, tri, nt, pp == q ? tr.y : to.y, s, f, P.t, flags, need_ndc);
-}
-
-DEV bool aa_pair(const float4* __restrict__ proj, const float4* __restrict__ scr, int nv, const uint32_t* __restrict__ tri, int nt,
-                 const float4* __restrict__ rast, long long q, int qx, int qy, int W, int dir, bool typo, float2 s,
-                 AAPair& P, int* flags, bool need_ndc) {
-    const float4 tr = rast[q], to = rast[dir == 0 ? q - 1 : q - W];
-    return aa_pair_zw(proj, scr, nv, tri, nt, make_float2(tr.z, tr.w), make_float2(to.z, to.w), q, qx, qy, W, dir,
-                      typo, s, P, flags, need_ndc);
+    return aa_fetch(proj, scr, nv, tri, nt, pp == q ? tr.w : to.w, s, f, P.t, flags, need_ndc);
 }
 
 // Forward antialias as a gather: each pixel evaluates the (up to four)
@@ -579,36 +571,12 @@ DEV void aat_pair_coords(int i, int x0, int y0, int& dir, int& qx, int& qy, bool
     }
 }
 
-// (z/w, id + 1) of the tile's pixels and its halo -- columns x0-1 .. x0+32,
-// rows y0-1 .. y0+8, every pixel any of the tile's pairs reads -- staged in
-// shared memory once (pixels outside the image hold zeros and are never
-// read).
-constexpr int AAT_SW = AAT_X + 2, AAT_SH = AAT_Y + 2;
-
-DEV void aat_stage(const float4* __restrict__ rast, long long vb, int W, int H, int x0, int y0, float2* s_zw) {
-    for (int i = threadIdx.x; i < AAT_SW * AAT_SH; i += blockDim.x) {
-        const int r = i / AAT_SW, c = i - r * AAT_SW;
-        const int x = x0 - 1 + c, y = y0 - 1 + r;
-        float2 v = make_float2(0.f, 0.f);
-        if (x >= 0 && x < W && y >= 0 && y < H) {
-            const float4 t = rast[vb + (long long)y * W + x];
-            v = make_float2(t.z, t.w);
-        }
-        s_zw[i] = v;
-    }
-}
-DEV float2 aat_zw(const float2* s_zw, int x0, int y0, int x, int y) {
-    return s_zw[(y - y0 + 1) * AAT_SW + (x - x0 + 1)];
-}
-
 // Lists the tile's pairs whose two pixels hold different triangle ids (the
 // only pairs with edge terms) in s_list and zeroes every pair's terms; the
-// pairs are then evaluated from the list with full warps.  Stages the tile's
-// (z/w, id + 1) first.  Returns the count.
+// pairs are then evaluated from the list with full warps.  Returns the count.
 DEV int aat_candidates(const float4* __restrict__ rast, long long vb, int W, int H, int x0, int y0, float4* s_lo,
-                       float4* s_hi, int* s_list, int* s_n, float2* s_zw) {
+                       float4* s_hi, int* s_list, int* s_n) {
     if (threadIdx.x == 0) *s_n = 0;
-    aat_stage(rast, vb, W, H, x0, y0, s_zw);
     __syncthreads();
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int base = 0; base < AAT_NP; base += blockDim.x) {
@@ -618,8 +586,10 @@ DEV int aat_candidates(const float4* __restrict__ rast, long long vb, int W, int
             int dir, qx, qy;
             bool own;
             aat_pair_coords(i, x0, y0, dir, qx, qy, own);
-            if (qx < W && qy < H && (dir == 0 ? qx > 0 : qy > 0))
-                cand = aat_zw(s_zw, x0, y0, qx, qy).y != aat_zw(s_zw, x0, y0, dir == 0 ? qx - 1 : qx, dir == 0 ? qy : qy - 1).y;
+            if (qx < W && qy < H && (dir == 0 ? qx > 0 : qy > 0)) {
+                const long long q = vb + (long long)qy * W + qx;
+                cand = rast[q].w != rast[dir == 0 ? q - 1 : q - W].w;
+            }
             s_lo[i] = z;
             s_hi[i] = z;
         }
@@ -662,14 +632,13 @@ __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict
                                                      MseOut mse) {
     __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
     __shared__ int s_list[AAT_NP], s_n;
-    __shared__ float2 s_zw[AAT_SW * AAT_SH];
     const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
     const long long vb = (long long)view * W * H;
     const float4* proj = clip + (size_t)view * nv;
     const float4* scr = scr_all ? scr_all + 2 * (size_t)view * nv : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n, s_zw);
+    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
     for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
         const int i = s_list[k];
         int dir, qx, qy;
@@ -678,9 +647,7 @@ __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict
         float4 lo = z, hi = z;
         AAPair P;
         const long long q = vb + (long long)qy * W + qx;
-        const float2 tq = aat_zw(s_zw, x0, y0, qx, qy);
-        const float2 to = aat_zw(s_zw, x0, y0, dir == 0 ? qx - 1 : qx, dir == 0 ? qy : qy - 1);
-        if (aa_pair_zw(proj, scr, nv, tri, nt, tq, to, q, qx, qy, W, dir, false, s, P, flags, false)) {
+        if (aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, false, s, P, flags, false)) {
 #pragma unroll
             for (int e = 0; e < 3; ++e) {
                 float a, alpha, ia, n;
@@ -736,7 +703,6 @@ __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict
                                                      int* flags) {
     __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
     __shared__ int s_list[AAT_NP], s_n;
-    __shared__ float2 s_zw[AAT_SW * AAT_SH];
     const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
     const long long vb = (long long)view * W * H;
     const float4* proj = clip + (size_t)view * nv;
@@ -744,7 +710,7 @@ __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict
     float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n, s_zw);
+    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
     for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
         const int i = s_list[k];
         int dir, qx, qy;
@@ -756,9 +722,7 @@ __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict
         const long long q = vb + (long long)qy * W + qx;
         // the reference's horizontal typo can give pp == op: its two colour
         // terms cancel and the clip term is zero (antialias.cu:279, :216-223)
-        const float2 tq = aat_zw(s_zw, x0, y0, qx, qy);
-        const float2 to = aat_zw(s_zw, x0, y0, dir == 0 ? qx - 1 : qx, dir == 0 ? qy : qy - 1);
-        if (aa_pair_zw(proj, scr, nv, tri, nt, tq, to, q, qx, qy, W, dir, !exact, s, P, flags, exact && own) &&
+        if (aa_pair(proj, scr, nv, tri, nt, rast, q, qx, qy, W, dir, !exact, s, P, flags, exact && own) &&
             P.pp != P.op) {
 #pragma unroll
             for (int e = 0; e < 3; ++e) {
