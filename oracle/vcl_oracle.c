@@ -114,7 +114,8 @@ void orc_project_bwd(int nv, const float* m, const float* g_out, int dim, float*
  *   u = A0/D, v = A1/D, zw = ((A0*z0 + A1*z1) + A2*z2) / ((A0*w0 + A1*w1) + A2*w2)
  *   near/far clip: -1 <= zw <= 1; depth test zw < depth (cleared to 1.0),
  *   equal depth keeps the lower triangle id (first drawn wins under GL_LESS);
- *   only pixels inside raster_bbox() are tested.
+ *   only pixels inside raster_bbox() are tested (half a pixel around the
+ *   projected vertex extent).
  * Depth is compared in FP32, not a 24-bit depth buffer.
  */
 typedef struct {
@@ -175,24 +176,31 @@ static inline int edge_in(float A, float a, float b, float sigma) {
     return gx > 0.f || (gx == 0.f && gy < 0.f);
 }
 
-/* Conservative pixel bounding box of a triangle, part of the restated
- * semantics (the CUDA binner uses the same float operations): when all
- * w > 0 it is the box of the projected vertices widened by one pixel,
- * otherwise the whole view.  Returns 0 when the box is empty. */
+/* Pixel bounding box of a triangle, part of the restated semantics (the CUDA
+ * rasterizer computes the same box with the same float operations): when all
+ * w > 0, the pixel centres within half a pixel of the projected vertices'
+ * extent (x/w taken as x * (1/w), both rounded), otherwise the whole view.
+ * A centre outside the vertex extent lies outside the triangle, so GL never
+ * draws it; the margin covers the rounding of the extent.  The FP32 edge
+ * functions of a nearly edge-on triangle can accept centres further out than
+ * that (their rounding error is large next to such a triangle's tiny
+ * determinant), and the box is what excludes them.  Returns 0 when empty. */
 static int raster_bbox(const float* c0, const float* c1, const float* c2, int W, int H, int* x0, int* x1, int* y0, int* y1) {
     float w0 = c0[3], w1 = c1[3], w2 = c2[3];
     if (w0 > 0.f && w1 > 0.f && w2 > 0.f) {
-        float X0 = c0[0] / w0, X1 = c1[0] / w1, X2 = c2[0] / w2;
-        float Y0 = c0[1] / w0, Y1 = c1[1] / w1, Y2 = c2[1] / w2;
+        float iw0 = 1.f / w0, iw1 = 1.f / w1, iw2 = 1.f / w2;
+        float X0 = c0[0] * iw0, X1 = c1[0] * iw1, X2 = c2[0] * iw2;
+        float Y0 = c0[1] * iw0, Y1 = c1[1] * iw1, Y2 = c2[1] * iw2;
         float xmn = fminf(fminf(X0, X1), X2), xmx = fmaxf(fmaxf(X0, X1), X2);
         float ymn = fminf(fminf(Y0, Y1), Y2), ymx = fmaxf(fmaxf(Y0, Y1), Y2);
-        float fx0 = (xmn + 1.f) * (0.5f * (float)W) - 0.5f, fx1 = (xmx + 1.f) * (0.5f * (float)W) - 0.5f;
-        float fy0 = (ymn + 1.f) * (0.5f * (float)H) - 0.5f, fy1 = (ymx + 1.f) * (0.5f * (float)H) - 0.5f;
+        float hw = 0.5f * (float)W, hh = 0.5f * (float)H;
+        float fx0 = (xmn + 1.f) * hw - 0.5f, fx1 = (xmx + 1.f) * hw - 0.5f;
+        float fy0 = (ymn + 1.f) * hh - 0.5f, fy1 = (ymx + 1.f) * hh - 0.5f;
         fx0 = fmaxf(fminf(fx0, (float)W), -2.f); fx1 = fmaxf(fminf(fx1, (float)W), -2.f);
         fy0 = fmaxf(fminf(fy0, (float)H), -2.f); fy1 = fmaxf(fminf(fy1, (float)H), -2.f);
         if (!(fx0 == fx0 && fx1 == fx1 && fy0 == fy0 && fy1 == fy1)) { *x0 = 0; *x1 = W - 1; *y0 = 0; *y1 = H - 1; return 1; }
-        int ix0 = (int)floorf(fx0) - 1, ix1 = (int)ceilf(fx1) + 1;
-        int iy0 = (int)floorf(fy0) - 1, iy1 = (int)ceilf(fy1) + 1;
+        int ix0 = (int)ceilf(fx0 - 0.5f), ix1 = (int)floorf(fx1 + 0.5f);
+        int iy0 = (int)ceilf(fy0 - 0.5f), iy1 = (int)floorf(fy1 + 0.5f);
         *x0 = ix0 < 0 ? 0 : ix0; *x1 = ix1 > W - 1 ? W - 1 : ix1;
         *y0 = iy0 < 0 ? 0 : iy0; *y1 = iy1 > H - 1 ? H - 1 : iy1;
         return *x0 <= *x1 && *y0 <= *y1;

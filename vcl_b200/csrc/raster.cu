@@ -198,13 +198,13 @@ DEV void setup_tri(float4 c0, float4 c1, float4 c2, int W, int H, RTri& t, bool&
     bool o2 = y0 > w0 && y1 > w1 && y2 > w2, o3 = y0 < -w0 && y1 < -w1 && y2 < -w2;
     bool o4 = c0.z > w0 && c1.z > w1 && c2.z > w2, o5 = c0.z < -w0 && c1.z < -w1 && c2.z < -w2;
     if (o0 || o1 || o2 || o3 || o4 || o5) valid = false;
-    // conservative pixel box: the pixel centres within half a pixel of the
-    // projected vertices' extent.  A centre the exact test accepts lies
-    // inside the projected triangle up to the rounding of the edge functions
-    // (~1e-4 px), and the extent below is off by a few ulps of x/w, so the
-    // half-pixel margin keeps every accepted pixel in the box (the CPU
-    // restatement's raster_bbox keeps one pixel each way; both boxes hold the
-    // same accepted pixels).
+    // pixel box: the pixel centres within half a pixel of the projected
+    // vertices' extent, the same float operations as the CPU restatement's
+    // raster_bbox.  A centre outside the vertex extent lies outside the
+    // triangle (GL never draws it); the FP32 edge functions of a nearly
+    // edge-on triangle can accept centres further out than that, and the box
+    // is part of the rule that excludes them, so both sides must use this
+    // one box.
     int bx0 = 0, bx1 = W - 1, by0 = 0, by1 = H - 1;
     if (w0 > 0.f && w1 > 0.f && w2 > 0.f) {
         const float iw0 = __frcp_rn(w0), iw1 = __frcp_rn(w1), iw2 = __frcp_rn(w2);
