@@ -51,7 +51,6 @@ struct Fused {
     cudaStream_t side = nullptr;               // lobe-gradient branch
     float tune_ms[3] = {0.f, 0.f, 0.f};        // best raster time per tile size 8/16/32
     cudaEvent_t fork = nullptr, join = nullptr;
-    cudaEvent_t claims_ready = nullptr;        // the lobe chunk counters are cleared
 };
 
 DEV float mulr(float a, float b) { return __fmul_rn(a, b); }
@@ -400,15 +399,10 @@ __global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const
 // one is consumed (its pixel indices one chunk earlier still).  At most 112
 // registers: three blocks of this kernel and two of the per-pixel backward
 // fit on an SM together.  C = 4.
-// With `claims` set, warps claim chunks from claims[blockIdx.y] (cleared
-// before the launch) instead of striding over them, so that a second launch
-// of this kernel on the SMs the per-pixel backward leaves free when it ends
-// takes over the remaining chunks.
-constexpr int LOBE_CLAIM0 = 16, LOBE_CLAIM_GROUPS = 48;   // d_step[16 ..]: chunk counters per lobe group
 template <bool EXACT>
 __global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
                                                      float* __restrict__ g_axis, float* __restrict__ g_sharp,
-                                                     float* __restrict__ g_amp, int* __restrict__ claims) {
+                                                     float* __restrict__ g_amp) {
     __shared__ float s_acc[32 * 8];                                  // [lobe][axis xyz, sharpness, amplitude 4]
     __shared__ SPair s_pix[4 * 16];
     const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -423,34 +417,24 @@ __global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n = *rec.count;
     const int nchunks = (n + 31) >> 5, stride = gridDim.x * nwarps;
-    int* claim = claims ? claims + blockIdx.y : nullptr;
-    // the warp's current chunk and the two after it (claimed or strided)
-    auto next = [&](int prev) -> int {
-        if (!claim) return prev + stride;
-        int v = 0;
-        if (lane == 0) v = atomicAdd(claim, 1);
-        return __shfl_sync(0xffffffffu, v, 0);
-    };
-    int c = claim ? next(0) : blockIdx.x * nwarps + wid;
-    int c1 = c < nchunks ? next(c) : nchunks;
-    int c2 = c1 < nchunks ? next(c1) : nchunks;
+    int c = blockIdx.x * nwarps + wid;
     float4 ra = z4, rb = z4, rc = z4, rg = z4;
     uint32_t pnext = 0;
     if (c < nchunks && c * 32 + lane < n) {
         const int k = c * 32 + lane;
         ra = rec.nss[k]; rb = rec.psa[k]; rc = rec.dfs[k]; rg = g_color[rec.pix[k]];
     }
-    if (c1 < nchunks && c1 * 32 + lane < n) pnext = rec.pix[c1 * 32 + lane];
-    for (; c < nchunks; c = c1, c1 = c2, c2 = c2 < nchunks ? next(c2) : nchunks) {
+    if (c + stride < nchunks && (c + stride) * 32 + lane < n) pnext = rec.pix[(c + stride) * 32 + lane];
+    for (; c < nchunks; c += stride) {
         const int m = min(32, n - c * 32);
         if (lane < m) spair_put(st + (lane >> 1), lane & 1, ra, rb, rc, rg);
         if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
-        if (c1 < nchunks) {
-            const int k1 = c1 * 32 + lane;
+        if (c + stride < nchunks) {
+            const int k1 = (c + stride) * 32 + lane;
             if (k1 < n) { ra = rec.nss[k1]; rb = rec.psa[k1]; rc = rec.dfs[k1]; rg = g_color[pnext]; }
         }
-        if (c2 < nchunks) {
-            const int k2 = c2 * 32 + lane;
+        if (c + 2 * stride < nchunks) {
+            const int k2 = (c + 2 * stride) * 32 + lane;
             if (k2 < n) pnext = rec.pix[k2];
         }
         __syncwarp();
@@ -609,7 +593,7 @@ vcl_status fused_init(vcl_fit* f) {
                 "fused strategy: shading record area too small (internal layout error)");
     Fused* F = new Fused();
     cudaStream_t as = ctx->aux;
-    cudaError_t e = cudaMallocAsync(&F->d_step, sizeof(int) * (LOBE_CLAIM0 + LOBE_CLAIM_GROUPS), as);
+    cudaError_t e = cudaMallocAsync(&F->d_step, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->d_corr, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->flags, 64, as);
     if (e == cudaSuccess) e = cudaMallocAsync(&F->scr, sizeof(float) * 8 * (size_t)d.views * d.nv, as);
@@ -630,7 +614,6 @@ vcl_status fused_init(vcl_fit* f) {
     e = cudaStreamCreateWithFlags(&F->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F->join, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&F->claims_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) return vcl_cuda_check(ctx, e, "fused streams");
     size_t sf = shade_smem(d.K);
     if (sf > 48 * 1024) cudaFuncSetAttribute(k_shade_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf);
@@ -845,18 +828,11 @@ vcl_status stage_aa_mse(vcl_fit* f, cudaStream_t s) {
                             f->target, f->g_aa, F->d_corr + 2, reinterpret_cast<unsigned*>(F->d_corr + 3), f->loss, s);
 }
 
-// The lobe gradients.  `ready` (optional) is recorded once the chunk
-// counters are cleared, for a tail launch (stage_lobes_tail) on another
-// stream to wait on.
-vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s, cudaEvent_t ready = nullptr) {
+vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
     vcl_ctx* ctx = f->ctx;
     const vcl_fit_desc& d = f->d;
     const long long N = a.npix;
     const int groups = (d.K + 31) / 32;
-    Fused* F = (Fused*)f->fused;
-    int* claims = groups <= LOBE_CLAIM_GROUPS ? F->d_step + LOBE_CLAIM0 : nullptr;
-    if (claims) TRY(vcl_cuda_check(ctx, cudaMemsetAsync(claims, 0, sizeof(int) * groups, s), "lobe claims"));
-    if (ready) TRY(vcl_cuda_check(ctx, cudaEventRecord(ready, s), "lobe claims"));
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
     // three lobe blocks per SM (over all lobe groups) leave registers for two
@@ -866,30 +842,9 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     const dim3 grid((unsigned)(want < capg ? (want < 1 ? 1 : want) : capg), (unsigned)groups);
     const float4* gc = (const float4*)f->g_color;
     const ShadeRec rec = shade_rec(f, true);
-    if (ctx->mode == VCL_MODE_COMPAT)
-        k_sg_lobes<false><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp, claims);
-    else k_sg_lobes<true><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp, claims);
+    if (ctx->mode == VCL_MODE_COMPAT) k_sg_lobes<false><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp);
+    else k_sg_lobes<true><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp);
     return vcl_launch_check(ctx, "fused lobe gradients");
-}
-
-// A second launch of the lobe gradients, queued on the main stream behind
-// the per-pixel backward: once that kernel's blocks leave the SMs, one more
-// lobe block per SM takes chunks from the same counters.
-vcl_status stage_lobes_tail(vcl_fit* f, const ShadeIn& a, cudaStream_t s, cudaEvent_t ready) {
-    vcl_ctx* ctx = f->ctx;
-    const vcl_fit_desc& d = f->d;
-    const int groups = (d.K + 31) / 32;
-    if (groups > LOBE_CLAIM_GROUPS) return VCL_OK;
-    Fused* F = (Fused*)f->fused;
-    TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, ready, 0), "lobe tail"));
-    const dim3 grid((unsigned)((ctx->sm_count + groups - 1) / groups), (unsigned)groups);
-    const float4* gc = (const float4*)f->g_color;
-    const ShadeRec rec = shade_rec(f, true);
-    int* claims = F->d_step + LOBE_CLAIM0;
-    if (ctx->mode == VCL_MODE_COMPAT)
-        k_sg_lobes<false><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp, claims);
-    else k_sg_lobes<true><<<grid, 128, 0, s>>>(a, rec, gc, f->g_axis, f->g_sharp, f->g_amp, claims);
-    return vcl_launch_check(ctx, "fused lobe gradients (tail)");
 }
 
 vcl_status stage_bwd_pix(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
@@ -924,7 +879,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     if (lobes) {
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->fork, s), "fork"));
         TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(F->side, F->fork, 0), "fork"));
-        TRY(stage_lobes(f, a, td, F->side, F->claims_ready));
+        TRY(stage_lobes(f, a, td, F->side));
         TRY(vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join"));
     }
     if (d.learn_tex || d.learn_pos) TRY(stage_bwd_pix(f, a, td, s));
@@ -954,8 +909,6 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
         }
         TRY(vcl_launch_check(ctx, "fused mips"));
     }
-    // what remains of the lobe chunks once the work above has left the SMs
-    if (lobes) TRY(stage_lobes_tail(f, a, s, F->claims_ready));
     if (lobes) TRY(vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join"));
     long long np = d.learn_pos ? (long long)d.nv * 3 : 0;
     long long nl = lobes ? (long long)d.K * 8 : 0;
@@ -1026,7 +979,7 @@ int fit_fused_launches(const vcl_fit* f) {
     int n = 1 /* begin */ + 1 /* project */ + 1 /* aa screen terms */ + raster_fwd_launches() + 1 /* shade */ +
             1 /* aa + mse */ + 1 /* aa bwd */;
     if (d.learn_tex || d.learn_pos) n += 1; /* per-pixel backward */
-    if (d.learn_lobes && d.K) n += (d.K + 31) / 32 <= LOBE_CLAIM_GROUPS ? 2 : 1;   /* lobe gradients (+ tail) */
+    if (d.learn_lobes && d.K) n += 1;       /* lobe gradients */
     if (d.learn_pos) n += 1;
     if (d.learn_tex) {
         const bool tile = d.tex_w % 32 == 0 && d.tex_h % 32 == 0 && d.levels >= 2;
@@ -1055,7 +1008,6 @@ void fit_fused_release(vcl_fit* f, cudaStream_t s, bool async) {
     if (F->side) cudaStreamDestroy(F->side);
     if (F->fork) cudaEventDestroy(F->fork);
     if (F->join) cudaEventDestroy(F->join);
-    if (F->claims_ready) cudaEventDestroy(F->claims_ready);
     delete F;
     f->fused = nullptr;
 }
