@@ -119,9 +119,8 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
  * not allocate device memory or synchronize the device on their per-frame
  * path.  No counterpart in the reference (its rasterizer has no workspace).
  * Same arguments and results as vcl_rasterize_fwd.  Requests whose depth
- * keys (8 B per pixel and view), triangle records, their barycentric-
- * derivative coefficients and medium-list entries
- * (VCL_RASTER_BYTES_PER_VIEW_TRIANGLE = 96 + 48 + 4 B per view and triangle) and
+ * keys (8 B per pixel and view), triangle records and medium-list entries
+ * (VCL_RASTER_BYTES_PER_VIEW_TRIANGLE = 96 + 4 B per view and triangle) and
  * tile counters (12 B per tile and view), each rounded up to 256 B, exceed
  * the limit return VCL_ERR_ARG; what is left holds the tile bin lists (4 B
  * per entry).  No part of the scratch needs to start at zero.  One scratch
@@ -132,7 +131,7 @@ VCL_API vcl_status vcl_rasterize_fwd(vcl_ctx* ctx, const float* clip, int nv, co
  * the scratch: after a reset, call vcl_raster_scratch_init again (it always
  * resolves the address anew) before the next static call. */
 #define VCL_RASTER_SCRATCH_BYTES (32u << 20)
-#define VCL_RASTER_BYTES_PER_VIEW_TRIANGLE 148
+#define VCL_RASTER_BYTES_PER_VIEW_TRIANGLE 100
 VCL_API size_t vcl_raster_scratch_bytes(void);
 VCL_API vcl_status vcl_raster_scratch_init(vcl_ctx* ctx);
 VCL_API vcl_status vcl_rasterize_fwd_static(vcl_ctx* ctx, const float* clip, int nv, const uint32_t* tri, int nt,

@@ -102,7 +102,7 @@ def test_static_scratch_rejects_oversize_request(ctx):
 def test_static_scratch_bin_list_cut_to_room(ctx):
     """A request whose depth keys nearly fill the scratch: the bin list gets
     only the room that is left, less than the automatic capacity asks for.
-    The documented sizes (8 B per pixel, 148 B per view and triangle, 12 B
+    The documented sizes (8 B per pixel, 100 B per view and triangle, 12 B
     per tile, each part rounded up to 256 B) say how much room that is; the
     result stays bit-identical to the workspace path, with every triangle
     through the bins and with the default direct paths."""
@@ -112,7 +112,7 @@ def test_static_scratch_bin_list_cut_to_room(ctx):
     npix, vt = S.W * S.H * S.views, S.nt * S.views
     tile = 16
     ntiles = -(-S.W // tile) * -(-S.H // tile) * S.views
-    fixed = a256(8 * npix) + a256(96 * vt) + a256(48 * vt) + a256(4 * vt) + 3 * a256(4 * (ntiles + 1))
+    fixed = a256(8 * npix) + a256(96 * vt) + a256(4 * vt) + 3 * a256(4 * (ntiles + 1))
     limit = capi.lib().vcl_raster_scratch_bytes()
     assert fixed < limit
     room = ((limit - fixed) // 4) & ~63

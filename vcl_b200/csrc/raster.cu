@@ -46,16 +46,9 @@ struct __align__(16) RTri {
     float4 w;   // w0 w1 w2 -
     int4 box;   // x0 x1 y0 y1 ; empty when x0 > x1
 };
-// The barycentric-derivative (DB) coefficients of a triangle: d[v] =
-// d(u, v)/d(x, y) of vertex v before the perspective weighting
-// (rasterize.cpp:141-164), computed once per (view, triangle).
-struct __align__(16) DBCoef {
-    float4 d0, d1, d2;
-};
-// the workspace's per-(view, triangle) cost that vcl.h states: this record,
-// the DB coefficients and one medium-list entry
-static_assert(sizeof(RTri) + sizeof(DBCoef) + sizeof(int) == VCL_RASTER_BYTES_PER_VIEW_TRIANGLE,
-              "raster record size changed");
+// the workspace's per-(view, triangle) cost that vcl.h states: this record
+// plus one medium-list entry
+static_assert(sizeof(RTri) + sizeof(int) == VCL_RASTER_BYTES_PER_VIEW_TRIANGLE, "raster record size changed");
 
 constexpr int CHUNK = 128;
 // default box areas (pixels): up to SMALL_AREA a triangle is rasterized by its
@@ -403,9 +396,29 @@ __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ in, int* 
     }
 }
 
+__global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int W, int H, int tile, int tiles_x,
+                       int ntiles, const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list,
+                       long long cap, int small_area, int med_area) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long long)views * nt) return;
+    int view = (int)(gid / nt), t = (int)(gid % nt);
+    const RTri r = setup[gid];
+    const int4 box = r.box;
+    if (box.x > box.y || box.z > box.w || is_direct(box, small_area, med_area)) return;
+    int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) {
+            if (!tile_overlaps(r, tx, ty, tile, W, H)) continue;
+            size_t ti = (size_t)view * ntiles + ty * tiles_x + tx;
+            int slot = atomicAdd(&cursor[ti], 1);
+            long long p = (long long)offset[ti] + slot;
+            if (p < cap) list[p] = t;
+        }
+}
+
 // The reference geometry shader's per-vertex barycentric derivatives
-// (rasterize.cpp:141-164) of one triangle, before the per-pixel weighting.
-DEV DBCoef db_coeffs(float4 c0, float4 c1, float4 c2, float xs, float ys) {
+// (rasterize.cpp:141-164), evaluated at (u, v) and scaled by w (:176).
+DEV float4 db_eval(float4 c0, float4 c1, float4 c2, float xs, float ys, float u, float v) {
     float w0 = c0.w, w1 = c1.w, w2 = c2.w;
     float e0x = sub(mul(w0, c2.x), mul(w2, c0.x)), e0y = sub(mul(w0, c2.y), mul(w2, c0.y));
     float e1x = sub(mul(w1, c2.x), mul(w2, c1.x)), e1y = sub(mul(w1, c2.y), mul(w2, c1.y));
@@ -417,53 +430,15 @@ DEV DBCoef db_coeffs(float4 c0, float4 c1, float4 c2, float xs, float ys) {
     e0x = mul(e0x, sx); e0y = mul(e0y, sy);
     e1x = mul(e1x, sx); e1y = mul(e1y, sy);
     ex = mul(ex, sx); ey = mul(ey, sy);
-    DBCoef d;
-    d.d0 = make_float4(sub(e0y, ey), add(-e0x, ex), -e0y, e0x);
-    d.d1 = make_float4(e1y, -e1x, sub(-e1y, ey), add(e1x, ex));
-    d.d2 = make_float4(e1y, -e1x, -e0y, e0x);
-    return d;
-}
-
-// DB at (u, v), scaled by the interpolated w (rasterize.cpp:176).
-DEV float4 db_eval(const DBCoef& d, float4 w, float u, float v) {
-    const float d0[4] = {d.d0.x, d.d0.y, d.d0.z, d.d0.w}, d1[4] = {d.d1.x, d.d1.y, d.d1.z, d.d1.w};
-    const float d2[4] = {d.d2.x, d.d2.y, d.d2.z, d.d2.w};
+    float d0[4] = {sub(e0y, ey), add(-e0x, ex), -e0y, e0x};
+    float d1[4] = {e1y, -e1x, sub(-e1y, ey), add(e1x, ex)};
+    float d2[4] = {e1y, -e1x, -e0y, e0x};
     float l2 = sub(sub(1.f, u), v);
-    float wi = add(add(mul(u, w.x), mul(v, w.y)), mul(l2, w.z));
+    float wi = add(add(mul(u, w0), mul(v, w1)), mul(l2, w2));
     float o[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) o[c] = mul(add(add(mul(u, d0[c]), mul(v, d1[c])), mul(l2, d2[c])), wi);
     return make_float4(o[0], o[1], o[2], o[3]);
-}
-
-// Bins the large triangles (see the file comment) and, when DB is wanted,
-// stores every drawable triangle's DB coefficients for the resolve pass.
-__global__ void k_emit(const RTri* __restrict__ setup, int nt, int views, int W, int H, int tile, int tiles_x,
-                       int ntiles, const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ list,
-                       long long cap, int small_area, int med_area, const float4* __restrict__ clip, int nv,
-                       const uint32_t* __restrict__ tri, DBCoef* __restrict__ dbc) {
-    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long long)views * nt) return;
-    int view = (int)(gid / nt), t = (int)(gid % nt);
-    const RTri r = setup[gid];
-    const int4 box = r.box;
-    if (box.x > box.y || box.z > box.w) return;
-    if (dbc) {
-        // indices were checked by the setup pass (an out-of-range triangle has an empty box)
-        const float4* cv = clip + (size_t)view * nv;
-        dbc[gid] = db_coeffs(cv[tri[3 * (size_t)t]], cv[tri[3 * (size_t)t + 1]], cv[tri[3 * (size_t)t + 2]],
-                             dvd(2.f, (float)W), dvd(2.f, (float)H));
-    }
-    if (is_direct(box, small_area, med_area)) return;
-    int tx0 = box.x / tile, tx1 = box.y / tile, ty0 = box.z / tile, ty1 = box.w / tile;
-    for (int ty = ty0; ty <= ty1; ++ty)
-        for (int tx = tx0; tx <= tx1; ++tx) {
-            if (!tile_overlaps(r, tx, ty, tile, W, H)) continue;
-            size_t ti = (size_t)view * ntiles + ty * tiles_x + tx;
-            int slot = atomicAdd(&cursor[ti], 1);
-            long long p = (long long)offset[ti] + slot;
-            if (p < cap) list[p] = t;
-        }
 }
 
 template <int T>
@@ -574,8 +549,8 @@ __global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, 
 // Winning key -> (u, v, z/w, id+1) and DB per pixel; held to 32 registers
 // for eight blocks per SM (the record and vertex gathers need the warps).
 __global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, long long npix,
-                          const unsigned long long* __restrict__ keys, const DBCoef* __restrict__ dbc,
-                          float4* __restrict__ rast, float4* __restrict__ db) {
+                          const unsigned long long* __restrict__ keys, const float4* __restrict__ clip, int nv,
+                          const uint32_t* __restrict__ tri, float4* __restrict__ rast, float4* __restrict__ db) {
     const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= npix) return;
     const unsigned long long key = keys[pix];
@@ -597,7 +572,11 @@ __global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ set
     float D = add(add(A0, A1), A2);
     float u = dvd(A0, D), v = dvd(A1, D);
     rast[pix] = make_float4(u, v, key_depth(key), (float)(t + 1));
-    if (db) db[pix] = db_eval(dbc[(size_t)view * nt + t], r.w, u, v);
+    if (db) {
+        const float4* cv = clip + (size_t)view * nv;
+        float4 c0 = cv[tri[3 * (size_t)t]], c1 = cv[tri[3 * (size_t)t + 1]], c2 = cv[tri[3 * (size_t)t + 2]];
+        db[pix] = db_eval(c0, c1, c2, dvd(2.f, (float)W), dvd(2.f, (float)H), u, v);
+    }
 }
 
 // rasterize.cu:84-141: dL/d(x, y, w) of the three clip-space vertices from
@@ -734,7 +713,6 @@ __global__ void k_tie_count(const unsigned* __restrict__ flags, long long n, uns
 struct RasterWS {
     unsigned long long* keys;
     RTri* setup;
-    DBCoef* dbc;       // [views * nt] DB coefficients
     int* med_list;     // [views * nt] medium triangles (view * nt + t)
     int* count;        // [ntiles + 1]; count[ntiles] = number of medium triangles
     int* offset;
@@ -754,7 +732,7 @@ long long auto_capacity_(long long views, long long nt, int W, int H, int tile) 
 size_t ws_bytes(long long npix, long long views, long long nt, long long ntiles, long long cap) {
     const size_t vt = (size_t)(views * nt > 0 ? views * nt : 1);
     return align256(sizeof(unsigned long long) * (size_t)npix) + align256(sizeof(RTri) * vt) +
-           align256(sizeof(DBCoef) * vt) + align256(sizeof(int) * vt) + 3 * align256(sizeof(int) * (size_t)(ntiles + 1)) +
+           align256(sizeof(int) * vt) + 3 * align256(sizeof(int) * (size_t)(ntiles + 1)) +
            align256(sizeof(int) * (size_t)cap);
 }
 
@@ -764,7 +742,6 @@ RasterWS carve(void* base, long long npix, long long views, long long nt, long l
     w.keys = (unsigned long long*)p; p += align256(sizeof(unsigned long long) * (size_t)npix);
     const size_t vt = (size_t)(views * nt > 0 ? views * nt : 1);
     w.setup = (RTri*)p; p += align256(sizeof(RTri) * vt);
-    w.dbc = (DBCoef*)p; p += align256(sizeof(DBCoef) * vt);
     w.med_list = (int*)p; p += align256(sizeof(int) * vt);
     w.count = (int*)p; p += align256(sizeof(int) * (size_t)(ntiles + 1));
     w.offset = (int*)p; p += align256(sizeof(int) * (size_t)(ntiles + 1));
@@ -822,8 +799,7 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     k_scan<<<1, 1024, 0, s>>>(w.count, w.offset, (int)ntiles);
     if (work > 0) {
         k_emit<<<vcl_blocks(work, 256), 256, 0, s>>>(w.setup, nt, views, W, H, T, tiles_x, (int)ntiles_view,
-                                                      w.offset, w.cursor, w.list, cap, sa, ma, (const float4*)clip,
-                                                      nv, tri, db ? w.dbc : nullptr);
+                                                      w.offset, w.cursor, w.list, cap, sa, ma);
     }
     dim3 grid((unsigned)ntiles_view, (unsigned)views);
     if (T == 8)
@@ -835,8 +811,8 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     else
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
                                                (int)ntiles_view, w.keys, flags, sa, ma);
-    k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, w.dbc, (float4*)rast,
-                                                     (float4*)db);
+    k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, (const float4*)clip, nv, tri,
+                                                     (float4*)rast, (float4*)db);
     return vcl_launch_check(ctx, "rasterize_fwd");
 }
 

@@ -14,13 +14,13 @@
 // Limits and rules:
 //   * RASTER_SCRATCH_BYTES (VCL_RASTER_SCRATCH_BYTES, 32 MiB) bounds the
 //     request: the per-pixel depth keys (8 B x W x H x views), the triangle
-//     records with their DB coefficients and medium-list entries (96 + 48 + 4
-//     = 148 B x views x nt, VCL_RASTER_BYTES_PER_VIEW_TRIANGLE) and the
-//     per-tile counters (12 B x tiles x views) must fit, and the remainder
-//     holds the tile bin lists.  Larger requests are rejected with
-//     VCL_ERR_ARG and a message that gives the bytes needed.  A bin list
-//     that does not fit the remainder falls back to testing every large
-//     triangle for the overflowing tiles: same result, slower.
+//     records with their medium-list entries (96 + 4 = 100 B x views x nt,
+//     VCL_RASTER_BYTES_PER_VIEW_TRIANGLE) and the per-tile counters (12 B x
+//     tiles x views) must fit, and the remainder holds the tile bin lists.
+//     Larger requests are rejected with VCL_ERR_ARG and a message that gives
+//     the bytes needed.  A bin list that
+//     does not fit the remainder falls back to testing every large triangle
+//     for the overflowing tiles: same result, slower.
 //   * Nothing in the scratch has to start at zero: every call initializes
 //     what it reads (depth keys to "empty", tile counters to 0) on the stream
 //     before any kernel uses them, so the scratch carries no state between
