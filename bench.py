@@ -199,8 +199,8 @@ def fused_bytes(S, ncov):
 # views of 1024x1024 of this workload, divided by the pixels); their traffic
 # grows with the pixel count.
 DRAM_BYTES_PER_PIXEL = {
-    "bwd_pix": (319.0e6 + 64.1e6) / (4 * 1024 * 1024),
-    "sg_lobes": (182.5e6 + 4.1e6) / (4 * 1024 * 1024),
+    "bwd_pix": (321.2e6 + 64.6e6) / (4 * 1024 * 1024),
+    "sg_lobes": (182.8e6 + 4.0e6) / (4 * 1024 * 1024),
 }
 # What bounds each of them instead of HBM bandwidth (same capture).
 BOUND_NOTE = {
