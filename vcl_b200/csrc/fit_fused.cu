@@ -342,9 +342,9 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // shuffles, as many rounds as the longest run needs) and the last lane of a
 // run issues its three vector reductions: neighbouring pixels of one
 // triangle no longer collide on the same three addresses.  Held to 40
-// registers so that its blocks fit on the SMs beside the lobe-gradient
-// blocks it runs with.
-__global__ void __launch_bounds__(256, 6) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+// registers in blocks of 128 threads so that its blocks fit, at a fine
+// grain, on the SMs beside the lobe-gradient blocks it runs with.
+__global__ void __launch_bounds__(128, 12) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
                                                  int want_tex, int want_geom) {
@@ -835,9 +835,9 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     const int groups = (d.K + 31) / 32;
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
-    // three lobe blocks per SM (over all lobe groups) leave registers for two
-    // blocks of the per-pixel backward that runs beside this kernel (the two
-    // overlap on each SM)
+    // three lobe blocks per SM (over all lobe groups) leave registers for
+    // four 128-thread blocks of the per-pixel backward that runs beside this
+    // kernel (the two overlap on each SM)
     long long capg = ((long long)ctx->sm_count * 3 + groups - 1) / groups;
     const dim3 grid((unsigned)(want < capg ? (want < 1 ? 1 : want) : capg), (unsigned)groups);
     const float4* gc = (const float4*)f->g_color;
@@ -849,7 +849,7 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
 
 vcl_status stage_bwd_pix(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
     const vcl_fit_desc& d = f->d;
-    k_bwd_pix<<<vcl_blocks(a.npix, 256), 256, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
+    k_bwd_pix<<<vcl_blocks(a.npix, 128), 128, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
                                                       f->g_pyr, f->clip, f->g_clip, d.learn_tex, d.learn_pos);
     return vcl_launch_check(f->ctx, "fused backward");
 }
