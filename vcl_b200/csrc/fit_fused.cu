@@ -157,9 +157,10 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
 // Forward shading of every pixel; writes the color and the diffuse
 // environment sum (kept for the backward's diffuse gradient) and, when
 // rec.count is set, the shading record of each covered pixel (one slot
-// claim per block).  C = 4; 256 threads, held to 40 registers for six blocks
-// per SM (more warps to cover the texture and attribute loads).
-__global__ void __launch_bounds__(256, 6) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
+// claim per block).  C = 4; 128 threads, held to 40 registers for twelve
+// blocks per SM (more warps to cover the texture and attribute loads, and a
+// finer grain for the block scheduler than 256-thread blocks).
+__global__ void __launch_bounds__(128, 12) k_shade_fwd(ShadeIn a, TexDesc td, float4* __restrict__ color,
                                                    float4* __restrict__ diffenv, ShadeRec rec) {
     extern __shared__ float4 sm4[];
     __shared__ int s_off[8], s_base;
@@ -813,7 +814,7 @@ ShadeRec shade_rec(const vcl_fit* f, bool want) {
 vcl_status stage_shade(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
     const ShadeRec rec = shade_rec(f, f->d.learn_lobes && f->d.K);
     if (rec.count) TRY(vcl_cuda_check(f->ctx, cudaMemsetAsync(rec.count, 0, sizeof(int), s), "record count"));
-    k_shade_fwd<<<vcl_blocks(a.npix, 256), 256, shade_smem(a.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse,
+    k_shade_fwd<<<vcl_blocks(a.npix, 128), 128, shade_smem(a.K), s>>>(a, td, (float4*)f->color, (float4*)f->diffuse,
                                                                      rec);
     return vcl_launch_check(f->ctx, "fused shade");
 }
