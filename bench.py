@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mix", action="store_true", help="default run: skip the batched-vs-plain mix measurement")
     ap.add_argument("--no-serve", action="store_true", help="default run: skip the serving measurement")
+    ap.add_argument("--no-config5", action="store_true",
+                    help="default run: skip the dense-stress fit iteration (4 x 2048^2, 1.31M triangles, 4096^2 texture)")
     ap.add_argument("--serve-lam", type=float, default=100.0, help="default run: serving arrival rate (jobs/s)")
     ap.add_argument("--serve-jobs", type=int, default=24, help="default run: serving jobs per repeat")
     ap.add_argument("--serve-repeats", type=int, default=3, help="default run: serving repeats")
@@ -708,6 +710,23 @@ def serve_summary(args):
                         f"arrivals at {args.serve_lam:g} jobs/s, {r['budget_gb']:g} GB admission budget"}
 
 
+def config5_summary(args):
+    """The dense-stress fit iteration (icosphere s8, 1,310,720 triangles, 4
+    views of 2048^2, 4096^2 texture with 13 levels, 64 lobes), fused and
+    plain, timed by this script in a child process (--config config5)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--config", "config5", "--no-mix", "--no-serve",
+           "--no-config5", "--no-cpu-baseline", "--no-e2e", "--steps", "10", "--warmup", "3"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    if out.returncode != 0 or not lines:
+        raise RuntimeError(f"config5 run failed: {out.stderr[-2000:]}")
+    d = json.loads(lines[-1])
+    return {"workload": d["config"]["workload"], "iters_per_s": d["value"], "ms_per_step": d["ms_per_step"],
+            "strategies_ms_per_step": d["strategies_ms_per_step"], "fused_kernels_ms": d.get("fused_kernels_ms"),
+            "stages_ms": d.get("stages_ms"), "raster_ties": d.get("raster_ties"), "steps": 10, "warmup": 3,
+            "clocks": d.get("clocks")}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -827,6 +846,8 @@ def main():
         per_iter, _, kind, cores, sample = time_reference(S, os.cpu_count() or 1, S.views, 1)
         line["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": "iters/s", "cores": cores, "kind": kind,
                                 "sample": sample}
+    if not args.no_config5 and args.config == "config2":
+        line["config5"] = config5_summary(args)
     if not args.no_mix:
         line["mix"] = mix_summary(args)
     if not args.no_serve:
