@@ -476,8 +476,10 @@ struct AdamArgs {
 // TextureGrad::gradSumup (buffer.cu:615-648) folded into level 0, Adam
 // (optimize.cu:95-106), clamp (buffer.cu:65-72), gradient clear, and the
 // 2x2 mip chain (buffer.cu:449-472) of each 32x32 level-0 tile up to level
-// `top` (<= 5).  One thread per 2x2 level-0 quad; C = 4.
-__global__ void __launch_bounds__(256) k_adam_tex_tile(TexDesc td, float* __restrict__ pyr, float* __restrict__ gpyr,
+// `top` (<= 5).  One thread per 2x2 level-0 quad; C = 4.  Held to 64
+// registers for four blocks per SM (the FP64 Adam arithmetic waits on its
+// divisions and square roots; the extra warps cover them).
+__global__ void __launch_bounds__(256, 4) k_adam_tex_tile(TexDesc td, float* __restrict__ pyr, float* __restrict__ gpyr,
                                                        float* __restrict__ m, float* __restrict__ v, AdamArgs aa,
                                                        float wpush, int top) {
     __shared__ float4 s_lvl[16][16];
