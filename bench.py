@@ -783,8 +783,9 @@ def main():
     if "fused_kernel_ms" in r:
         # the dominant kernel of the fused step, timed live (CUDA events on its
         # stream, after the timed region)
-        kms = r["fused_kernel_ms"]
+        kall = r["fused_kernel_ms"]
         byts = fused_bytes(S, ncov)
+        kms = {k: v for k, v in kall.items() if k in byts}
         top = max(kms, key=lambda k: kms[k])
         b = byts[top]
         achieved = b / (kms[top] * 1e-3) / 1e9
@@ -794,7 +795,7 @@ def main():
                             "frac": achieved / hbm_peak, "traffic": traffic, "peak_source": peak_src,
                             "algorithmic_bytes": b, "avg_ms": kms[top],
                             "note": BOUND_NOTE.get(top)}
-        line["fused_kernels_ms"] = {k: round(v, 4) for k, v in kms.items()}
+        line["fused_kernels_ms"] = {k: round(v, 4) for k, v in kall.items()}
         line["fused_kernels_frac_hbm"] = {k: round(byts[k] / (v * 1e-3) / 1e9 / hbm_peak, 3)
                                           for k, v in kms.items() if v > 0}
         # the SG kernels' own bound, the MUFU pipe: 2 rsqrt + 4 ex2 per covered

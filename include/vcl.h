@@ -387,8 +387,9 @@ VCL_API vcl_status vcl_fit_raster_schedule(vcl_fit* fit, int* tile, int* small_a
 VCL_API void vcl_raster_tuning_cache_clear(void);
 /* Average device time (ms per launch) of each fused-step stage on the job's
  * current state, after at least one fused step: ms[i] for stage i of
- * vcl_fit_kernel_name(i) ("raster", "shade_fwd", "aa_fwd", "mse", "aa_bwd",
- * "bwd_pix", "sg_lobes"); one untimed launch, then `reps` timed ones on
+ * vcl_fit_kernel_name(i) ("raster", "shade_fwd", "aa_fwd_mse", "aa_bwd",
+ * "bwd_pix", "sg_lobes", and "bwd_pix+sg_lobes": the last two on two streams
+ * as the step runs them); one untimed launch, then `reps` timed ones on
  * `stream`.  Parameters and Adam moments are untouched; the gradient
  * buffers are cleared (the next step recomputes them).  Synchronizes. */
 VCL_API int vcl_fit_kernel_count(void);

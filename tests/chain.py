@@ -152,19 +152,23 @@ def oracle_fit(S, mode, steps, target, lr=None):
             "g_tex_resolved": g_tex_res.reshape(S.tex_h, S.tex_w, C)}
 
 
-def run_isolated64(S, o, mode=0):
+def run_isolated64(S, o, mode=0, chained=False):
     """Every operator of run_chain evaluated once more by the double-precision
     restatement (liborc64), each fed the FP32 oracle's own inputs for its
     stage (the values the isolated GPU chain gets), promoted to double: the
     exact result of each stage for those inputs, up to double rounding.  The
     parity tests measure how far the CUDA path and the FP32 restatement each
-    are from it."""
+    are from it.  chained=True feeds each stage the double results of the
+    stages before it instead (the exact chain from the same scene, target and
+    rasterization; the raster's own outputs are discrete and bit-identical on
+    both sides, so they stay the oracle's), for the chained comparison."""
     L = O.orc64()
     W, H, V, C, K = S.W, S.H, S.views, S.C, S.K
     N = W * H * V
     d = lambda a: np.ascontiguousarray(np.asarray(a, np.float64))
     z = lambda *shape: np.zeros(shape, np.float64)
     r = {}
+    src = (lambda k: r[k]) if chained else (lambda k: d(o[k]))
     clip = z(V, S.nv, 4)
     for v in range(V):
         out = z(S.nv, 4)
@@ -177,7 +181,7 @@ def run_isolated64(S, o, mode=0):
     r["uv"], r["uv_da"] = uv, uv_da
     pyr = d(o["pyr"])
     diffuse = z(N, C)
-    L.texture_fwd(W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, d(o["uv"]), d(o["uv_da"]), diffuse)
+    L.texture_fwd(W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, src("uv"), src("uv_da"), diffuse)
     r["diffuse"] = diffuse
     normal, view = z(N, 3), z(N, 3)
     L.normal_axis_fwd(W, H, V, rast, d(S.rot), d(S.normal), S.tri, normal)
@@ -185,50 +189,50 @@ def run_isolated64(S, o, mode=0):
     r["normal"], r["view"] = normal, view
     rough = np.full((N,), S.roughness, np.float64)
     sax, ssh, sam = z(N, 3), z(N), z(N)
-    L.sg_specular_fwd(W, H, V, rast, d(o["normal"]), d(o["view"]), rough, S.ior, sax, ssh, sam)
+    L.sg_specular_fwd(W, H, V, rast, src("normal"), src("view"), rough, S.ior, sax, ssh, sam)
     r["spec_axis"], r["spec_sharp"], r["spec_amp"] = sax, ssh, sam
     axis, sharp, amp = d(S.lobe_axis_init), d(S.lobe_sharp_init), d(S.lobe_amp_init)
     color, denv, senv = z(N, C), z(N, C), z(N, C)
-    L.sg_fwd(W, H, V, C, rast, K, axis, sharp, amp, d(o["normal"]), d(o["diffuse"]), d(o["spec_axis"]),
-             d(o["spec_sharp"]), d(o["spec_amp"]), color, denv, senv)
+    L.sg_fwd(W, H, V, C, rast, K, axis, sharp, amp, src("normal"), src("diffuse"), src("spec_axis"),
+             src("spec_sharp"), src("spec_amp"), color, denv, senv)
     r["color"], r["diffenv"], r["specenv"] = color, denv, senv
     aa = z(N, C)
-    L.antialias_fwd(W, H, V, C, d(o["clip"]), S.nv, S.tri, rast, d(o["color"]), aa)
+    L.antialias_fwd(W, H, V, C, src("clip"), S.nv, S.tri, rast, src("color"), aa)
     r["aa"] = aa
     g_aa = z(N, C)
-    L.mse(mode, N * C, d(o["aa"]), d(o["target"]), g_aa)
+    L.mse(mode, N * C, src("aa"), d(o["target"]), g_aa)
     r["g_aa"] = g_aa
     g_color, g_clip = z(N, C), z(V, S.nv, 4)
-    L.antialias_bwd(mode, W, H, V, C, d(o["clip"]), S.nv, S.tri, rast, d(o["color"]), d(o["g_aa"]), g_color, g_clip)
+    L.antialias_bwd(mode, W, H, V, C, src("clip"), S.nv, S.tri, rast, src("color"), src("g_aa"), g_color, g_clip)
     r["g_color"], r["g_clip_aa"] = g_color, g_clip
     g_diffuse, g_axis, g_sharp, g_amp = z(N, C), z(K, 3), z(K), z(K, C)
     g_sax, g_ssh, g_sam = z(N, 3), z(N), z(N * C)
-    L.sg_bwd(mode, W, H, V, C, rast, K, axis, sharp, amp, d(o["normal"]), d(o["diffuse"]), d(o["spec_axis"]),
-             d(o["spec_sharp"]), d(o["spec_amp"]), d(o["g_color"]), g_diffuse, g_axis, g_sharp, g_amp, g_sax, g_ssh,
+    L.sg_bwd(mode, W, H, V, C, rast, K, axis, sharp, amp, src("normal"), src("diffuse"), src("spec_axis"),
+             src("spec_sharp"), src("spec_amp"), src("g_color"), g_diffuse, g_axis, g_sharp, g_amp, g_sax, g_ssh,
              g_sam)
     r.update(g_diffuse=g_diffuse, g_axis=g_axis, g_sharp=g_sharp, g_amp=g_amp, g_sax=g_sax, g_ssh=g_ssh, g_sam=g_sam)
     g_rough = z(N)
-    L.sg_specular_bwd(W, H, V, rast, d(o["normal"]), d(o["view"]), rough, S.ior, d(o["g_sam"]), d(o["g_ssh"]),
+    L.sg_specular_bwd(W, H, V, rast, src("normal"), src("view"), rough, S.ior, src("g_sam"), src("g_ssh"),
                       g_rough)
     r["g_rough"] = g_rough
     g_pyr, g_uv, g_uv_da = np.zeros_like(pyr), z(N, 2), z(N, 4)
-    L.texture_bwd(mode, W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, d(o["uv"]), d(o["uv_da"]),
-                  d(o["g_diffuse"]), g_pyr, g_uv, g_uv_da)
+    L.texture_bwd(mode, W, H, V, S.tex_w, S.tex_h, C, S.levels, pyr, rast, src("uv"), src("uv_da"),
+                  src("g_diffuse"), g_pyr, g_uv, g_uv_da)
     r["g_pyr"], r["g_uv"], r["g_uv_da"] = g_pyr, g_uv, g_uv_da
     g_uvattr, g_bary = z(S.nv, 2), z(N, 2)
-    L.interpolate_bwd(mode, W, H, V, 2, rast, d(S.uv), S.tri, d(o["g_uv"]), g_uvattr, g_bary)
+    L.interpolate_bwd(mode, W, H, V, 2, rast, d(S.uv), S.tri, src("g_uv"), g_uvattr, g_bary)
     r["g_uvattr"], r["g_bary"] = g_uvattr, g_bary
-    g_clip2 = d(o["g_clip_aa"]).copy()
-    L.rasterize_bwd(W, H, V, d(o["clip"]), S.nv, S.tri, rast, d(o["g_bary"]), g_clip2)
+    g_clip2 = src("g_clip_aa").copy()
+    L.rasterize_bwd(W, H, V, src("clip"), S.nv, S.tri, rast, src("g_bary"), g_clip2)
     r["g_clip"] = g_clip2
     g_pos = z(S.nv, 3)
-    gc = d(o["g_clip"])
+    gc = src("g_clip")
     for v in range(V):
         L.project_bwd(S.nv, d(S.mvp[v]), np.ascontiguousarray(gc[v]), 4, g_pos)
     r["g_pos"] = g_pos
     if "adam_p" in o:
         n0 = S.tex_w * S.tex_h * C
         p, m, vv = d(o["pyr"][:n0]).copy(), z(n0), z(n0)
-        L.adam(mode, n0, p, d(o["g_pyr"][:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, 1)
+        L.adam(mode, n0, p, np.ascontiguousarray(src("g_pyr")[:n0]), m, vv, S.lr, 0.9, 0.999, 1e-8, 1)
         r["adam_p"], r["adam_m"], r["adam_v"] = p, m, vv
     return r

@@ -103,6 +103,47 @@ def test_fused_odd_sizes_match_oracle(ctx, mode):
         assert_adam_close(got, want, S.lr, steps, name)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("strategy", [0, 1])
+def test_fit_with_non_finite_target_pixels_matches_oracle(ctx, mode, strategy):
+    """NaN and +-inf target pixels (a hole in a mask, a broken image) make the
+    loss NaN and every gradient that flows from those pixels non-finite.  The
+    reference drops such terms where it adds through its guarded add
+    (common.h:181: the SG lobe sums, material.cu:428-436; the mip gradient
+    push-down, buffer.cu:615-648; the Adam update, optimize.cu:106) and lets
+    them through where it does not (antialias, texture and raster
+    backward), so the parameters whose update was dropped keep their values
+    and all parameters stay finite.  Both strategies must leave every
+    parameter as the oracle's fit does."""
+    from vcl_b200 import capi
+    S = _scene()
+    tgt = _target(S)
+    N = S.W * S.H * S.views
+    pick = np.random.default_rng(5).choice(N, 12, replace=False)
+    tgt[pick[:4], 1] = np.nan
+    tgt[pick[4:8]] = np.inf
+    tgt[pick[8:], 2] = -np.inf
+    steps = 3
+    with np.errstate(invalid="ignore"):
+        ref = chain.oracle_fit(S, mode, steps, tgt)
+    ctx.set_mode(mode)
+    fit = capi.Fit(ctx, S, strategy=strategy)
+    fit.set_target(tgt)
+    stream = torch.cuda.Stream()
+    losses = []
+    for _ in range(steps):
+        fit.step(stream.cuda_stream)
+        losses.append(fit.read_loss(stream.cuda_stream))
+    pos, tex, (ax, sh, am) = fit.read_params(stream.cuda_stream)
+    fit.close()
+    ctx.set_mode(0)
+    assert not np.isfinite(ref["losses"]).any() and not np.isfinite(losses).any(), (losses, ref["losses"])
+    for name, got, want in (("tex", tex, ref["tex"]), ("pos", pos, ref["pos"]), ("axis", ax, ref["axis"]),
+                            ("sharp", sh, ref["sharp"]), ("amp", am, ref["amp"])):
+        assert np.isfinite(want).all() and np.isfinite(got).all(), name
+        assert_adam_close(got, want, S.lr, steps, name)
+
+
 @pytest.mark.parametrize("strategy", [0, 1])
 def test_state_save_load_resumes(ctx, strategy):
     """A job saved after 3 steps and loaded into a fresh job of the same

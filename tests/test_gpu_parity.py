@@ -3,12 +3,14 @@
 Each operator gets the oracle's inputs for its stage, so every comparison
 isolates one kernel.  Bars: triangle ids, barycentrics, depth and DB are
 bit-identical (the rasterizer uses exactly rounded arithmetic); every other
-output within 1e-5 relative to the array's largest magnitude (FP32; atomic
-accumulation order differs)."""
+output is held to the bars of parity.py (1e-5 normwise against the FP32
+oracle, and element by element as close to the exact stage value as the
+oracle is); the narrower checks below use the 1e-5 normwise bar."""
 import numpy as np
 import pytest
 
 import chain
+import parity
 from oracle import oracle as O
 from vcl_b200 import scenes
 
@@ -67,7 +69,8 @@ def test_operators_match_oracle(ctx, si, mode):
     assert np.array_equal(g["rast"][:, 3], o["rast"][:, 3]), "triangle ids differ"
     assert np.array_equal(g["rast"], o["rast"]), "barycentrics/depth differ"
     assert np.array_equal(g["db"], o["db"]), "DB differs"
-    bad = {k: rel_err(g[k], o[k]) for k in KEYS if rel_err(g[k], o[k]) > REL_TOL}
+    exact = chain.run_isolated64(S, o, mode)
+    res, bad = parity.check_keys(g, o, exact, KEYS, f"small{si}:mode{mode}")
     assert not bad, bad
     n = S.W * S.H * S.views * S.C
     exact_loss = O.orc().mse(1, n, o["aa"], o["target"], np.zeros(n, np.float32))
@@ -99,16 +102,67 @@ def test_sg_bwd_diffuse_and_lobes_only(ctx, si, mode):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("si", [0, 2])
+def test_sg_bwd_drops_non_finite_contributions(ctx, si, mode):
+    """The reference adds every SG gradient contribution through its guarded
+    add (common.h:181, material.cu:428-436): a contribution that would make
+    the sum non-finite is dropped.  With NaN and +-inf in dL/dout at a few
+    covered pixels (one channel, or all four), the diffuse and lobe
+    gradients must equal the oracle's, which drops exactly those
+    contributions, and stay finite."""
+    G = _gpu_chain()
+    S = SCENES[si]
+    assert S.C == 4
+    o = chain.run_chain(O.orc(), S, mode, pyr=chain.build_pyramid(S, S.tex_target))
+    N, C, K = S.W * S.H * S.views, S.C, S.K
+    gout = o["g_color"].reshape(N, C).copy()
+    covered = np.nonzero(o["rast"][:, 3] > 0)[0]
+    pick = np.random.default_rng(11).choice(covered, 6, replace=False)
+    gout[pick[0], 1] = np.nan
+    gout[pick[1], 0] = np.inf
+    gout[pick[2], :] = -np.inf
+    gout[pick[3], 3] = np.nan
+    gout[pick[4], 2] = -np.inf
+    gout[pick[5], :] = np.nan
+    want = {"g_diffuse": np.zeros((N, C), np.float32), "g_axis": np.zeros((K, 3), np.float32),
+            "g_sharp": np.zeros(K, np.float32), "g_amp": np.zeros((K, C), np.float32)}
+    O.orc().sg_bwd(mode, S.W, S.H, S.views, C, o["rast"], K, S.lobe_axis_init, S.lobe_sharp_init, S.lobe_amp_init,
+                   o["normal"], o["diffuse"], o["spec_axis"], o["spec_sharp"], o["spec_amp"], gout,
+                   want["g_diffuse"], want["g_axis"], want["g_sharp"], want["g_amp"], None, None, None)
+    ctx.set_mode(mode)
+    d = lambda k: G.dev(o[k])
+    got = {"g_diffuse": G.zeros(N, C), "g_axis": G.zeros(K, 3), "g_sharp": G.zeros(K), "g_amp": G.zeros(K, C)}
+    ctx.sg_bwd(d("rast"), S.W, S.H, S.views, C, K, G.dev(S.lobe_axis_init), G.dev(S.lobe_sharp_init),
+               G.dev(S.lobe_amp_init), d("normal"), d("diffuse"), d("spec_axis"), d("spec_sharp"), d("spec_amp"),
+               G.dev(gout), got["g_diffuse"], got["g_axis"], got["g_sharp"], got["g_amp"], None, None, None, None)
+    ctx.set_mode(0)
+    for k in want:
+        a = G.host(got[k])
+        assert np.isfinite(want[k]).all() and np.isfinite(a).all(), k
+        assert rel_err(a, want[k]) <= REL_TOL, (k, rel_err(a, want[k]))
+    # the dropped pixels' diffuse gradients stay at their initial 0 where the
+    # oracle drops every lobe's term
+    assert np.array_equal(G.host(got["g_diffuse"])[pick[5]], want["g_diffuse"][pick[5]])
+
+
+@pytest.mark.parametrize("mode", [0, 1])
 def test_chained_pipeline_matches_oracle(ctx, mode):
     S = SCENES[2]
     pyr = chain.build_pyramid(S, S.tex_target)
     o = chain.run_chain(O.orc(), S, mode, pyr=pyr)
     g = _gpu_chain().run_chain_gpu(ctx, S, o, mode, chained=True)
     assert np.array_equal(g["rast"], o["rast"])
-    # (the first Adam step is ~lr*sign(grad), so it is compared on isolated
-    # inputs in test_adam_bit_exact_over_steps, not after chained gradients)
-    for k in ("aa", "g_pyr", "g_pos", "g_axis", "g_amp"):
-        assert rel_err(g[k], o[k]) <= 1e-4, (k, rel_err(g[k], o[k]))
+    # Chained, each side's rounding feeds its own later stages, so both are
+    # measured against the exact chain (every stage in double from the same
+    # scene and rasterization) with the bars of the isolated comparison: the
+    # CUDA chain as close to it as the FP32 oracle's chain, key by key and
+    # element by element.  (The first Adam step is ~lr*sign(grad), so it is
+    # compared on isolated inputs in test_adam_bit_exact_over_steps, not
+    # after chained gradients.)
+    exact = chain.run_isolated64(S, o, mode, chained=True)
+    keys = [k for k in KEYS if not k.startswith("adam_")]
+    res, bad = parity.check_keys(g, o, exact, keys, f"chained:mode{mode}")
+    assert not bad, bad
 
 
 @pytest.mark.parametrize("tile,cap", [(8, 0), (16, 0), (32, 0), (16, 64), (8, 1)])

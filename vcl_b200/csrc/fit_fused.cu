@@ -236,8 +236,13 @@ DEV void pix_sample(const ShadeIn& a, const TexDesc& td, const float4* __restric
     if (idx < 0 || idx >= a.nt) return;
     const uint32_t i0 = a.tri[3 * (size_t)idx], i1 = a.tri[3 * (size_t)idx + 1], i2 = a.tri[3 * (size_t)idx + 2];
     if (i0 >= (uint32_t)a.nv || i1 >= (uint32_t)a.nv || i2 >= (uint32_t)a.nv) return;
+    // dL/d diffuse = dL/dout * diffuse environment sum, through the
+    // reference's guarded add into a cleared gradient (material.cu:429): a
+    // non-finite product is dropped (0), so it reaches neither the texels nor
+    // the geometry
     const float4 gc = g_color[p], de = diffenv[p];
-    S.g = make_float4(gc.x * de.x, gc.y * de.y, gc.z * de.z, gc.w * de.w);
+    S.g = make_float4(finite_or0(gc.x * de.x), finite_or0(gc.y * de.y), finite_or0(gc.z * de.z),
+                      finite_or0(gc.w * de.w));
     // uv and its screen derivatives (interpolate.cu:20-49)
     const float4 d = a.db[p];
     const double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
@@ -418,31 +423,42 @@ __global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n = *rec.count;
     const int nchunks = (n + 31) >> 5, stride = gridDim.x * nwarps;
-    int c = blockIdx.x * nwarps + wid;
-    float4 ra = z4, rb = z4, rc = z4, rg = z4;
-    uint32_t pnext = 0;
-    if (c < nchunks && c * 32 + lane < n) {
-        const int k = c * 32 + lane;
-        ra = rec.nss[k]; rb = rec.psa[k]; rc = rec.dfs[k]; rg = g_color[rec.pix[k]];
-    }
-    if (c + stride < nchunks && (c + stride) * 32 + lane < n) pnext = rec.pix[(c + stride) * 32 + lane];
-    for (; c < nchunks; c += stride) {
-        const int m = min(32, n - c * 32);
-        if (lane < m) spair_put(st + (lane >> 1), lane & 1, ra, rb, rc, rg);
-        if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
-        if (c + stride < nchunks) {
-            const int k1 = (c + stride) * 32 + lane;
-            if (k1 < n) { ra = rec.nss[k1]; rb = rec.psa[k1]; rc = rec.dfs[k1]; rg = g_color[pnext]; }
+    // Pass 0 adds every contribution plainly.  A lane whose sums come out
+    // non-finite met a non-finite contribution; its warp then walks the same
+    // chunks again and that lane alone adds them checked (pass 1).
+    bool guard = false;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        int c = blockIdx.x * nwarps + wid;
+        float4 ra = z4, rb = z4, rc = z4, rg = z4;
+        uint32_t pnext = 0;
+        if (c < nchunks && c * 32 + lane < n) {
+            const int k = c * 32 + lane;
+            ra = rec.nss[k]; rb = rec.psa[k]; rc = rec.dfs[k]; rg = g_color[rec.pix[k]];
         }
-        if (c + 2 * stride < nchunks) {
-            const int k2 = (c + 2 * stride) * 32 + lane;
-            if (k2 < n) pnext = rec.pix[k2];
+        if (c + stride < nchunks && (c + stride) * 32 + lane < n) pnext = rec.pix[(c + stride) * 32 + lane];
+        for (; c < nchunks; c += stride) {
+            const int m = min(32, n - c * 32);
+            if (lane < m) spair_put(st + (lane >> 1), lane & 1, ra, rb, rc, rg);
+            if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
+            if (c + stride < nchunks) {
+                const int k1 = (c + stride) * 32 + lane;
+                if (k1 < n) { ra = rec.nss[k1]; rb = rec.psa[k1]; rc = rec.dfs[k1]; rg = g_color[pnext]; }
+            }
+            if (c + 2 * stride < nchunks) {
+                const int k2 = (c + 2 * stride) * 32 + lane;
+                if (k2 < n) pnext = rec.pix[k2];
+            }
+            __syncwarp();
+            const int npair = (m + 1) >> 1;
+            if (L.valid && (pass == 0 || guard))
+                for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j], pass != 0);
+            __syncwarp();
         }
-        __syncwarp();
-        const int npair = (m + 1) >> 1;
-        if (L.valid)
-            for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j]);
-        __syncwarp();
+        if (pass == 1) break;
+        guard = lobe4x2_needs_guard(L);
+        if (!__any_sync(0xffffffffu, guard)) break;
+        if (guard) lobe4x2_clear(L);
     }
     lobe4x2_flush(L, li, Kp, s_acc);
     __syncthreads();
@@ -1053,8 +1069,11 @@ vcl_status fit_fused_raster_schedule(vcl_fit* f, int* tile, int* small_area, lon
     return VCL_OK;
 }
 
-const char* const kFusedKernelNames[] = {"raster", "shade_fwd", "aa_fwd_mse", "aa_bwd", "bwd_pix", "sg_lobes"};
-constexpr int kFusedKernels = 6;
+// The six stages alone, then the per-pixel backward and the lobe gradients
+// together as the step runs them (forked stream, joined).
+const char* const kFusedKernelNames[] = {"raster", "shade_fwd", "aa_fwd_mse", "aa_bwd", "bwd_pix", "sg_lobes",
+                                         "bwd_pix+sg_lobes"};
+constexpr int kFusedKernels = 7;
 
 int fit_fused_kernel_count() { return kFusedKernels; }
 const char* fit_fused_kernel_name(int i) { return i >= 0 && i < kFusedKernels ? kFusedKernelNames[i] : nullptr; }
@@ -1087,7 +1106,17 @@ vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* m
                 case 3: return aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
                                             f->g_color, d.learn_pos ? f->g_clip : nullptr, s);
                 case 4: return stage_bwd_pix(f, a, td, s);
-                default: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;
+                case 5: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;
+                default: {
+                    if (!(d.learn_lobes && d.K)) return stage_bwd_pix(f, a, td, s);
+                    vcl_status r = vcl_cuda_check(ctx, cudaEventRecord(F->fork, s), "fork");
+                    if (r == VCL_OK) r = vcl_cuda_check(ctx, cudaStreamWaitEvent(F->side, F->fork, 0), "fork");
+                    if (r == VCL_OK) r = stage_lobes(f, a, td, F->side);
+                    if (r == VCL_OK) r = vcl_cuda_check(ctx, cudaEventRecord(F->join, F->side), "join");
+                    if (r == VCL_OK) r = stage_bwd_pix(f, a, td, s);
+                    if (r == VCL_OK) r = vcl_cuda_check(ctx, cudaStreamWaitEvent(s, F->join, 0), "join");
+                    return r;
+                }
             }
         };
         st = run();

@@ -685,28 +685,31 @@ struct __align__(16) SPair {
     float2 sa, nssl;         // sa, -ss log2 e
     float2 dn2, sn2;         // |2.133 n|^2, |ss p|^2
     float2 gx, gy, gz, gw;   // dL/dout
-    float2 hx, hy, hz, hw;   // dL/dout * diffuse
+    float2 hx, hy, hz, hw;   // dL/dout * diffuse * 2.34
 };
 constexpr int SPAIR_FIELDS = (int)(sizeof(SPair) / sizeof(float2));
 
 // Writes one pixel into half `h` of a staged pair from its shading record
 // (nss = (n, ss), psa = (p, sa), the diffuse texture colour dfs) and its
-// dL/dout.  All-zero inputs pad an odd count: a zero pixel adds exactly
-// nothing to any sum.
+// dL/dout.  The diffuse environment amplitude 2.34 rides on dL/dout *
+// diffuse, the only per-pixel factor every diffuse term carries.  All-zero
+// inputs pad an odd count: a zero pixel adds exactly nothing to any sum.
 DEV void spair_put(SPair* s, int h, float4 nss, float4 psa, float4 dfs, float4 go) {
     const float3 dn = f3(nss.x, nss.y, nss.z) * SG_DIFF_SHARP, sn = f3(psa.x, psa.y, psa.z) * nss.w;
     const float v[SPAIR_FIELDS] = {dn.x, dn.y, dn.z, sn.x, sn.y, sn.z, psa.w, -(nss.w * SG_L2E), dot3(dn, dn),
-                                   dot3(sn, sn), go.x, go.y, go.z, go.w, go.x * dfs.x, go.y * dfs.y, go.z * dfs.z,
-                                   go.w * dfs.w};
+                                   dot3(sn, sn), go.x, go.y, go.z, go.w, go.x * dfs.x * SG_DIFF_AMP,
+                                   go.y * dfs.y * SG_DIFF_AMP, go.z * dfs.z * SG_DIFF_AMP, go.w * dfs.w * SG_DIFF_AMP};
     float* f = reinterpret_cast<float*>(s) + h;
 #pragma unroll
     for (int i = 0; i < SPAIR_FIELDS; ++i) f[2 * i] = v[i];
 }
 
 // One lane's lobe (C = 4): its constants broadcast to both halves and its
-// gradient sums per half.  The axis gradient sum_p c1 (u_d + s a) + c2 (u_s + s a)
-// is kept as ax = sum (c1 u_d + c2 u_s) plus axs = sum (c1 + c2), combined with
-// s a when the lane flushes.
+// gradient sums per half.  Every axis term carries the lobe's sharpness s
+// (d|v|/da = s v/|v| for v = u + s a), so the sums leave it out and the
+// flush multiplies it back in; the axis sum
+// sum_p c1 (u_d + s a) + c2 (u_s + s a) is kept as ax = sum (c1 u_d + c2 u_s)
+// plus axs = sum (c1 + c2), combined with s a when the lane flushes.
 struct Lobe4x2 {
     bool valid;
     float3 sgn;                  // s a (scalar, for the flush)
@@ -716,6 +719,10 @@ struct Lobe4x2 {
     float2 ax4, ay4, az4, aw4;   // amplitude
     float2 gax, gay, gaz, gaxs, gsh, gam0, gam1, gam2, gam3;   // sums
 };
+
+DEV void lobe4x2_clear(Lobe4x2& L) {
+    L.gax = L.gay = L.gaz = L.gaxs = L.gsh = L.gam0 = L.gam1 = L.gam2 = L.gam3 = p2(0.f);
+}
 
 DEV void lobe4x2_load(Lobe4x2& L, int i, int K, const float* axis, const float* sharp, const float* amp) {
     L.valid = i < K;
@@ -732,22 +739,22 @@ DEV void lobe4x2_load(Lobe4x2& L, int i, int K, const float* axis, const float* 
     const float4 am = K ? make_float4(amp[4 * ii], amp[4 * ii + 1], amp[4 * ii + 2], amp[4 * ii + 3])
                         : make_float4(0.f, 0.f, 0.f, 0.f);
     L.ax4 = p2(am.x); L.ay4 = p2(am.y); L.az4 = p2(am.z); L.aw4 = p2(am.w);
-    L.gax = L.gay = L.gaz = L.gaxs = L.gsh = L.gam0 = L.gam1 = L.gam2 = L.gam3 = p2(0.f);
+    lobe4x2_clear(L);
 }
 
-// One half's contributions with each checked (the reference's guarded adds,
-// common.h:181): the rare path when some contribution is not finite.
+// One half's contributions, each added only when finite (the reference's
+// guarded adds, common.h:181, material.cu:428-437): the amplitude per
+// channel, the axis terms when both lobe factors (with s) are finite, the
+// sharpness term when finite.
 DEV void lobe4x2_guarded(float& am0, float& am1, float& am2, float& am3, float& ax, float& ay, float& az, float& axs,
-                         float& sh, float dg, float sgv, float c1, float c2, float shc, float dnx, float dny, float dnz,
-                         float snx, float sny, float snz, float gx, float gy, float gz, float gw, float hx, float hy,
-                         float hz, float hw) {
-    if (isfinite(dg) && isfinite(sgv)) {
-        am0 = fmaf(sgv, gx, fmaf(dg, hx, am0));
-        am1 = fmaf(sgv, gy, fmaf(dg, hy, am1));
-        am2 = fmaf(sgv, gz, fmaf(dg, hz, am2));
-        am3 = fmaf(sgv, gw, fmaf(dg, hw, am3));
-    }
-    if (isfinite(c1) && isfinite(c2)) {
+                         float& sh, float s, float dg, float sgv, float c1, float c2, float shc, float dnx, float dny,
+                         float dnz, float snx, float sny, float snz, float gx, float gy, float gz, float gw, float hx,
+                         float hy, float hz, float hw) {
+    am0 += finite_or0(fmaf(sgv, gx, dg * hx));
+    am1 += finite_or0(fmaf(sgv, gy, dg * hy));
+    am2 += finite_or0(fmaf(sgv, gz, dg * hz));
+    am3 += finite_or0(fmaf(sgv, gw, dg * hw));
+    if (isfinite(c1 * s) && isfinite(c2 * s)) {
         ax = fmaf(c2, snx, fmaf(c1, dnx, ax));
         ay = fmaf(c2, sny, fmaf(c1, dny, ay));
         az = fmaf(c2, snz, fmaf(c1, dnz, az));
@@ -763,11 +770,11 @@ DEV void lobe4x2_guarded(float& am0, float& am1, float& am2, float& am3, float& 
 // exponentials, Dm = e- - e+ and T = (e- + e+) - il Dm:  value = Dm il,
 // (d value/d|v|)/|v| = T il^2,  d value/ds = il (dotn T - Dm)  (the
 // reference's ((dotn (1-il) - 1) e- + (dotn (1+il) + 1) e+) il, expanded).
-// The reference's guarded adds (common.h:181) drop a non-finite
-// contribution; when a pixel's contributions sum to a finite value they are
-// all finite and are added plainly, else each is checked.
+// guard = false adds every contribution plainly (the walk's first pass);
+// guard = true checks each one (the pass that redoes a lane whose plain sums
+// came out non-finite).
 template <bool EXACT>
-DEV void lobe4x2_accumulate(Lobe4x2& L, const SPair& P) {
+DEV void lobe4x2_accumulate(Lobe4x2& L, const SPair& P, bool guard) {
     // diffuse lobe
     const float2 dd = fma2(L.sz, P.dnz, fma2(L.sy, P.dny, mul2(L.sx, P.dnx)));
     float2 dl, dil;
@@ -786,20 +793,18 @@ DEV void lobe4x2_accumulate(Lobe4x2& L, const SPair& P) {
     em = ex2_2(fma2(sl, p2(SG_L2E), nc));
     ep = ex2_2(fma2(sl, p2(-SG_L2E), nc));
     const float2 sDm = sub2(em, ep), sT = fma2(neg2(sil), sDm, add2(em, ep));
-    // channel sums
+    // channel sums (h carries the diffuse amplitude 2.34)
     const float2 sum = fma2(P.gw, L.aw4, fma2(P.gz, L.az4, fma2(P.gy, L.ay4, mul2(P.gx, L.ax4))));
     const float2 sumd = fma2(P.hw, L.aw4, fma2(P.hz, L.az4, fma2(P.hy, L.ay4, mul2(P.hx, L.ax4))));
-    const float2 dilA = mul2(dil, p2(SG_DIFF_AMP));
-    const float2 dg = mul2(dDm, dilA);                        // diffuse value
-    const float2 sdA = mul2(sumd, dilA);
-    const float2 c1 = mul2(mul2(sdA, mul2(dT, dil)), L.gs);   // sumd T il^2 2.34 s
+    const float2 dg = mul2(dDm, dil);                         // diffuse value / 2.34
+    const float2 sdA = mul2(sumd, dil);
+    const float2 c1 = mul2(sdA, mul2(dT, dil));               // sumd T il^2 2.34 (s in the flush)
     const float2 sils = mul2(sil, P.sa);
     const float2 sgv = mul2(sDm, sils);                       // specular value
     const float2 ssa = mul2(sum, sils);
-    const float2 c2 = mul2(mul2(ssa, mul2(sT, sil)), L.gs);   // sum T il^2 sa s
+    const float2 c2 = mul2(ssa, mul2(sT, sil));               // sum T il^2 sa (s in the flush)
     const float2 shc = fma2(sdA, fma2(dotn, dT, neg2(dDm)), mul2(ssa, fma2(dots, sT, neg2(sDm))));
-    const float2 t = add2(add2(add2(dg, sgv), add2(c1, c2)), shc);
-    if (isfinite(t.x) && isfinite(t.y)) {
+    if (!guard) {
         L.gam0 = fma2(sgv, P.gx, fma2(dg, P.hx, L.gam0));
         L.gam1 = fma2(sgv, P.gy, fma2(dg, P.hy, L.gam1));
         L.gam2 = fma2(sgv, P.gz, fma2(dg, P.hz, L.gam2));
@@ -811,28 +816,55 @@ DEV void lobe4x2_accumulate(Lobe4x2& L, const SPair& P) {
         L.gsh = add2(L.gsh, shc);
         return;
     }
-    lobe4x2_guarded(L.gam0.x, L.gam1.x, L.gam2.x, L.gam3.x, L.gax.x, L.gay.x, L.gaz.x, L.gaxs.x, L.gsh.x, dg.x, sgv.x,
-                    c1.x, c2.x, shc.x, P.dnx.x, P.dny.x, P.dnz.x, P.snx.x, P.sny.x, P.snz.x, P.gx.x, P.gy.x, P.gz.x,
-                    P.gw.x, P.hx.x, P.hy.x, P.hz.x, P.hw.x);
-    lobe4x2_guarded(L.gam0.y, L.gam1.y, L.gam2.y, L.gam3.y, L.gax.y, L.gay.y, L.gaz.y, L.gaxs.y, L.gsh.y, dg.y, sgv.y,
-                    c1.y, c2.y, shc.y, P.dnx.y, P.dny.y, P.dnz.y, P.snx.y, P.sny.y, P.snz.y, P.gx.y, P.gy.y, P.gz.y,
-                    P.gw.y, P.hx.y, P.hy.y, P.hz.y, P.hw.y);
+    lobe4x2_guarded(L.gam0.x, L.gam1.x, L.gam2.x, L.gam3.x, L.gax.x, L.gay.x, L.gaz.x, L.gaxs.x, L.gsh.x, L.gs.x, dg.x,
+                    sgv.x, c1.x, c2.x, shc.x, P.dnx.x, P.dny.x, P.dnz.x, P.snx.x, P.sny.x, P.snz.x, P.gx.x, P.gy.x,
+                    P.gz.x, P.gw.x, P.hx.x, P.hy.x, P.hz.x, P.hw.x);
+    lobe4x2_guarded(L.gam0.y, L.gam1.y, L.gam2.y, L.gam3.y, L.gax.y, L.gay.y, L.gaz.y, L.gaxs.y, L.gsh.y, L.gs.y, dg.y,
+                    sgv.y, c1.y, c2.y, shc.y, P.dnx.y, P.dny.y, P.dnz.y, P.snx.y, P.sny.y, P.snz.y, P.gx.y, P.gy.y,
+                    P.gz.y, P.gw.y, P.hx.y, P.hy.y, P.hz.y, P.hw.y);
 }
 
-// Folds the two halves and the lobe groups of the warp together and adds the
-// lane's sums into the block accumulator s_acc [K][8] (axis xyz, sharpness,
-// amplitude[4]).
-DEV void lobe4x2_flush(Lobe4x2& L, int i, int Kp, float* s_acc) {
-    const float axs = L.gaxs.x + L.gaxs.y;
-    float v[8] = {fmaf(axs, L.sgn.x, L.gax.x + L.gax.y), fmaf(axs, L.sgn.y, L.gay.x + L.gay.y),
-                  fmaf(axs, L.sgn.z, L.gaz.x + L.gaz.y), L.gsh.x + L.gsh.y, L.gam0.x + L.gam0.y,
-                  L.gam1.x + L.gam1.y, L.gam2.x + L.gam2.y, L.gam3.x + L.gam3.y};
+// The lane's eight totals (axis xyz, sharpness, amplitude[4]), both halves
+// folded together and the axis sums multiplied by s.
+DEV void lobe4x2_values(const Lobe4x2& L, float v[8]) {
+    const float s = L.gs.x, axs = L.gaxs.x + L.gaxs.y;
+    v[0] = s * fmaf(axs, L.sgn.x, L.gax.x + L.gax.y);
+    v[1] = s * fmaf(axs, L.sgn.y, L.gay.x + L.gay.y);
+    v[2] = s * fmaf(axs, L.sgn.z, L.gaz.x + L.gaz.y);
+    v[3] = L.gsh.x + L.gsh.y;
+    v[4] = L.gam0.x + L.gam0.y;
+    v[5] = L.gam1.x + L.gam1.y;
+    v[6] = L.gam2.x + L.gam2.y;
+    v[7] = L.gam3.x + L.gam3.y;
+}
+
+// True when the lane has to walk its pixels again with every contribution
+// checked: its plain sums are not all finite, which happens exactly when
+// some contribution was not finite (or a sum overflowed).
+DEV bool lobe4x2_needs_guard(const Lobe4x2& L) {
+    if (!L.valid) return false;
+    float v[8];
+    lobe4x2_values(L, v);
+    bool ok = true;
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+    for (int q = 0; q < 8; ++q) ok = ok && isfinite(v[q]);
+    return !ok;
+}
+
+// Folds the lobe groups of the warp together and adds the lane's totals into
+// the block accumulator s_acc [K][8] (axis xyz, sharpness, amplitude[4]); a
+// total that is not finite is dropped, as the reference's guarded add of it.
+DEV void lobe4x2_flush(const Lobe4x2& L, int i, int Kp, float* s_acc) {
+    float v[8];
+    lobe4x2_values(L, v);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        v[q] = finite_or0(v[q]);
         for (int o = 16; o >= Kp; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
     const int lane = threadIdx.x & 31;
     if (lane < Kp && L.valid) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) atomicAdd(&s_acc[(size_t)i * 8 + q], v[q]);
+        for (int q = 0; q < 8; ++q) atomicAdd(&s_acc[(size_t)i * 8 + q], finite_or0(v[q]));
     }
 }

@@ -344,24 +344,34 @@ __global__ void __launch_bounds__(128, 4) k_sg_lobes_op(int K, const float* __re
     SPair* st = s_pix + wid * 16;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const long long nchunks = (npix + 31) / 32;
-    for (long long c = (long long)blockIdx.x * nwarps + wid; c < nchunks; c += (long long)gridDim.x * nwarps) {
-        const long long p = c * 32 + lane;
-        const bool live = p < npix && rast_id(rast[p].w) >= 0;
-        const unsigned ball = __ballot_sync(0xffffffffu, live);
-        const int m = __popc(ball);
-        if (m == 0) continue;
-        if (live) {
-            const int k = __popc(ball & ((1u << lane) - 1u));
-            const float3 n = ld3(normal, p), pa = ld3(sax, p);
-            spair_put(st + (k >> 1), k & 1, make_float4(n.x, n.y, n.z, ssh[p]), make_float4(pa.x, pa.y, pa.z, sam[p]),
-                      diffuse[p], gout[p]);
+    // Plain pass, then a checked pass for lanes whose sums are not finite
+    // (as in the fused step's lobe-gradient kernel).
+    bool guard = false;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+        for (long long c = (long long)blockIdx.x * nwarps + wid; c < nchunks; c += (long long)gridDim.x * nwarps) {
+            const long long p = c * 32 + lane;
+            const bool live = p < npix && rast_id(rast[p].w) >= 0;
+            const unsigned ball = __ballot_sync(0xffffffffu, live);
+            const int m = __popc(ball);
+            if (m == 0) continue;
+            if (live) {
+                const int k = __popc(ball & ((1u << lane) - 1u));
+                const float3 n = ld3(normal, p), pa = ld3(sax, p);
+                spair_put(st + (k >> 1), k & 1, make_float4(n.x, n.y, n.z, ssh[p]),
+                          make_float4(pa.x, pa.y, pa.z, sam[p]), diffuse[p], gout[p]);
+            }
+            if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
+            __syncwarp();
+            const int npair = (m + 1) >> 1;
+            if (L.valid && (pass == 0 || guard))
+                for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j], pass != 0);
+            __syncwarp();
         }
-        if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
-        __syncwarp();
-        const int npair = (m + 1) >> 1;
-        if (L.valid)
-            for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j]);
-        __syncwarp();
+        if (pass == 1) break;
+        guard = lobe4x2_needs_guard(L);
+        if (!__any_sync(0xffffffffu, guard)) break;
+        if (guard) lobe4x2_clear(L);
     }
     lobe4x2_flush(L, li, Kp, s_acc);
     __syncthreads();
