@@ -107,3 +107,14 @@ DEV void red_add2(float* p, float a, float b) {
 
 // Triangle id of a raster texel (u, v, z/w, id+1); -1 for background.
 DEV int rast_id(float w) { return (int)w - 1; }
+
+// Asynchronous 16-byte global -> shared copies (sm_80+ cp.async, L2 only):
+// a thread's copies land in the order of its commit groups; wait_group N
+// returns once at most N of the thread's groups are still in flight.
+DEV void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }

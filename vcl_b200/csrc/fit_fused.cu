@@ -347,10 +347,10 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // each run of consecutive lanes on the same triangle (a segmented scan by
 // shuffles, as many rounds as the longest run needs) and the last lane of a
 // run issues its three vector reductions: neighbouring pixels of one
-// triangle no longer collide on the same three addresses.  Held to 40
-// registers in blocks of 128 threads so that its blocks fit, at a fine
-// grain, on the SMs beside the lobe-gradient blocks it runs with.
-__global__ void __launch_bounds__(128, 12) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+// triangle no longer collide on the same three addresses.  Blocks of 128
+// threads at up to 64 registers (no spills), so that its blocks fit, at a
+// fine grain, on the SMs beside the lobe-gradient blocks it runs with.
+__global__ void __launch_bounds__(128, 8) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
                                                  int want_tex, int want_geom) {
@@ -401,16 +401,20 @@ __global__ void __launch_bounds__(128, 12) k_bwd_pix(ShadeIn a, TexDesc td, cons
 // lobe on paired FP32 instructions; sums stay in registers until the end.
 // Block row blockIdx.y takes lobes [32 y, 32 y + 32) (fewer than 32 lobes:
 // the warp splits into 32 / Kp groups of Kp lanes that walk alternate
-// pairs).  The next chunk's records and dL/dout are loaded while the current
-// one is consumed (its pixel indices one chunk earlier still).  At most 112
-// registers: three blocks of this kernel and two of the per-pixel backward
-// fit on an SM together.  C = 4.
+// pairs).  Once a chunk is staged, the next chunk's records and dL/dout
+// are copied into shared memory asynchronously (cp.async, one buffer per
+// warp) while the current one is consumed, their pixel indices loaded one
+// chunk earlier still, so no registers hold data in flight.  At most LOBE_REGS registers, so
+// that three blocks of this kernel and the per-pixel backward's blocks share
+// each SM.  C = 4.
+constexpr int LOBE_REGS = 112;
 template <bool EXACT>
-__global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
-                                                     float* __restrict__ g_axis, float* __restrict__ g_sharp,
-                                                     float* __restrict__ g_amp) {
+__global__ void __maxnreg__(LOBE_REGS) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
+                                                 float* __restrict__ g_axis, float* __restrict__ g_sharp,
+                                                 float* __restrict__ g_amp) {
     __shared__ float s_acc[32 * 8];                                  // [lobe][axis xyz, sharpness, amplitude 4]
     __shared__ SPair s_pix[4 * 16];
+    __shared__ float4 s_raw[4][4][32];                               // [warp][nss, psa, dfs, dL/dout][lane]
     const int nwarps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int base = 32 * blockIdx.y, Kg = min(32, a.K - base);
     for (int i = threadIdx.x; i < 32 * 8; i += blockDim.x) s_acc[i] = 0.f;
@@ -420,9 +424,21 @@ __global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float
     Lobe4x2 L;
     lobe4x2_load(L, li, Kg, a.axis + 3 * base, a.sharp + base, a.amp + 4 * base);
     SPair* st = s_pix + wid * 16;
+    float4 (*raw)[32] = s_raw[wid];
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const int n = *rec.count;
     const int nchunks = (n + 31) >> 5, stride = gridDim.x * nwarps;
+    // copies of chunk cc (this lane's record and dL/dout at pixel pix)
+    auto issue = [&](int cc, uint32_t pix) {
+        const int k = cc * 32 + lane;
+        if (cc < nchunks && k < n) {
+            cp_async16(&raw[0][lane], rec.nss + k);
+            cp_async16(&raw[1][lane], rec.psa + k);
+            cp_async16(&raw[2][lane], rec.dfs + k);
+            cp_async16(&raw[3][lane], g_color + pix);
+        }
+        cp_async_commit();
+    };
     // Pass 0 adds every contribution plainly.  A lane whose sums come out
     // non-finite met a non-finite contribution; its warp then walks the same
     // chunks again and that lane alone adds them checked (pass 1).
@@ -430,31 +446,27 @@ __global__ void __maxnreg__(112) k_sg_lobes(ShadeIn a, ShadeRec rec, const float
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
         int c = blockIdx.x * nwarps + wid;
-        float4 ra = z4, rb = z4, rc = z4, rg = z4;
-        uint32_t pnext = 0;
-        if (c < nchunks && c * 32 + lane < n) {
-            const int k = c * 32 + lane;
-            ra = rec.nss[k]; rb = rec.psa[k]; rc = rec.dfs[k]; rg = g_color[rec.pix[k]];
-        }
-        if (c + stride < nchunks && (c + stride) * 32 + lane < n) pnext = rec.pix[(c + stride) * 32 + lane];
+        issue(c, (c < nchunks && c * 32 + lane < n) ? rec.pix[c * 32 + lane] : 0u);
+        uint32_t pnext = (c + stride < nchunks && (c + stride) * 32 + lane < n) ? rec.pix[(c + stride) * 32 + lane] : 0u;
         for (; c < nchunks; c += stride) {
             const int m = min(32, n - c * 32);
-            if (lane < m) spair_put(st + (lane >> 1), lane & 1, ra, rb, rc, rg);
+            cp_async_wait<0>();                                      // this chunk's copies (this lane's own)
+            if (lane < m) spair_put(st + (lane >> 1), lane & 1, raw[0][lane], raw[1][lane], raw[2][lane], raw[3][lane]);
             if ((m & 1) && lane == 31) spair_put(st + (m >> 1), 1, z4, z4, z4, z4);
-            if (c + stride < nchunks) {
-                const int k1 = (c + stride) * 32 + lane;
-                if (k1 < n) { ra = rec.nss[k1]; rb = rec.psa[k1]; rc = rec.dfs[k1]; rg = g_color[pnext]; }
-            }
+            __syncwarp();
+            // the staged pair stores consumed this lane's copies: the buffer
+            // takes the next chunk's
+            issue(c + stride, pnext);
             if (c + 2 * stride < nchunks) {
                 const int k2 = (c + 2 * stride) * 32 + lane;
                 if (k2 < n) pnext = rec.pix[k2];
             }
-            __syncwarp();
             const int npair = (m + 1) >> 1;
             if (L.valid && (pass == 0 || guard))
                 for (int j = g; j < npair; j += G) lobe4x2_accumulate<EXACT>(L, st[j], pass != 0);
             __syncwarp();
         }
+        cp_async_wait<0>();
         if (pass == 1) break;
         guard = lobe4x2_needs_guard(L);
         if (!__any_sync(0xffffffffu, guard)) break;
