@@ -77,6 +77,7 @@ struct ShadeIn {
 struct PixIn {
     float2 uv; float4 uvda; float4 dfs; float3 n, pax; float ss, sa;
     uint32_t i0, i1, i2; float4 r;
+    float fl; int lv;    // trilinear fraction, levels l0 | l1 << 8
 };
 
 // Shading records of the covered pixels, written by k_shade_fwd and read by
@@ -88,6 +89,10 @@ struct PixIn {
 struct ShadeRec {
     float4* nss; float4* psa; float4* dfs; uint32_t* pix;
     int* count;          // records written this step (reset before the shading pass)
+    // Per pixel (not compacted), for the per-pixel backward: the texture
+    // sample (u, v, level fraction, l0 | l1 << 8 as int bits) of each covered
+    // pixel, so that its texel loads need not wait on triangle -> attributes.
+    float4* tsr;
 };
 
 template <int C4>
@@ -117,6 +122,8 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
     int l0 = 0, l1 = 0;
     float fl = 0.f;
     if (td.L > 1) calc_level(td, o.uvda, l0, l1, fl, nullptr, 0);
+    o.fl = fl;
+    o.lv = l0 | l1 << 8;
     int q0[4];
     float2 f0;
     index_fetch(td, l0, o.uv, q0, f0);
@@ -187,6 +194,7 @@ __global__ void __launch_bounds__(128, 12) k_shade_fwd(ShadeIn a, TexDesc td, fl
         color[p] = diffenv[p] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
+    if (rec.tsr) rec.tsr[p] = make_float4(q.uv.x, q.uv.y, q.fl, __int_as_float(q.lv));
     if (rec.count) {
         const int k = s_base + s_off[wid] + __popc(ball & ((1u << lane) - 1u));
         rec.nss[k] = make_float4(q.n.x, q.n.y, q.n.z, q.ss);
@@ -229,7 +237,7 @@ struct PixSample {
 };
 
 DEV void pix_sample(const ShadeIn& a, const TexDesc& td, const float4* __restrict__ g_color,
-                    const float4* __restrict__ diffenv, long long p, PixSample& S) {
+                    const float4* __restrict__ diffenv, const float4* __restrict__ tsr, long long p, PixSample& S) {
     S.ok = false;
     const float4 r = a.rast[p];
     const int idx = rast_id(r.w);
@@ -243,22 +251,12 @@ DEV void pix_sample(const ShadeIn& a, const TexDesc& td, const float4* __restric
     const float4 gc = g_color[p], de = diffenv[p];
     S.g = make_float4(finite_or0(gc.x * de.x), finite_or0(gc.y * de.y), finite_or0(gc.z * de.z),
                       finite_or0(gc.w * de.w));
-    // uv and its screen derivatives (interpolate.cu:20-49)
-    const float4 d = a.db[p];
-    const double l2 = __dsub_rn(__dsub_rn(1.0, (double)r.x), (double)r.y);
-    float u[2], dx[2], dy[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        float a0 = a.uvattr[2 * i0 + i], a1 = a.uvattr[2 * i1 + i], a2 = a.uvattr[2 * i2 + i];
-        u[i] = (float)__dadd_rn((double)addr(mulr(a0, r.x), mulr(a1, r.y)), __dmul_rn((double)a2, l2));
-        float dadu = a0 - a2, dadv = a1 - a2;
-        dx[i] = addr(mulr(dadu, d.x), mulr(dadv, d.z));
-        dy[i] = addr(mulr(dadu, d.y), mulr(dadv, d.w));
-    }
-    const float2 uv = make_float2(u[0], u[1]);
-    S.l0 = 0; S.l1 = 0; S.fl = 0.f;
+    // the texture sample the shading pass took at this pixel (texturemap.cu:67-95)
+    const float4 t = tsr[p];
+    const float2 uv = make_float2(t.x, t.y);
+    const int lv = __float_as_int(t.w);
+    S.l0 = lv & 255; S.l1 = lv >> 8; S.fl = t.z;
     const bool mip = td.L > 1;
-    if (mip) calc_level(td, make_float4(dx[0], dy[0], dx[1], dy[1]), S.l0, S.l1, S.fl, nullptr, 0);
     cell_fetch(td, S.l0, uv, S.u0, S.u1, S.v0, S.v1, S.f0);
     S.tri = mip && S.fl > 0;
     S.f1 = make_float2(0.f, 0.f);
@@ -351,14 +349,15 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // threads at up to 64 registers (no spills), so that its blocks fit, at a
 // fine grain, on the SMs beside the lobe-gradient blocks it runs with.
 __global__ void __launch_bounds__(128, 8) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
-                                                 const float4* __restrict__ diffenv, float* __restrict__ g_pyr,
+                                                 const float4* __restrict__ diffenv, const float4* __restrict__ tsr,
+                                                 float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
                                                  int want_tex, int want_geom) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     PixSample S;
     S.ok = false;
-    if (p < a.npix) pix_sample(a, td, g_color, diffenv, p, S);
+    if (p < a.npix) pix_sample(a, td, g_color, diffenv, tsr, p, S);
     if (want_tex && S.ok) {
         const float wl0 = td.L > 1 ? 1.f - S.fl : 1.f;
         const float2 f0 = S.f0;
@@ -620,6 +619,7 @@ vcl_status fused_init(vcl_fit* f) {
     VCL_REQUIRE(N <= (size_t)INT32_MAX - (1u << 24), "fused strategy: W*H*views = %zu pixels, above 2^31 - 2^24", N);
     VCL_REQUIRE((size_t)((const char*)(f->sam + N) - (const char*)f->normal) >= (2 * sizeof(float4) + 4) * N &&
                     f->normal < f->sam && ((uintptr_t)f->normal & 15) == 0 && ((uintptr_t)f->uv_da & 15) == 0 &&
+                    ((uintptr_t)f->g_diffuse & 15) == 0 &&
                     (f->rough < f->normal || f->rough >= f->sam + N),
                 "fused strategy: shading record area too small (internal layout error)");
     Fused* F = new Fused();
@@ -827,7 +827,8 @@ ShadeIn shade_in(const vcl_fit* f) {
 // The fused step does not use the plain strategy's per-pixel intermediates,
 // so its shading records live there: the stretch from `normal` to the end of
 // `sam` (11 floats per pixel, checked in fused_init) holds (n, ss), (p, sa)
-// and the pixel indices, `uv_da` (4 floats per pixel) the diffuse colours.
+// and the pixel indices, `uv_da` (4 floats per pixel) the diffuse colours,
+// `g_diffuse` (C = 4 floats per pixel) the texture samples.
 ShadeRec shade_rec(const vcl_fit* f, bool want) {
     const size_t N = (size_t)f->d.W * f->d.H * f->d.views;
     float4* r = reinterpret_cast<float4*>(f->normal);
@@ -836,6 +837,7 @@ ShadeRec shade_rec(const vcl_fit* f, bool want) {
     x.pix = reinterpret_cast<uint32_t*>(r + 2 * N);
     x.dfs = reinterpret_cast<float4*>(f->uv_da);
     x.count = want ? ((Fused*)f->fused)->d_step + 8 : nullptr;
+    x.tsr = (f->d.learn_tex || f->d.learn_pos) ? reinterpret_cast<float4*>(f->g_diffuse) : nullptr;
     return x;
 }
 
@@ -881,7 +883,8 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
 vcl_status stage_bwd_pix(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
     const vcl_fit_desc& d = f->d;
     k_bwd_pix<<<vcl_blocks(a.npix, 128), 128, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
-                                                      f->g_pyr, f->clip, f->g_clip, d.learn_tex, d.learn_pos);
+                                                      shade_rec(f, false).tsr, f->g_pyr, f->clip, f->g_clip,
+                                                      d.learn_tex, d.learn_pos);
     return vcl_launch_check(f->ctx, "fused backward");
 }
 
