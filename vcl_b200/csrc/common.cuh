@@ -108,6 +108,21 @@ DEV void red_add2(float* p, float a, float b) {
 // Triangle id of a raster texel (u, v, z/w, id+1); -1 for background.
 DEV int rast_id(float w) { return (int)w - 1; }
 
+// n / d for 32-bit n by one multiply-high with m = floor((2^64 - 1) / d) + 1
+// (exact for every 32-bit n when d >= 2; m = 0 stands for d = 1): Lemire,
+// Kaser and Kurz, "Faster remainder by direct computation" (2019).  Keeps
+// the per-pixel (view, row, column) split off the conversion / reciprocal
+// unit that an integer division uses.
+struct FastDiv {
+    unsigned long long m;
+};
+inline FastDiv fastdiv_make(unsigned d) {
+    FastDiv f;
+    f.m = d > 1 ? ~0ull / d + 1 : 0ull;
+    return f;
+}
+DEV unsigned fastdiv(unsigned n, FastDiv f) { return f.m ? (unsigned)__umul64hi(f.m, (unsigned long long)n) : n; }
+
 // Asynchronous 16-byte global -> shared copies (sm_80+ cp.async, L2 only):
 // a thread's copies land in the order of its commit groups; wait_group N
 // returns once at most N of the thread's groups are still in flight.

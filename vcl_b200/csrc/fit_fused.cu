@@ -70,6 +70,10 @@ struct ShadeIn {
     const float* pyr; const float* rot; const float* nrm; const float* pvinv;
     int W, H; long long npix; float rough, ior;
     const float* axis; const float* sharp; const float* amp; int K, C;
+    // pixel index -> (view, row, column) by multiply-high (npix < 2^31), and
+    // W, H, 2 / W, 2 / H as floats (exactly what the kernels would compute)
+    FastDiv div_w, div_hw;
+    float fW, fH, xs, ys;
 };
 
 // Everything the SG stage needs at one covered pixel, recomputed from the
@@ -146,12 +150,10 @@ DEV bool shade_inputs(const ShadeIn& a, const TexDesc& td, long long p, PixIn& o
     o.n = f3(R[0] * N.x + R[4] * N.y + R[8] * N.z, R[1] * N.x + R[5] * N.y + R[9] * N.z,
              R[2] * N.x + R[6] * N.y + R[10] * N.z);
     // material.cu:99-107 (ViewAxis)
-    long long hw = (long long)a.W * a.H;
-    int view = (int)(p / hw);
-    int rem = (int)(p - view * hw);
-    int py = rem / a.W, px = rem - py * a.W;
+    const unsigned hw = (unsigned)a.W * (unsigned)a.H, view = fastdiv((unsigned)p, a.div_hw);
+    const unsigned rem = (unsigned)p - view * hw, py = fastdiv(rem, a.div_w), px = rem - py * (unsigned)a.W;
     const float* M = a.pvinv + (size_t)view * 9;
-    float sx = (float)px / (float)a.W * 2.f - 1.f, sy = (float)py / (float)a.H * 2.f - 1.f;
+    float sx = (float)px / a.fW * 2.f - 1.f, sy = (float)py / a.fH * 2.f - 1.f;
     float3 vw = normalize3(f3(M[0], M[1], M[2]) * sx + f3(M[3], M[4], M[5]) * sy + f3(M[6], M[7], M[8]));
     // material.cu:155-182 (SGSpecular)
     SpecLobe s = spec_eval(o.n, vw, a.rough, a.ior);
@@ -317,7 +319,7 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
         gbv += gi * (a.uvattr[2 * S.i1 + i] - a2);
     }
     if (((__float_as_uint(gbu) | __float_as_uint(gbv)) << 1) == 0u) return;
-    const float xs = 2.f / (float)a.W, ys = 2.f / (float)a.H;
+    const float xs = a.xs, ys = a.ys;
     const float pxn = (float)(((double)px + 0.5) * (double)xs - 1.0);
     const float pyn = (float)(((double)py + 0.5) * (double)ys - 1.0);
     const float4* cv = reinterpret_cast<const float4*>(clip) + (size_t)view * a.nv;
@@ -375,9 +377,9 @@ __global__ void __launch_bounds__(128, 8) k_bwd_pix(ShadeIn a, TexDesc td, const
         }
     }
     if (!want_geom) return;
-    const long long hw = (long long)a.W * a.H;
-    const int view = (int)(p / hw), rem = (int)(p - view * hw);
-    const int py = rem / a.W, px = rem - py * a.W;
+    const unsigned hw = (unsigned)a.W * (unsigned)a.H;
+    const int view = (int)fastdiv((unsigned)p, a.div_hw), rem = (int)((unsigned)p - (unsigned)view * hw);
+    const int py = (int)fastdiv((unsigned)rem, a.div_w), px = rem - py * a.W;
     VtxGrad o;
     o.ok = false;
     if (S.ok) pix_geom(a, td, clip, S, px, py, view, o);
@@ -821,6 +823,10 @@ ShadeIn shade_in(const vcl_fit* f) {
     a.nt = d.nt; a.nv = d.nv; a.pyr = f->pyr; a.rot = f->rot; a.nrm = f->nrmattr; a.pvinv = f->pvinv;
     a.W = d.W; a.H = d.H; a.npix = (long long)d.W * d.H * d.views; a.rough = d.roughness; a.ior = d.ior;
     a.axis = f->axis; a.sharp = f->sharp; a.amp = f->amp; a.K = d.K; a.C = 4;
+    a.div_w = fastdiv_make((unsigned)d.W);
+    a.div_hw = fastdiv_make((unsigned)d.W * (unsigned)d.H);
+    a.fW = (float)d.W; a.fH = (float)d.H;
+    a.xs = 2.f / a.fW; a.ys = 2.f / a.fH;
     return a;
 }
 

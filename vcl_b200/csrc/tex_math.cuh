@@ -10,14 +10,18 @@ DEV float t_sub(float a, float b) { return __fsub_rn(a, b); }
 struct TexDesc {
     int tw, th, C, L;
     long long off[16];
+    // level sizes and L - 2, L - 1 as floats (exact), so that the kernels
+    // do not convert them per pixel
+    float fw[16], fh[16];
+    float fL2, fL1;
 };
 
 // texturemap.cu:22-47 (level) and :160-197 (level + Jacobian); the level
 // arithmetic is rounded exactly like the CPU restatement so that the same
 // mip levels are chosen.
 DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, float4* dl, int exact) {
-    float dsdx = t_mul(da.x, (float)t.tw), dsdy = t_mul(da.y, (float)t.tw);
-    float dtdx = t_mul(da.z, (float)t.th), dtdy = t_mul(da.w, (float)t.th);
+    float dsdx = t_mul(da.x, t.fw[0]), dsdy = t_mul(da.y, t.fw[0]);
+    float dtdx = t_mul(da.z, t.fh[0]), dtdy = t_mul(da.w, t.fh[0]);
     float s2 = t_add(t_mul(dsdx, dsdx), t_mul(dsdy, dsdy));
     float t2 = t_add(t_mul(dtdx, dtdx), t_mul(dtdy, dtdy));
     float a = t_sub(t_mul(dsdx, dtdy), t_mul(dtdx, dsdy));
@@ -26,9 +30,9 @@ DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, fl
     float c = sqrtf(c2);
     float level = t_mul(.5f, log2f(t_add(b, c)));
     const int L = t.L;
-    l0 = level <= 0 ? 0 : (float)(L - 2) <= level ? L - 2 : (int)floorf(level);
-    l1 = level <= 1 ? 1 : (float)(L - 1) <= level ? L - 1 : (int)floorf(level) + 1;
-    fl = level <= 0 ? 0.f : (float)(L - 1) <= level ? 1.f : level - floorf(level);
+    l0 = level <= 0 ? 0 : t.fL2 <= level ? L - 2 : (int)floorf(level);
+    l1 = level <= 1 ? 1 : t.fL1 <= level ? L - 1 : (int)floorf(level) + 1;
+    fl = level <= 0 ? 0.f : t.fL1 <= level ? 1.f : level - floorf(level);
     if (dl) {
         float d = b * c + c2;
         if ((double)fabsf(d) > 1e-6) {
@@ -50,14 +54,15 @@ DEV void calc_level(const TexDesc& t, float4 da, int& l0, int& l1, float& fl, fl
 // coordinates (columns u0, u1, rows v0, v1; u1 is u0 or u0 + 1, likewise v1)
 // and the bilinear fractions.
 DEV void cell_fetch(const TexDesc& t, int level, float2 uv, int& u0, int& u1, int& v0, int& v1, float2& f) {
-    int sx = t.tw >> level, sy = t.th >> level;
-    float tx = uv.x * (float)sx, ty = uv.y * (float)sy;
-    u0 = tx < 0 ? 0 : tx > (float)(sx - 1) ? sx - 1 : (int)tx;
-    u1 = tx < 1 ? 0 : tx > (float)(sx - 2) ? sx - 1 : (int)tx + 1;
-    v0 = ty < 0 ? 0 : ty > (float)(sy - 1) ? sy - 1 : (int)ty;
-    v1 = ty < 1 ? 0 : ty > (float)(sy - 2) ? sy - 1 : (int)ty + 1;
-    f.x = tx < 0 ? 0.f : (float)sx < tx ? 1.f : tx - floorf(tx);
-    f.y = ty < 0 ? 0.f : (float)sy < ty ? 1.f : ty - floorf(ty);
+    const int sx = t.tw >> level, sy = t.th >> level;
+    const float fsx = t.fw[level], fsy = t.fh[level];
+    float tx = uv.x * fsx, ty = uv.y * fsy;
+    u0 = tx < 0 ? 0 : tx > fsx - 1.f ? sx - 1 : (int)tx;
+    u1 = tx < 1 ? 0 : tx > fsx - 2.f ? sx - 1 : (int)tx + 1;
+    v0 = ty < 0 ? 0 : ty > fsy - 1.f ? sy - 1 : (int)ty;
+    v1 = ty < 1 ? 0 : ty > fsy - 2.f ? sy - 1 : (int)ty + 1;
+    f.x = tx < 0 ? 0.f : fsx < tx ? 1.f : tx - floorf(tx);
+    f.y = ty < 0 ? 0.f : fsy < ty ? 1.f : ty - floorf(ty);
 }
 
 // The same cell as texel indices within the level.
@@ -87,6 +92,10 @@ inline TexDesc make_desc(int tw, int th, int C, int L) {
     for (int l = 0; l < 16; ++l) {
         d.off[l] = off;
         if (l < L) off += (long long)(tw >> l) * (th >> l) * C;
+        d.fw[l] = (float)(tw >> l);
+        d.fh[l] = (float)(th >> l);
     }
+    d.fL2 = (float)(L - 2);
+    d.fL1 = (float)(L - 1);
     return d;
 }
