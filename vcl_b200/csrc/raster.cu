@@ -548,9 +548,19 @@ __global__ void __launch_bounds__(256) k_medium(const RTri* __restrict__ setup, 
 
 // Winning key -> (u, v, z/w, id+1) and DB per pixel; held to 32 registers
 // for eight blocks per SM (the record and vertex gathers need the warps).
+// The pixel's (view, row, column) come by multiply-high division (when
+// npix < 2^32; 64-bit division above) and W, H, 2 / W, 2 / H as
+// host-computed floats (the same values): no integer division or conversion
+// per pixel beyond the pixel centre's.
+struct ResolveDims {
+    FastDiv div_w, div_hw;
+    float fW, fH, xs, ys;
+    int big;
+};
 __global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ setup, int nt, int W, int H, long long npix,
                           const unsigned long long* __restrict__ keys, const float4* __restrict__ clip, int nv,
-                          const uint32_t* __restrict__ tri, float4* __restrict__ rast, float4* __restrict__ db) {
+                          const uint32_t* __restrict__ tri, float4* __restrict__ rast, float4* __restrict__ db,
+                          ResolveDims rd) {
     const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= npix) return;
     const unsigned long long key = keys[pix];
@@ -559,13 +569,19 @@ __global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ set
         if (db) db[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
-    const long long hw = (long long)W * H;
-    const int view = (int)(pix / hw);
-    const int rem = (int)(pix - view * hw);
-    const int py = rem / W, px = rem - py * W;
+    int view, rem;
+    if (rd.big) {
+        const long long hw = (long long)W * H;
+        view = (int)(pix / hw);
+        rem = (int)(pix - view * hw);
+    } else {
+        view = (int)fastdiv((unsigned)pix, rd.div_hw);
+        rem = (int)((unsigned)pix - (unsigned)view * ((unsigned)W * (unsigned)H));
+    }
+    const int py = (int)fastdiv((unsigned)rem, rd.div_w), px = rem - py * W;
     const int t = (int)(unsigned)(key & 0xffffffffu);
     const RTri r = setup[(size_t)view * nt + t];
-    const float sx = ndc(px, W), sy = ndc(py, H);
+    const float sx = dvd((float)(2 * px + 1 - W), rd.fW), sy = dvd((float)(2 * py + 1 - H), rd.fH);
     float A0 = edge(r.a.x, r.b.x, r.k.x, sx, sy);
     float A1 = edge(r.a.y, r.b.y, r.k.y, sx, sy);
     float A2 = edge(r.a.z, r.b.z, r.k.z, sx, sy);
@@ -575,7 +591,7 @@ __global__ void __launch_bounds__(256, 8) k_resolve(const RTri* __restrict__ set
     if (db) {
         const float4* cv = clip + (size_t)view * nv;
         float4 c0 = cv[tri[3 * (size_t)t]], c1 = cv[tri[3 * (size_t)t + 1]], c2 = cv[tri[3 * (size_t)t + 2]];
-        db[pix] = db_eval(c0, c1, c2, dvd(2.f, (float)W), dvd(2.f, (float)H), u, v);
+        db[pix] = db_eval(c0, c1, c2, rd.xs, rd.ys, u, v);
     }
 }
 
@@ -811,8 +827,14 @@ vcl_status raster_fwd_ws(vcl_ctx* ctx, void* ws, const RasterSched& rs, int* fla
     else
         k_fine<32><<<grid, dim3(32, 32), 0, s>>>(w.setup, w.count, w.offset, w.list, cap, nt, W, H, tiles_x,
                                                (int)ntiles_view, w.keys, flags, sa, ma);
+    ResolveDims rd;
+    rd.div_w = fastdiv_make((unsigned)W);
+    rd.div_hw = fastdiv_make((unsigned)W * (unsigned)H);
+    rd.fW = (float)W; rd.fH = (float)H;
+    rd.xs = 2.f / rd.fW; rd.ys = 2.f / rd.fH;
+    rd.big = npix > 0xffffffffll;
     k_resolve<<<vcl_blocks(npix, 256), 256, 0, s>>>(w.setup, nt, W, H, npix, w.keys, (const float4*)clip, nv, tri,
-                                                     (float4*)rast, (float4*)db);
+                                                     (float4*)rast, (float4*)db, rd);
     return vcl_launch_check(ctx, "rasterize_fwd");
 }
 
