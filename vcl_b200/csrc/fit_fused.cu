@@ -348,9 +348,10 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // shuffles, as many rounds as the longest run needs) and the last lane of a
 // run issues its three vector reductions: neighbouring pixels of one
 // triangle no longer collide on the same three addresses.  Blocks of 128
-// threads at up to 64 registers (no spills), so that its blocks fit, at a
-// fine grain, on the SMs beside the lobe-gradient blocks it runs with.
-__global__ void __launch_bounds__(128, 8) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+// threads at up to 48 registers (a few spills, in L1), so that four of its
+// blocks fit, at a fine grain, on each SM beside the three lobe-gradient
+// blocks it runs with.
+__global__ void __launch_bounds__(128, 10) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, const float4* __restrict__ tsr,
                                                  float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
@@ -405,10 +406,12 @@ __global__ void __launch_bounds__(128, 8) k_bwd_pix(ShadeIn a, TexDesc td, const
 // pairs).  Once a chunk is staged, the next chunk's records and dL/dout
 // are copied into shared memory asynchronously (cp.async, one buffer per
 // warp) while the current one is consumed, their pixel indices loaded one
-// chunk earlier still, so no registers hold data in flight.  At most LOBE_REGS registers, so
-// that three blocks of this kernel and the per-pixel backward's blocks share
-// each SM.  C = 4.
-constexpr int LOBE_REGS = 112;
+// chunk earlier still, so no registers hold data in flight.  At most
+// LOBE_REGS registers (a few loop-invariant values spill to L1), so that
+// three blocks of this kernel and five of the per-pixel backward share each
+// SM: the pair finishes sooner than with the lobe kernel spill-free at 96
+// registers beside four per-pixel blocks.  C = 4.
+constexpr int LOBE_REGS = 88;
 template <bool EXACT>
 __global__ void __maxnreg__(LOBE_REGS) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
                                                  float* __restrict__ g_axis, float* __restrict__ g_sharp,
