@@ -208,8 +208,8 @@ DRAM_BYTES_PER_PIXEL = {
 BOUND_NOTE = {
     "bwd_pix": "k_bwd_pix is bound by the scatter of texel gradients through L2 (vector reductions; "
                "L2 ~50% busy, warps waiting on loads and the LSU queue), not by HBM bandwidth",
-    "sg_lobes": "k_sg_lobes is FP32/MUFU-bound (per pixel and lobe: 2 rsqrt, 4 ex2, ~35 paired FP32 ops), "
-                "not HBM-bound",
+    "sg_lobes": "k_sg_lobes is bound by its FMA pipe and MUFU (per pixel and lobe: 2 rsqrt, 4 ex2 and ~65 FP32 "
+                "operations issued as ~33 paired instructions for two pixels), not by HBM",
 }
 
 
