@@ -850,6 +850,16 @@ ShadeRec shade_rec(const vcl_fit* f, bool want) {
     return x;
 }
 
+// The antialias candidate lists (aa_cand_list_bytes) live in `g_uv`, which
+// the fused step does not use, when they fit there (8 bytes per pixel; only
+// images of a few pixels per tile do not), else the backward finds its
+// candidates again.
+uint16_t* aa_cand_list(const vcl_fit* f) {
+    const size_t N = (size_t)f->d.W * f->d.H * f->d.views;
+    return aa_cand_list_bytes(f->d.W, f->d.H, f->d.views) <= sizeof(float) * 2 * N
+               ? reinterpret_cast<uint16_t*>(f->g_uv) : nullptr;
+}
+
 // The fused stages, each one launch (shared by the captured step and the
 // per-kernel timing).
 vcl_status stage_shade(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
@@ -867,7 +877,16 @@ vcl_status stage_aa_mse(vcl_fit* f, cudaStream_t s) {
     const vcl_fit_desc& d = f->d;
     Fused* F = (Fused*)f->fused;
     return aa_edges_fwd_mse(f->ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, d.W, d.H, d.views, f->color,
-                            f->target, f->g_aa, F->d_corr + 2, reinterpret_cast<unsigned*>(F->d_corr + 3), f->loss, s);
+                            f->target, f->g_aa, F->d_corr + 2, reinterpret_cast<unsigned*>(F->d_corr + 3), f->loss,
+                            aa_cand_list(f), s);
+}
+
+// The antialias backward of the step, reusing the forward's candidate lists.
+vcl_status stage_aa_bwd(vcl_fit* f, cudaStream_t s) {
+    const vcl_fit_desc& d = f->d;
+    Fused* F = (Fused*)f->fused;
+    return aa_edges_bwd(f->ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, d.W, d.H, d.views, 4, f->color, f->g_aa,
+                        f->g_color, d.learn_pos ? f->g_clip : nullptr, s, aa_cand_list(f));
 }
 
 vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
@@ -915,8 +934,7 @@ vcl_status enqueue(vcl_fit* f, cudaStream_t s) {
     const TexDesc td = make_desc(d.tex_w, d.tex_h, 4, d.levels);
     TRY(stage_shade(f, a, td, s));
     TRY(stage_aa_mse(f, s));
-    TRY(aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa, f->g_color,
-                     d.learn_pos ? f->g_clip : nullptr, s));
+    TRY(stage_aa_bwd(f, s));
     const bool lobes = d.learn_lobes && d.K;
     // the lobe gradients run beside the per-pixel backward on a forked stream
     if (lobes) {
@@ -1127,8 +1145,7 @@ vcl_status fit_fused_time_kernels(vcl_fit* f, cudaStream_t s, int reps, float* m
                                              V, f->rast, f->db, s);
                 case 1: return stage_shade(f, a, td, s);
                 case 2: return stage_aa_mse(f, s);
-                case 3: return aa_edges_bwd(ctx, f->clip, F->scr, d.nv, f->tri, d.nt, f->rast, W, H, V, 4, f->color, f->g_aa,
-                                            f->g_color, d.learn_pos ? f->g_clip : nullptr, s);
+                case 3: return stage_aa_bwd(f, s);
                 case 4: return stage_bwd_pix(f, a, td, s);
                 case 5: return (d.learn_lobes && d.K) ? stage_lobes(f, a, td, s) : VCL_OK;
                 default: {

@@ -558,6 +558,10 @@ __global__ void k_aa_bwd(const float4* __restrict__ clip, const float4* __restri
 constexpr int AAT_X = 32, AAT_Y = 8;
 constexpr int AAT_NH = (AAT_X + 1) * AAT_Y;   // horizontal pairs of a tile (with halo column)
 constexpr int AAT_NP = AAT_NH + AAT_X * (AAT_Y + 1);
+// A tile's candidate list kept between the forward and the backward of one
+// step (entry 0: the count; then the pair indices), AAT_CL entries per tile.
+constexpr int AAT_CL = 560;
+static_assert(AAT_NP < AAT_CL && AAT_NP < 65536, "candidate list entries");
 
 // Pair i of the tile at (x0, y0): direction and the coordinates of q;
 // `own`: the pair belongs to this tile (not its halo).
@@ -629,7 +633,7 @@ __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict
                                                      int nv, const uint32_t* __restrict__ tri, int nt,
                                                      const float4* __restrict__ rast, int W, int H,
                                                      const float4* __restrict__ in, float4* __restrict__ out, int* flags,
-                                                     MseOut mse) {
+                                                     MseOut mse, uint16_t* __restrict__ clist) {
     __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
     __shared__ int s_list[AAT_NP], s_n;
     const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
@@ -639,6 +643,11 @@ __global__ void __launch_bounds__(256, 8) k_aa_fwd_tile(const float4* __restrict
     const float2 s = make_float2(W / 2.f, H / 2.f);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
+    if (clist) {   // for the backward of the same step (same rast, same candidates)
+        uint16_t* cl = clist + ((size_t)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * AAT_CL;
+        for (int k = threadIdx.x; k < ncand; k += blockDim.x) cl[1 + k] = (uint16_t)s_list[k];
+        if (threadIdx.x == 0) cl[0] = (uint16_t)ncand;
+    }
     for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
         const int i = s_list[k];
         int dir, qx, qy;
@@ -700,7 +709,7 @@ __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict
                                                      const float4* __restrict__ rast, int W, int H,
                                                      const float4* __restrict__ in, const float4* __restrict__ gout,
                                                      float4* __restrict__ gin, float* __restrict__ gclip, int exact,
-                                                     int* flags) {
+                                                     int* flags, const uint16_t* __restrict__ clist) {
     __shared__ float4 s_lo[AAT_NP], s_hi[AAT_NP];
     __shared__ int s_list[AAT_NP], s_n;
     const int view = blockIdx.z, x0 = blockIdx.x * AAT_X, y0 = blockIdx.y * AAT_Y;
@@ -710,7 +719,19 @@ __global__ void __launch_bounds__(256, 8) k_aa_bwd_tile(const float4* __restrict
     float* gv = gclip ? gclip + (size_t)view * nv * 4 : nullptr;
     const float2 s = make_float2(W / 2.f, H / 2.f);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
+    int ncand;
+    if (clist) {   // the forward's list of this tile
+        const uint16_t* cl = clist + ((size_t)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * AAT_CL;
+        ncand = cl[0];
+        for (int i = threadIdx.x; i < AAT_NP; i += blockDim.x) {
+            s_lo[i] = z;
+            s_hi[i] = z;
+            if (i < ncand) s_list[i] = cl[1 + i];
+        }
+        __syncthreads();
+    } else {
+        ncand = aat_candidates(rast, vb, W, H, x0, y0, s_lo, s_hi, s_list, &s_n);
+    }
     for (int k = threadIdx.x; k < ncand; k += blockDim.x) {
         const int i = s_list[k];
         int dir, qx, qy;
@@ -826,35 +847,40 @@ vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int n
     if (C == 4 && aligned16(in) && aligned16(out) && views <= 65535)
         k_aa_fwd_tile<false><<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt,
                                                                     (const float4*)rast, W, H, (const float4*)in,
-                                                                    (float4*)out, ctx->dev_flags, MseOut{});
+                                                                    (float4*)out, ctx->dev_flags, MseOut{}, nullptr);
     else
         k_aa_fwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                          H, npix, C, in, out, ctx->dev_flags);
     return vcl_launch_check(ctx, "antialias_fwd");
 }
 
+size_t aa_cand_list_bytes(int W, int H, int views) {
+    const dim3 g = aat_grid(W, H, views);
+    return sizeof(uint16_t) * AAT_CL * (size_t)g.x * g.y * g.z;
+}
+
 vcl_status aa_edges_fwd_mse(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                             const float* rast, int W, int H, int views, const float* in, const float* target,
-                            float* grad, double* sum, unsigned* done, float* loss, cudaStream_t s) {
+                            float* grad, double* sum, unsigned* done, float* loss, uint16_t* clist, cudaStream_t s) {
     VCL_REQUIRE(aligned16(in) && aligned16(target) && aligned16(grad) && views <= 65535,
                 "antialias+mse: 16-byte aligned C = 4 buffers and at most 65535 views");
     k_aa_fwd_tile<true><<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, (const float4*)scr, nv, tri, nt,
                                                                (const float4*)rast, W, H, (const float4*)in,
                                                                (float4*)grad, ctx->dev_flags,
-                                                               MseOut{(const float4*)target, sum, done, loss});
+                                                               MseOut{(const float4*)target, sum, done, loss}, clist);
     return vcl_launch_check(ctx, "antialias_fwd+mse");
 }
 
 vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                         const float* rast, int W, int H, int views, int C, const float* in, const float* grad_out,
-                        float* grad_in, float* grad_clip, cudaStream_t s) {
+                        float* grad_in, float* grad_clip, cudaStream_t s, const uint16_t* clist) {
     long long npix = (long long)W * H * views;
     int exact = ctx->mode == VCL_MODE_EXACT;
     const float4* sc = (const float4*)scr;
     if (C == 4 && aligned16(in) && aligned16(grad_out) && aligned16(grad_in) && views <= 65535)
         k_aa_bwd_tile<<<aat_grid(W, H, views), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                              H, (const float4*)in, (const float4*)grad_out,
-                                                             (float4*)grad_in, grad_clip, exact, ctx->dev_flags);
+                                                             (float4*)grad_in, grad_clip, exact, ctx->dev_flags, clist);
     else
         k_aa_bwd<0><<<vcl_blocks(npix, 256), 256, 0, s>>>((const float4*)clip, sc, nv, tri, nt, (const float4*)rast, W,
                                                          H, npix, C, in, grad_out, grad_in, grad_clip, exact,

@@ -9,12 +9,16 @@ vcl_status aa_edges_fwd(vcl_ctx* ctx, const float* clip, const float* scr, int n
 // Antialias forward (C = 4) fused with the MSE: writes grad = aa - target and
 // the loss 0.5 sum |aa - target|^2 (through the double `sum` and block counter
 // `done`, both zero before the first call and left zero after each call).
+// `clist` (may be NULL): the per-tile candidate lists this forward finds,
+// aa_cand_list_bytes(W, H, views) bytes, for aa_edges_bwd of the same step
+// (same rast) to reuse instead of finding them again.
+size_t aa_cand_list_bytes(int W, int H, int views);
 vcl_status aa_edges_fwd_mse(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                             const float* rast, int W, int H, int views, const float* in, const float* target,
-                            float* grad, double* sum, unsigned* done, float* loss, cudaStream_t s);
+                            float* grad, double* sum, unsigned* done, float* loss, uint16_t* clist, cudaStream_t s);
 vcl_status aa_edges_bwd(vcl_ctx* ctx, const float* clip, const float* scr, int nv, const uint32_t* tri, int nt,
                         const float* rast, int W, int H, int views, int C, const float* in, const float* grad_out,
-                        float* grad_in, float* grad_clip, cudaStream_t s);
+                        float* grad_in, float* grad_clip, cudaStream_t s, const uint16_t* clist = nullptr);
 // Per-vertex screen terms for the antialias kernels (`scr` above, 8 floats
 // per view-vertex; NULL there computes them per pixel pair instead).
 void launch_aa_screen(const float* clip, long long n, int W, int H, float* scr, cudaStream_t s);
