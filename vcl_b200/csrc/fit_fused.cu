@@ -347,11 +347,11 @@ DEV void pix_geom(const ShadeIn& a, const TexDesc& td, const float* __restrict__
 // each run of consecutive lanes on the same triangle (a segmented scan by
 // shuffles, as many rounds as the longest run needs) and the last lane of a
 // run issues its three vector reductions: neighbouring pixels of one
-// triangle no longer collide on the same three addresses.  Blocks of 128
-// threads at up to 48 registers (a few spills, in L1), so that four of its
-// blocks fit, at a fine grain, on each SM beside the three lobe-gradient
-// blocks it runs with.
-__global__ void __launch_bounds__(128, 10) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
+// triangle no longer collide on the same three addresses.  Blocks of 64
+// threads at up to 48 registers (a few spills, in L1), so that its blocks
+// fit, at a fine grain, on each SM beside the three lobe-gradient blocks it
+// runs with.
+__global__ void __launch_bounds__(64, 20) k_bwd_pix(ShadeIn a, TexDesc td, const float4* __restrict__ g_color,
                                                  const float4* __restrict__ diffenv, const float4* __restrict__ tsr,
                                                  float* __restrict__ g_pyr,
                                                  const float* __restrict__ clip, float* __restrict__ g_clip,
@@ -408,9 +408,9 @@ __global__ void __launch_bounds__(128, 10) k_bwd_pix(ShadeIn a, TexDesc td, cons
 // warp) while the current one is consumed, their pixel indices loaded one
 // chunk earlier still, so no registers hold data in flight.  At most
 // LOBE_REGS registers (a few loop-invariant values spill to L1), so that
-// three blocks of this kernel and five of the per-pixel backward share each
-// SM: the pair finishes sooner than with the lobe kernel spill-free at 96
-// registers beside four per-pixel blocks.  C = 4.
+// three blocks of this kernel and ten 64-thread blocks of the per-pixel
+// backward share each SM: the pair finishes sooner than with the lobe kernel
+// spill-free at 96 registers beside fewer per-pixel blocks.  C = 4.
 constexpr int LOBE_REGS = 88;
 template <bool EXACT>
 __global__ void __maxnreg__(LOBE_REGS) k_sg_lobes(ShadeIn a, ShadeRec rec, const float4* __restrict__ g_color,
@@ -910,7 +910,7 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
 
 vcl_status stage_bwd_pix(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStream_t s) {
     const vcl_fit_desc& d = f->d;
-    k_bwd_pix<<<vcl_blocks(a.npix, 128), 128, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
+    k_bwd_pix<<<vcl_blocks(a.npix, 64), 64, 0, s>>>(a, td, (const float4*)f->g_color, (const float4*)f->diffuse,
                                                       shade_rec(f, false).tsr, f->g_pyr, f->clip, f->g_clip,
                                                       d.learn_tex, d.learn_pos);
     return vcl_launch_check(f->ctx, "fused backward");
