@@ -219,16 +219,21 @@ def test_raster_edge_cases(ctx):
         (np.array([[-0.5, -0.5, -2, 0.5], [2, -1, 0.5, 1.5], [-1, 2, 0.9, 1.0]], np.float32), [[0, 1, 2]]),  # near clip
         (np.array([[-1, -1, 0, -1], [3, -1, 0, 2], [-1, 3, 0, 2]], np.float32), [[0, 1, 2]]),  # one vertex behind
     ]
-    for W, H in ((7, 5), (16, 16), (33, 17)):
+    # image sizes down to one pixel, one row and one column, and several
+    # views of them (the pixel -> (view, row, column) split at its edges)
+    for W, H, V in ((7, 5, 1), (16, 16, 1), (33, 17, 1), (1, 1, 1), (1, 6, 1), (6, 1, 1), (2, 3, 1), (1, 5, 3),
+                    (5, 1, 2), (1, 1, 4), (7, 5, 3)):
         for clip, tri in cases:
             tri = np.array(tri, np.uint32)
-            N = W * H
+            clipv = np.ascontiguousarray(np.tile(clip[None], (V, 1, 1)))
+            N = W * H * V
             r = np.zeros((N, 4), np.float32); d = np.zeros((N, 4), np.float32)
-            O.orc().rasterize_fwd(W, H, 1, clip, clip.shape[0], tri, tri.shape[0], 1, r, d)
+            O.orc().rasterize_fwd(W, H, V, clipv, clip.shape[0], tri, tri.shape[0], 1, r, d)
             gr = G.zeros(N, 4); gd = G.zeros(N, 4)
-            ctx.rasterize_fwd(G.dev(clip), clip.shape[0], G.dev(tri.astype(np.int32)), tri.shape[0], W, H, 1, gr, gd, None)
-            assert np.array_equal(G.host(gr), r), (W, H, tri.shape)
-            assert np.array_equal(G.host(gd), d)
+            ctx.rasterize_fwd(G.dev(clipv), clip.shape[0], G.dev(tri.astype(np.int32)), tri.shape[0], W, H, V, gr, gd,
+                              None)
+            assert np.array_equal(G.host(gr), r), (W, H, V, tri.shape)
+            assert np.array_equal(G.host(gd), d), (W, H, V, tri.shape)
     # empty mesh
     gr = G.zeros(64, 4)
     ctx.rasterize_fwd(G.zeros(1, 4), 0, G.dev(np.zeros((1, 3), np.int32)), 0, 8, 8, 1, gr, None, None)
