@@ -337,8 +337,11 @@ VCL_API vcl_status vcl_fit_step(vcl_fit* fit, void* stream);
 VCL_API vcl_status vcl_fit_prepare(vcl_fit* fit, void* stream);
 /* Uploads the NEXT step's target images from host memory (pinned, for an
  * asynchronous copy) into a staging buffer on `copy_stream`, so that the
- * upload overlaps the current step; the next vcl_fit_step consumes it.  One
- * staged target at a time (VCL_ERR_ARG if the last one was not consumed). */
+ * upload overlaps the current step; the next vcl_fit_step consumes it.  Two
+ * device staging buffers are used in turn (allocated at the first two
+ * calls), so an upload does not wait for the step that consumes the one
+ * before it.  One staged target at a time (VCL_ERR_ARG if the last one was
+ * not consumed). */
 VCL_API vcl_status vcl_fit_stage_target(vcl_fit* fit, const float* host_src, void* copy_stream);
 /* Forward only with the current parameters: antialiased image
  * [views][H][W][C] into the device buffer `out`. */

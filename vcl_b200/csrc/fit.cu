@@ -173,9 +173,11 @@ VCL_API vcl_status vcl_fit_create(vcl_ctx* ctx, const vcl_fit_desc* desc, vcl_fi
 
 VCL_API void vcl_fit_destroy(vcl_fit* f) {
     if (!f) return;
-    if (f->staging) cudaFree(f->staging);
-    if (f->st_full) cudaEventDestroy(f->st_full);
-    if (f->st_free) cudaEventDestroy(f->st_free);
+    for (int b = 0; b < 2; ++b) {
+        if (f->staging[b]) cudaFree(f->staging[b]);
+        if (f->st_full[b]) cudaEventDestroy(f->st_full[b]);
+        if (f->st_free[b]) cudaEventDestroy(f->st_free[b]);
+    }
     if (f->arena) cudaFree(f->arena);
     fit_fused_release(f, nullptr, false);
     delete f;
@@ -184,9 +186,11 @@ VCL_API void vcl_fit_destroy(vcl_fit* f) {
 VCL_API void vcl_fit_destroy_async(vcl_fit* f, void* stream) {
     if (!f) return;
     cudaStream_t s = (cudaStream_t)stream;
-    if (f->staging) cudaFreeAsync(f->staging, s);
-    if (f->st_full) cudaEventDestroy(f->st_full);
-    if (f->st_free) cudaEventDestroy(f->st_free);
+    for (int b = 0; b < 2; ++b) {
+        if (f->staging[b]) cudaFreeAsync(f->staging[b], s);
+        if (f->st_full[b]) cudaEventDestroy(f->st_full[b]);
+        if (f->st_free[b]) cudaEventDestroy(f->st_free[b]);
+    }
     if (f->arena) cudaFreeAsync(f->arena, s);
     fit_fused_release(f, s, true);
     delete f;
@@ -428,25 +432,30 @@ VCL_API vcl_status vcl_fit_stage_target(vcl_fit* f, const float* host_src, void*
     VCL_REQUIRE(host_src, "null target");
     VCL_REQUIRE(!f->st_pending, "a staged target has not been consumed by a step yet");
     const size_t bytes = sizeof(float) * (size_t)f->d.W * f->d.H * f->d.views * f->d.C;
-    if (!f->staging) {
-        cudaError_t e = cudaMalloc(&f->staging, bytes);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_full, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_free, cudaEventDisableTiming);
+    const int b = f->st_next;
+    if (!f->staging[b]) {
+        cudaError_t e = cudaMalloc(&f->staging[b], bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_full[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->st_free[b], cudaEventDisableTiming);
         if (e != cudaSuccess) {
             (void)cudaGetLastError();
             return vcl_fail(ctx, VCL_ERR_NOMEM, "target staging buffer: %s", cudaGetErrorString(e));
         }
     }
     cudaStream_t cs = (cudaStream_t)copy_stream;
-    // the previous staged target must have been moved out of the buffer
-    if (f->st_used) {
-        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(cs, f->st_free, 0), "staging wait");
+    // the target this buffer held last (two uploads ago) must have been
+    // moved out of it; the previous upload's buffer is the other one
+    if (f->st_used[b]) {
+        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(cs, f->st_free[b], 0), "staging wait");
         if (st) return st;
     }
-    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->staging, host_src, bytes, cudaMemcpyHostToDevice, cs),
+    vcl_status st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->staging[b], host_src, bytes, cudaMemcpyHostToDevice, cs),
                                    "target staging copy");
-    if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_full, cs), "staging event");
-    if (!st) f->st_pending = true;
+    if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_full[b], cs), "staging event");
+    if (!st) {
+        f->st_pending = true;
+        f->st_next = b ^ 1;
+    }
     return st;
 }
 
@@ -458,13 +467,14 @@ VCL_API vcl_status vcl_fit_step(vcl_fit* f, void* stream) {
         // a staged target becomes this step's target: wait for its upload,
         // move it in on the device, free the staging buffer for the next one
         const size_t bytes = sizeof(float) * (size_t)f->d.W * f->d.H * f->d.views * f->d.C;
-        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(s, f->st_full, 0), "staging wait");
-        if (!st) st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->target, f->staging, bytes, cudaMemcpyDeviceToDevice, s),
+        const int b = f->st_next ^ 1;
+        vcl_status st = vcl_cuda_check(ctx, cudaStreamWaitEvent(s, f->st_full[b], 0), "staging wait");
+        if (!st) st = vcl_cuda_check(ctx, cudaMemcpyAsync(f->target, f->staging[b], bytes, cudaMemcpyDeviceToDevice, s),
                                      "staged target");
-        if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_free, s), "staging event");
+        if (!st) st = vcl_cuda_check(ctx, cudaEventRecord(f->st_free[b], s), "staging event");
         if (st) return st;
         f->st_pending = false;
-        f->st_used = true;
+        f->st_used[b] = true;
     }
     return f->strategy == VCL_FIT_FUSED ? fit_step_fused(f, s) : fit_step_plain(f, s);
 }

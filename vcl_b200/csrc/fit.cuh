@@ -21,11 +21,16 @@ struct vcl_fit {
     float* loss;
     // fused-strategy resources
     void* fused = nullptr;
-    // staged target upload (vcl_fit_stage_target): device staging buffer,
-    // "staging filled" / "staging consumed" events, a fill not yet consumed
-    float* staging = nullptr;
-    cudaEvent_t st_full = nullptr, st_free = nullptr;
-    bool st_pending = false, st_used = false;
+    // staged target upload (vcl_fit_stage_target): two device staging
+    // buffers used in turn, so that an upload never waits for the step that
+    // consumes the previous one; per buffer a "filled" and a "consumed"
+    // event; st_next = the buffer the next upload fills, st_pending = a fill
+    // not yet consumed (of buffer st_next ^ 1), st_used[b] = buffer b was
+    // consumed at least once
+    float* staging[2] = {nullptr, nullptr};
+    cudaEvent_t st_full[2] = {nullptr, nullptr}, st_free[2] = {nullptr, nullptr};
+    int st_next = 0;
+    bool st_pending = false, st_used[2] = {false, false};
 };
 
 vcl_status fit_step_plain(vcl_fit* f, cudaStream_t s);
