@@ -246,10 +246,14 @@ def measure_unit_peaks(ctx, stream, reps=3):
     t_mufu = best(lambda: ctx._check(L.vcl_probe_mufu_throughput(ctx.h, out.data_ptr(), 4096, ctypes.byref(n), sh),
                                      "probe"))
     mufu = n.value
-    return {"l2_red_v4_per_s": reds / t_red, "mufu_ops_per_s": mufu / t_mufu,
-            "how": "vcl_probe_red_throughput (coalesced red.global.add.v4.f32 over 32 MB, 20 passes) and "
-                   "vcl_probe_mufu_throughput (8 independent ex2.approx/rsqrt.approx chains per thread, "
-                   "8 blocks of 256 per SM); best of 3, CUDA events"}
+    t_fma = best(lambda: ctx._check(L.vcl_probe_fma_throughput(ctx.h, out.data_ptr(), 16384, ctypes.byref(n), sh),
+                                    "probe"))
+    fma = n.value
+    return {"l2_red_v4_per_s": reds / t_red, "mufu_ops_per_s": mufu / t_mufu, "fma_ops_per_s": fma / t_fma,
+            "how": "vcl_probe_red_throughput (coalesced red.global.add.v4.f32 over 32 MB, 20 passes), "
+                   "vcl_probe_mufu_throughput (8 independent ex2.approx/rsqrt.approx chains per thread) and "
+                   "vcl_probe_fma_throughput (8 independent paired-FP32 fma chains per thread), 8 blocks of 256 "
+                   "per SM; best of 3, CUDA events"}
 
 
 # ------------------------------------------------------------------ vcl arm
@@ -813,6 +817,20 @@ def main():
                 "frac": ops / (kms[k] * 1e-3) / sfu_peak, "covered_pixels": ncov,
                 "peak_source": "measured (vcl_probe_mufu_throughput)" if "mufu_ops_per_s" in up else "nominal",
                 "nominal_gops": nominal / 1e9}
+            for k in ("shade_fwd", "sg_lobes") if kms.get(k, 0) > 0}
+        # their other bound, the FP32 FMA pipe: FP32 operations per covered
+        # pixel and lobe in the SG arithmetic as written (paired instructions
+        # counted as two): 34 in the shading sums (two lobes per
+        # instruction), 65 in the lobe gradients (COMPAT; two pixels per
+        # instruction), against the paired-FMA rate measured by the probe
+        fma_nominal = 128.0 * sms * mhz * 1e6
+        fma_peak = up.get("fma_ops_per_s") or fma_nominal
+        fma_ops = {"shade_fwd": 34.0 * ncov * S.K, "sg_lobes": 65.0 * ncov * S.K}
+        line["fma_roofline"] = {
+            k: {"fp32_ops": fma_ops[k], "achieved_gops": fma_ops[k] / (kms[k] * 1e-3) / 1e9,
+                "peak_gops": fma_peak / 1e9, "frac": fma_ops[k] / (kms[k] * 1e-3) / fma_peak,
+                "peak_source": "measured (vcl_probe_fma_throughput)" if "fma_ops_per_s" in up else "nominal",
+                "nominal_gops": fma_nominal / 1e9}
             for k in ("shade_fwd", "sg_lobes") if kms.get(k, 0) > 0}
         if "l2_red_v4_per_s" in up and kms.get("bwd_pix", 0) > 0:
             # the per-pixel backward's texel scatter: 4 vector reductions per

@@ -526,6 +526,11 @@ VCL_API vcl_status vcl_probe_red_throughput(vcl_ctx* ctx, float* buf, long long 
  * MUFU operations issued. */
 VCL_API long long vcl_probe_mufu_threads(const vcl_ctx* ctx);
 VCL_API vcl_status vcl_probe_mufu_throughput(vcl_ctx* ctx, float* out, int iters, long long* ops, void* stream);
+/* The same shape for the FP32 FMA pipe: eight independent chains per thread
+ * of paired FP32 fused multiply-adds (the form the SG kernels issue), `iters`
+ * links each; `out` holds vcl_probe_mufu_threads(ctx) floats; *ops = the
+ * number of FP32 operations (two per paired instruction). */
+VCL_API vcl_status vcl_probe_fma_throughput(vcl_ctx* ctx, float* out, int iters, long long* ops, void* stream);
 
 #ifdef __cplusplus
 }

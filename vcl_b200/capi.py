@@ -48,6 +48,7 @@ SIGNATURES = {
     "vcl_probe_red_throughput": (c_int, [P, P, c_ll, c_int, ctypes.POINTER(c_ll), P]),
     "vcl_probe_mufu_threads": (c_ll, [P]),
     "vcl_probe_mufu_throughput": (c_int, [P, P, c_int, ctypes.POINTER(c_ll), P]),
+    "vcl_probe_fma_throughput": (c_int, [P, P, c_int, ctypes.POINTER(c_ll), P]),
     "vcl_interpolate_fwd": (c_int, [P, P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P]),
     "vcl_interpolate_bwd": (c_int, [P, P, c_int, c_int, c_int, P, c_int, c_int, P, c_int, P, P, P, P]),
     "vcl_texture_fwd": (c_int, [P, P, P, P, c_int, c_int, c_int, P, c_int, c_int, c_int, c_int, P, P]),

@@ -1,10 +1,12 @@
-// Throughput probes for the two units other than HBM that bound the fit's
+// Throughput probes for the units other than HBM that bound the fit's
 // kernels: the L2 reduction units (the texel and vertex gradient scatters
-// issue red.global.add.v4.f32) and the MUFU pipe (the SG kernels' ex2 and
-// rsqrt).  Each probe runs a long, known number of those operations over the
+// issue red.global.add.v4.f32), the MUFU pipe (the SG kernels' ex2 and
+// rsqrt) and the FP32 FMA pipe driven by paired instructions (the SG
+// kernels' arithmetic).  Each probe runs a long, known number of those operations over the
 // whole GPU; the caller times it with CUDA events and divides.  Measurement
 // utilities only: no part of the fit path calls them.
 #include "common.cuh"
+#include "sg_math.cuh"
 
 namespace {
 
@@ -47,6 +49,24 @@ __global__ void __launch_bounds__(256) k_probe_mufu(float* __restrict__ out, int
     out[(long long)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Eight independent chains per thread of paired FP32 multiply-adds,
+// x -> x * 0.999 + 0.001 on both halves (values stay near 1): 16 FP32
+// operations per link.  One result per thread is stored.
+__global__ void __launch_bounds__(256) k_probe_ffma2(float* __restrict__ out, int iters) {
+    float2 a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = make_float2(0.5f + 0.01f * (float)((threadIdx.x + k) & 31), 0.75f);
+    const float2 m = p2(0.999f), c = p2(0.001f);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma2(a[k], m, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k].x + a[k].y;
+    out[(long long)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
 
 extern "C" {
@@ -72,6 +92,15 @@ VCL_API vcl_status vcl_probe_mufu_throughput(vcl_ctx* ctx, float* out, int iters
     k_probe_mufu<<<blocks, 256, 0, (cudaStream_t)stream>>>(out, iters);
     *ops = (long long)blocks * 256 * iters * 8 * 2;
     return vcl_launch_check(ctx, "probe_mufu_throughput");
+}
+
+VCL_API vcl_status vcl_probe_fma_throughput(vcl_ctx* ctx, float* out, int iters, long long* ops, void* stream) {
+    VCL_CTX_CHECK();
+    VCL_REQUIRE(out && iters > 0 && ops, "bad probe arguments");
+    const int blocks = ctx->sm_count * 8;
+    k_probe_ffma2<<<blocks, 256, 0, (cudaStream_t)stream>>>(out, iters);
+    *ops = (long long)blocks * 256 * iters * 8 * 2;
+    return vcl_launch_check(ctx, "probe_fma_throughput");
 }
 
 }  // extern "C"
