@@ -897,7 +897,7 @@ vcl_status stage_lobes(vcl_fit* f, const ShadeIn& a, const TexDesc& td, cudaStre
     long long chunks = (N + 31) / 32;
     long long want = (chunks + 3) / 4;
     // three lobe blocks per SM (over all lobe groups) leave registers for
-    // four 128-thread blocks of the per-pixel backward that runs beside this
+    // ten 64-thread blocks of the per-pixel backward that runs beside this
     // kernel (the two overlap on each SM)
     long long capg = ((long long)ctx->sm_count * 3 + groups - 1) / groups;
     const dim3 grid((unsigned)(want < capg ? (want < 1 ? 1 : want) : capg), (unsigned)groups);
