@@ -217,3 +217,28 @@ def test_position_gradients_match_central_differences():
         assert abs(fd - g[i]) <= 2e-4 * scale, (i, fd, g[i])
         checked += 1
     assert checked >= 20
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_exact_stage_values_close_to_fp32_chain(mode):
+    """The exact stage values the GPU parity bars measure against
+    (chain.run_isolated64, each operator of the double build fed the FP32
+    chain's inputs, or with chained=True its own double results) are the
+    same computation as the FP32 restatement: every key within FP32 rounding
+    of it, normwise (2e-5 isolated; 1e-4 chained, where the rounding of each
+    stage feeds the next)."""
+    import chain as C32
+    from vcl_b200 import scenes
+    keys = ["clip", "uv", "uv_da", "diffuse", "normal", "view", "spec_axis", "spec_sharp", "spec_amp", "color",
+            "diffenv", "specenv", "aa", "g_aa", "g_color", "g_clip_aa", "g_diffuse", "g_axis", "g_sharp", "g_amp",
+            "g_sax", "g_ssh", "g_sam", "g_rough", "g_pyr", "g_uv", "g_uv_da", "g_uvattr", "g_bary", "g_clip",
+            "g_pos"]
+    S = scenes.small(seed=2, W=64, H=48, views=3, subdiv=2, tex=64, K=5)
+    o = C32.run_chain(O.orc(), S, mode, pyr=C32.build_pyramid(S, S.tex_target))
+    for chained, tol in ((False, 2e-5), (True, 1e-4)):
+        e = C32.run_isolated64(S, o, mode, chained=chained)
+        for k in keys:
+            a = np.asarray(o[k], np.float64).reshape(-1)
+            b = np.asarray(e[k], np.float64).reshape(-1)
+            err = np.abs(a - b).max(initial=0.0) / max(np.abs(b).max(initial=0.0), 1e-30)
+            assert err <= tol, (k, chained, err)
