@@ -222,3 +222,38 @@ def test_tie_census_known_answers():
     f = np.zeros(S.W * S.H, np.uint32)
     O.orc().raster_ties(S.W, S.H, 1, clip, S.nv, S.tri, S.nt, r, f, c)
     assert tuple(c) == (0, 0)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_sg_bwd_guarded_adds_drop_exactly_the_non_finite_terms(mode):
+    """The restatement of the reference's guarded add (common.h:181) in the
+    SG backward (material.cu:428-433): a NaN in channel c of dL/dout at one
+    pixel drops that pixel's amplitude and diffuse terms of channel c (the
+    same sums as with that channel's dL/dout set to 0) and its axis and
+    sharpness terms, which mix every channel (the same sums as with the
+    pixel's whole dL/dout set to 0); the results stay finite."""
+    S = scenes.small(seed=2, W=64, H=48, views=3, subdiv=2, tex=64, K=5)
+    o = chain.run_chain(O.orc(), S, mode, pyr=chain.build_pyramid(S, S.tex_target))
+    N, C, K = S.W * S.H * S.views, S.C, S.K
+    p = int(np.nonzero(o["rast"][:, 3] > 0)[0][17])
+
+    def lobes(g):
+        out = {"g_diffuse": np.zeros((N, C), np.float32), "g_axis": np.zeros((K, 3), np.float32),
+               "g_sharp": np.zeros(K, np.float32), "g_amp": np.zeros((K, C), np.float32)}
+        O.orc().sg_bwd(mode, S.W, S.H, S.views, C, o["rast"], K, S.lobe_axis_init, S.lobe_sharp_init,
+                       S.lobe_amp_init, o["normal"], o["diffuse"], o["spec_axis"], o["spec_sharp"], o["spec_amp"],
+                       np.ascontiguousarray(g, np.float32), out["g_diffuse"], out["g_axis"], out["g_sharp"],
+                       out["g_amp"], None, None, None)
+        return out
+
+    g = o["g_color"].reshape(N, C).copy()
+    g_nan = g.copy(); g_nan[p, 1] = np.nan
+    g_ch0 = g.copy(); g_ch0[p, 1] = 0.0
+    g_px0 = g.copy(); g_px0[p, :] = 0.0
+    a, b, c = lobes(g_nan), lobes(g_ch0), lobes(g_px0)
+    for k in a:
+        assert np.isfinite(a[k]).all(), k
+    assert np.array_equal(a["g_amp"], b["g_amp"])
+    assert np.array_equal(a["g_diffuse"], b["g_diffuse"])
+    assert np.array_equal(a["g_axis"], c["g_axis"])
+    assert np.array_equal(a["g_sharp"], c["g_sharp"])
